@@ -1,0 +1,475 @@
+// C ABI of libdpkem.so (declared in include/dpkem.h): contexts, the scratch arena,
+// host<->device staging, chunking, status codes and the reference-compatible shims.
+//
+// The reference allocates, copies and frees device buffers inside every call
+// (FrodoKEM976-GPU/src/cuda_kernel.cu:29-46, SABER-GPU/src/cuda_kernel.cu:36-58) and
+// checks no CUDA status.  Here a context owns one device arena that grows only when a
+// larger chunk is requested (never inside a steady-state loop), calls on one context
+// are serialised on the device with an event so scratch is never shared by two
+// in-flight chains, and every entry point returns a status.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/dpkem.h"
+#include "common.cuh"
+
+using namespace dpkem;
+
+struct dpkem_ctx {
+  int device = 0;
+  size_t budget = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t last = nullptr;
+  uint8_t *arena = nullptr;
+  size_t arena_bytes = 0;
+  uint32_t *d_err = nullptr;
+  std::mutex mu;
+};
+
+namespace {
+
+thread_local int g_last_status = DPKEM_OK;
+
+int set_status(int s) {
+  g_last_status = s;
+  return s;
+}
+
+constexpr size_t kAlign = 256;
+constexpr size_t kDefaultBudget = 8ull << 30;
+
+size_t up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
+
+struct Sizes {
+  size_t pk, sk, ct, ss, kpc, encc;
+};
+
+bool scheme_sizes(int scheme, Sizes *z) {
+  if (scheme == DPKEM_FRODO976) {
+    *z = {frodo::PK, frodo::SK, frodo::CT, frodo::SS, frodo::KP_COINS, frodo::ENC_COINS};
+    return true;
+  }
+  if (scheme < 2 || scheme > 4) return false;
+  const saber::Params p = saber::params(scheme);
+  *z = {(size_t)p.pk, (size_t)p.sk, (size_t)p.ct, 32, 96, 32};
+  return true;
+}
+
+// Per-instance bytes of scratch and, in host mode, of device staging for each op.
+size_t scratch_per_instance(int scheme) {
+  if (scheme == DPKEM_FRODO976) return (size_t)frodo::RW * 2 + 24 + 24 + 4 + 64;
+  return saber_scratch_bytes(scheme) + 4 + 16;
+}
+
+size_t staging_per_instance(int scheme, int op) {
+  Sizes z;
+  scheme_sizes(scheme, &z);
+  switch (op) {
+    case OP_KEYPAIR: return z.kpc + z.pk + z.sk;
+    case OP_ENC: return z.pk + z.encc + z.ct + z.ss;
+    default: return z.ct + z.sk + z.ss;
+  }
+}
+
+size_t chunk_for(dpkem_ctx *c, int scheme, int op, bool host) {
+  const size_t per = scratch_per_instance(scheme) + (host ? staging_per_instance(scheme, op) : 0) + 8 * kAlign / 64;
+  const size_t usable = c->budget > (64u << 20) ? c->budget - (64u << 20) : c->budget / 2;
+  return std::max<size_t>(1, usable / per);
+}
+
+int ensure_arena(dpkem_ctx *c, size_t bytes) {
+  if (bytes <= c->arena_bytes) return DPKEM_OK;
+  if (bytes > c->budget) return DPKEM_ENOMEM;
+  if (c->arena) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->arena);
+    c->arena = nullptr;
+    c->arena_bytes = 0;
+  }
+  if (cudaMalloc(&c->arena, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return DPKEM_ENOMEM;
+  }
+  c->arena_bytes = bytes;
+  return DPKEM_OK;
+}
+
+struct Carver {
+  uint8_t *base;
+  size_t off = 0;
+  template <typename T>
+  T *take(size_t bytes) {
+    T *p = reinterpret_cast<T *>(base + off);
+    off += up(bytes);
+    return p;
+  }
+};
+
+// Layout of one chunk's arena: scratch first, then (host mode) staging.
+size_t arena_need(int scheme, int op, size_t chunk, bool host) {
+  size_t s = 0;
+  if (scheme == DPKEM_FRODO976) {
+    s += up(chunk * frodo::RW * 2) + up(chunk * 24) * 2 + up(chunk * 4);
+  } else {
+    s += up(chunk * saber_scratch_bytes(scheme)) + up(chunk * 4);
+  }
+  if (host) {
+    Sizes z;
+    scheme_sizes(scheme, &z);
+    switch (op) {
+      case OP_KEYPAIR: s += up(chunk * z.kpc) + up(chunk * z.pk) + up(chunk * z.sk); break;
+      case OP_ENC: s += up(chunk * z.pk) + up(chunk * z.encc) + up(chunk * z.ct) + up(chunk * z.ss); break;
+      default: s += up(chunk * z.ct) + up(chunk * z.sk) + up(chunk * z.ss); break;
+    }
+  }
+  return s;
+}
+
+bool aligned8(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 7u) == 0; }
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return DPKEM_OK;
+  cudaGetLastError();
+  return DPKEM_ECUDA;
+}
+
+// Runs op on n instances.  in0/in1/out0/out1 follow the op's argument order:
+//   keypair: in0 = coins, out0 = pk, out1 = sk
+//   enc:     in0 = coins, in1 = pk, out0 = ct, out1 = ss
+//   dec:     in0 = ct, in1 = sk, out0 = ss
+int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *in0, const uint8_t *in1, uint8_t *out0,
+           uint8_t *out1, unsigned flags, void *stream) {
+  Sizes z;
+  if (!c || !scheme_sizes(scheme, &z)) return DPKEM_EINVAL;
+  if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC && form != DPKEM_FORM_INT32) return DPKEM_EINVAL;
+  if (form == DPKEM_FORM_INT32) return DPKEM_EUNSUPPORTED;
+  if (n == 0) return DPKEM_OK;
+  if (n > (size_t)INT32_MAX) return DPKEM_EINVAL;
+  if (!in0 || !out0 || (op != OP_KEYPAIR && !in1) || (op != OP_DEC && !out1)) return DPKEM_EINVAL;
+  const bool dev = (flags & DPKEM_FLAG_DEVICE_PTRS) != 0;
+  if (dev && !(aligned8(in0) && aligned8(out0) && (!in1 || aligned8(in1)) && (!out1 || aligned8(out1))))
+    return DPKEM_EINVAL;
+  std::lock_guard<std::mutex> lock(c->mu);
+  if (cudaSetDevice(c->device) != cudaSuccess) return cuda_status(cudaErrorInvalidDevice);
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  const size_t chunk = std::min(n, chunk_for(c, scheme, op, !dev));
+  int rc = ensure_arena(c, arena_need(scheme, op, chunk, !dev));
+  if (rc) return rc;
+  cudaError_t e = cudaStreamWaitEvent(st, c->last, 0);
+  if (e != cudaSuccess) return cuda_status(e);
+
+  size_t in0_sz, in1_sz = 0, out0_sz, out1_sz = 0;
+  switch (op) {
+    case OP_KEYPAIR: in0_sz = z.kpc; out0_sz = z.pk; out1_sz = z.sk; break;
+    case OP_ENC: in0_sz = z.encc; in1_sz = z.pk; out0_sz = z.ct; out1_sz = z.ss; break;
+    default: in0_sz = z.ct; in1_sz = z.sk; out0_sz = z.ss; break;
+  }
+  for (size_t first = 0; first < n; first += chunk) {
+    const size_t m = std::min(chunk, n - first);
+    Carver cv{c->arena};
+    const uint8_t *d_in0, *d_in1 = nullptr;
+    uint8_t *d_out0, *d_out1 = nullptr;
+    FrodoBatch fb{};
+    SaberBatch sb{};
+    if (scheme == DPKEM_FRODO976) {
+      fb.rw = cv.take<uint16_t>(chunk * frodo::RW * 2);
+      fb.kk = cv.take<uint8_t>(chunk * 24);
+      fb.mu = cv.take<uint8_t>(chunk * 24);
+      fb.fail = cv.take<uint32_t>(chunk * 4);
+    } else {
+      sb.scr = cv.take<uint8_t>(chunk * saber_scratch_bytes(scheme));
+      sb.fail = cv.take<uint32_t>(chunk * 4);
+    }
+    if (dev) {
+      d_in0 = in0 + first * in0_sz;
+      d_in1 = in1 ? in1 + first * in1_sz : nullptr;
+      d_out0 = out0 + first * out0_sz;
+      d_out1 = out1 ? out1 + first * out1_sz : nullptr;
+    } else {
+      uint8_t *a = cv.take<uint8_t>(chunk * in0_sz);
+      uint8_t *b = in1_sz ? cv.take<uint8_t>(chunk * in1_sz) : nullptr;
+      d_out0 = cv.take<uint8_t>(chunk * out0_sz);
+      d_out1 = out1_sz ? cv.take<uint8_t>(chunk * out1_sz) : nullptr;
+      if ((e = cudaMemcpyAsync(a, in0 + first * in0_sz, m * in0_sz, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return cuda_status(e);
+      if (b && (e = cudaMemcpyAsync(b, in1 + first * in1_sz, m * in1_sz, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return cuda_status(e);
+      d_in0 = a;
+      d_in1 = b;
+    }
+    if (scheme == DPKEM_FRODO976) {
+      fb.n = (int)m;
+      fb.err = c->d_err;
+      switch (op) {
+        case OP_KEYPAIR:
+          fb.coins = d_in0; fb.pk = d_out0; fb.sk = d_out1;
+          e = frodo_keypair(fb, form, st);
+          break;
+        case OP_ENC:
+          fb.coins = d_in0; fb.pk = const_cast<uint8_t *>(d_in1); fb.ct = d_out0; fb.ss = d_out1;
+          e = frodo_enc(fb, form, st);
+          break;
+        default:
+          fb.ct = const_cast<uint8_t *>(d_in0); fb.sk = const_cast<uint8_t *>(d_in1); fb.ss = d_out0;
+          e = frodo_dec(fb, form, st);
+          break;
+      }
+    } else {
+      sb.n = (int)m;
+      sb.level = scheme;
+      sb.err = c->d_err;
+      switch (op) {
+        case OP_KEYPAIR:
+          sb.coins = d_in0; sb.pk = d_out0; sb.sk = d_out1;
+          e = saber_keypair(sb, form, st);
+          break;
+        case OP_ENC:
+          sb.coins = d_in0; sb.pk = const_cast<uint8_t *>(d_in1); sb.ct = d_out0; sb.ss = d_out1;
+          e = saber_enc(sb, form, st);
+          break;
+        default:
+          sb.ct = const_cast<uint8_t *>(d_in0); sb.sk = const_cast<uint8_t *>(d_in1); sb.ss = d_out0;
+          e = saber_dec(sb, form, st);
+          break;
+      }
+    }
+    if (e != cudaSuccess) return cuda_status(e);
+    if (!dev) {
+      if ((e = cudaMemcpyAsync(out0 + first * out0_sz, d_out0, m * out0_sz, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_status(e);
+      if (d_out1 &&
+          (e = cudaMemcpyAsync(out1 + first * out1_sz, d_out1, m * out1_sz, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_status(e);
+      // The next chunk reuses the staging buffers: finish this one first.
+      if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_status(e);
+    }
+  }
+  if ((e = cudaEventRecord(c->last, st)) != cudaSuccess) return cuda_status(e);
+  if (!dev) {
+    uint32_t err = 0;
+    if ((e = cudaMemcpyAsync(&err, c->d_err, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return cuda_status(e);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_status(e);
+    if (err) {
+      cudaMemsetAsync(c->d_err, 0, 4, st);
+      cudaStreamSynchronize(st);
+      return DPKEM_ETIMEOUT;
+    }
+  }
+  return DPKEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dpkem_ctx_create(dpkem_ctx **out, int device, size_t hbm_budget_bytes) {
+  if (!out) return set_status(DPKEM_EINVAL);
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return set_status(DPKEM_ECUDA);
+  }
+  if (cudaSetDevice(device) != cudaSuccess) return set_status(DPKEM_ECUDA);
+  dpkem_ctx *c = new dpkem_ctx();
+  c->device = device;
+  c->budget = hbm_budget_bytes ? hbm_budget_bytes : kDefaultBudget;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->last, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMalloc(&c->d_err, 4) != cudaSuccess || cudaMemset(c->d_err, 0, 4) != cudaSuccess) {
+    cudaGetLastError();
+    dpkem_ctx_destroy(c);
+    return set_status(DPKEM_ECUDA);
+  }
+  *out = c;
+  return set_status(DPKEM_OK);
+}
+
+int dpkem_ctx_destroy(dpkem_ctx *c) {
+  if (!c) return set_status(DPKEM_EINVAL);
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->last) cudaEventSynchronize(c->last);
+  if (c->arena) cudaFree(c->arena);
+  if (c->d_err) cudaFree(c->d_err);
+  if (c->last) cudaEventDestroy(c->last);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return set_status(DPKEM_OK);
+}
+
+int dpkem_sizes(int scheme, size_t *pk, size_t *sk, size_t *ct, size_t *ss, size_t *kp_coins, size_t *enc_coins) {
+  Sizes z;
+  if (!scheme_sizes(scheme, &z)) return set_status(DPKEM_EINVAL);
+  if (pk) *pk = z.pk;
+  if (sk) *sk = z.sk;
+  if (ct) *ct = z.ct;
+  if (ss) *ss = z.ss;
+  if (kp_coins) *kp_coins = z.kpc;
+  if (enc_coins) *enc_coins = z.encc;
+  return set_status(DPKEM_OK);
+}
+
+size_t dpkem_max_chunk(dpkem_ctx *c, int scheme) {
+  Sizes z;
+  if (!c || !scheme_sizes(scheme, &z)) return 0;
+  return std::min({chunk_for(c, scheme, OP_KEYPAIR, true), chunk_for(c, scheme, OP_ENC, true),
+                   chunk_for(c, scheme, OP_DEC, true)});
+}
+
+int dpkem_keypair_batch(dpkem_ctx *c, int scheme, int form, size_t n, const uint8_t *coins, uint8_t *pk, uint8_t *sk,
+                        unsigned flags, void *stream) {
+  return set_status(run_op(c, scheme, form, OP_KEYPAIR, n, coins, nullptr, pk, sk, flags, stream));
+}
+
+int dpkem_enc_batch(dpkem_ctx *c, int scheme, int form, size_t n, const uint8_t *coins, const uint8_t *pk, uint8_t *ct,
+                    uint8_t *ss, unsigned flags, void *stream) {
+  return set_status(run_op(c, scheme, form, OP_ENC, n, coins, pk, ct, ss, flags, stream));
+}
+
+int dpkem_dec_batch(dpkem_ctx *c, int scheme, int form, size_t n, const uint8_t *ct, const uint8_t *sk, uint8_t *ss,
+                    unsigned flags, void *stream) {
+  return set_status(run_op(c, scheme, form, OP_DEC, n, ct, sk, ss, nullptr, flags, stream));
+}
+
+int dpkem_coins(dpkem_ctx *c, size_t n, size_t len, uint64_t first, const char *tag, uint8_t *out, unsigned flags,
+                void *stream) {
+  if (!c || !out || !tag || len == 0 || len > 136 || strlen(tag) > 16 || n > (size_t)INT32_MAX)
+    return set_status(DPKEM_EINVAL);
+  if (n == 0) return set_status(DPKEM_OK);
+  const bool dev = (flags & DPKEM_FLAG_DEVICE_PTRS) != 0;
+  std::lock_guard<std::mutex> lock(c->mu);
+  cudaSetDevice(c->device);
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  CoinsBatch b{};
+  b.len = (int)len;
+  b.taglen = (int)strlen(tag);
+  memcpy(b.tag, tag, b.taglen);
+  cudaError_t e = cudaStreamWaitEvent(st, c->last, 0);
+  if (e != cudaSuccess) return set_status(cuda_status(e));
+  if (dev) {
+    b.n = (int)n;
+    b.first = first;
+    b.out = out;
+    if ((e = coins_generate(b, st)) != cudaSuccess) return set_status(cuda_status(e));
+    cudaEventRecord(c->last, st);
+    return set_status(DPKEM_OK);
+  }
+  const size_t chunk = std::max<size_t>(1, std::min(n, (c->budget / 2) / len));
+  int rc = ensure_arena(c, up(chunk * len));
+  if (rc) return set_status(rc);
+  for (size_t f = 0; f < n; f += chunk) {
+    const size_t m = std::min(chunk, n - f);
+    b.n = (int)m;
+    b.first = first + f;
+    b.out = c->arena;
+    if ((e = coins_generate(b, st)) != cudaSuccess) return set_status(cuda_status(e));
+    if ((e = cudaMemcpyAsync(out + f * len, c->arena, m * len, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      return set_status(cuda_status(e));
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return set_status(cuda_status(e));
+  }
+  cudaEventRecord(c->last, st);
+  return set_status(DPKEM_OK);
+}
+
+int dpkem_sync(dpkem_ctx *c, void *stream) {
+  if (!c) return set_status(DPKEM_EINVAL);
+  std::lock_guard<std::mutex> lock(c->mu);
+  cudaSetDevice(c->device);
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  uint32_t err = 0;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaMemcpy(&err, c->d_err, 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_status(cuda_status(e));
+  if (err) {
+    cudaMemset(c->d_err, 0, 4);
+    return set_status(DPKEM_ETIMEOUT);
+  }
+  return set_status(DPKEM_OK);
+}
+
+const char *dpkem_strerror(int s) {
+  switch (s) {
+    case DPKEM_OK: return "ok";
+    case DPKEM_EINVAL: return "invalid argument";
+    case DPKEM_ENOMEM: return "out of device memory or over the HBM budget";
+    case DPKEM_ECUDA: return "CUDA runtime error";
+    case DPKEM_ETIMEOUT: return "bounded device wait expired";
+    case DPKEM_EUNSUPPORTED: return "unsupported form";
+    default: return "unknown status";
+  }
+}
+
+int dpkem_last_status(void) { return g_last_status; }
+
+// ---------------------------------------------------------------- compatibility shims
+static std::mutex g_compat_mu;
+static dpkem_ctx *g_compat = nullptr;
+static size_t g_compat_batch = 768;
+static int g_compat_level = 3;
+static int g_compat_form = DPKEM_FORM_TC;
+
+static dpkem_ctx *compat_ctx() {
+  std::lock_guard<std::mutex> lock(g_compat_mu);
+  if (!g_compat && dpkem_ctx_create(&g_compat, 0, 0) != DPKEM_OK) g_compat = nullptr;
+  return g_compat;
+}
+
+void dpkem_set_compat_batch(size_t n) { g_compat_batch = n; }
+void dpkem_set_compat_saber_level(int l) { g_compat_level = l; }
+void dpkem_set_compat_form(int form) { g_compat_form = form; }
+
+static int compat_form_from_mode(uint8_t mode) {
+  return mode == 0 ? DPKEM_FORM_DP4A : mode == 2 ? DPKEM_FORM_TC : DPKEM_FORM_INT32;
+}
+
+void frodoKEMKeypair(uint8_t *h_pk, uint8_t *h_sk) {
+  dpkem_ctx *c = compat_ctx();
+  if (!c) return (void)set_status(DPKEM_ECUDA);
+  std::vector<uint8_t> coins(g_compat_batch * frodo::KP_COINS);
+  int rc = dpkem_coins(c, g_compat_batch, frodo::KP_COINS, 0, "kp", coins.data(), 0, nullptr);
+  if (rc == DPKEM_OK)
+    rc = dpkem_keypair_batch(c, DPKEM_FRODO976, g_compat_form, g_compat_batch, coins.data(), h_pk, h_sk, 0, nullptr);
+  set_status(rc);
+}
+
+void frodoKEMEncap(uint8_t *ct, uint8_t *ss, const uint8_t *pk) {
+  dpkem_ctx *c = compat_ctx();
+  if (!c) return (void)set_status(DPKEM_ECUDA);
+  std::vector<uint8_t> coins(g_compat_batch * frodo::ENC_COINS);
+  int rc = dpkem_coins(c, g_compat_batch, frodo::ENC_COINS, 0, "enc", coins.data(), 0, nullptr);
+  if (rc == DPKEM_OK)
+    rc = dpkem_enc_batch(c, DPKEM_FRODO976, g_compat_form, g_compat_batch, coins.data(), pk, ct, ss, 0, nullptr);
+  set_status(rc);
+}
+
+void frodoKEMDecap(uint8_t *ss, const uint8_t *ct, const uint8_t *sk) {
+  dpkem_ctx *c = compat_ctx();
+  if (!c) return (void)set_status(DPKEM_ECUDA);
+  set_status(dpkem_dec_batch(c, DPKEM_FRODO976, g_compat_form, g_compat_batch, ct, sk, ss, 0, nullptr));
+}
+
+void saber_enc(uint8_t mode, uint8_t *h_k, uint8_t *h_pk, uint8_t *h_c) {
+  dpkem_ctx *c = compat_ctx();
+  if (!c) return (void)set_status(DPKEM_ECUDA);
+  std::vector<uint8_t> coins(g_compat_batch * 32);
+  int rc = dpkem_coins(c, g_compat_batch, 32, 0, "enc", coins.data(), 0, nullptr);
+  if (rc == DPKEM_OK)
+    rc = dpkem_enc_batch(c, g_compat_level, compat_form_from_mode(mode), g_compat_batch, coins.data(), h_pk, h_c, h_k,
+                         0, nullptr);
+  set_status(rc);
+}
+
+void saber_dec(uint8_t mode, uint8_t *h_c, uint8_t *h_pk, uint8_t *h_sk, uint8_t *h_k) {
+  (void)h_pk;  // the public key travels inside sk
+  dpkem_ctx *c = compat_ctx();
+  if (!c) return (void)set_status(DPKEM_ECUDA);
+  set_status(dpkem_dec_batch(c, g_compat_level, compat_form_from_mode(mode), g_compat_batch, h_c, h_sk, h_k, 0, nullptr));
+}
+
+}  // extern "C"

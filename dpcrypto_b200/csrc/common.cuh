@@ -1,0 +1,83 @@
+// Shared definitions for the batched KEM kernels: scheme parameters, batch
+// descriptors and launcher prototypes.  Host code (abi.cu) fills the descriptors
+// with device pointers to caller data and to the context's scratch arena.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace dpkem {
+
+// ---- FrodoKEM-976-SHAKE (FrodoKEM976-GPU/include/params.h:9-25, api.h:7-10) ----
+namespace frodo {
+constexpr int N = 976, NBAR = 8, SEEDA = 16, LENS = 24, LENSE = 24, LENMU = 24, LENPKH = 24;
+constexpr int PK = 15632, SK = 31296, CT = 15744, SS = 24, KP_COINS = 64, ENC_COINS = 24;
+constexpr int PKB = N * NBAR * 2;               // packed B / B' bytes (15616)
+constexpr int RW = (2 * N + NBAR) * NBAR;       // sampled words per instance (15680)
+constexpr int SK_S = LENS + PK;                 // offset of S^T in sk (15656)
+constexpr int SK_PKH = SK_S + PKB;              // offset of H(pk) in sk (31272)
+constexpr int ROWS_PAD = 992;                   // 31 chunks of 32 rows
+}  // namespace frodo
+
+// ---- Saber (SABER-GPU/include/params.h:4-48) ----
+namespace saber {
+constexpr int N = 256, EQ = 13, EP = 10;
+struct Params {
+  int l, mu, et;
+  int polyvec, polyveccomp, pk, sk, ct, coins_poly;
+};
+__host__ __device__ constexpr Params params(int level) {
+  const int l = level, mu = level == 2 ? 10 : level == 3 ? 8 : 6, et = level == 2 ? 3 : level == 3 ? 4 : 6;
+  const int polyvec = l * EQ * N / 8, polyveccomp = l * EP * N / 8;
+  const int pk = polyveccomp + 32;
+  return Params{l, mu, et, polyvec, polyveccomp, pk, polyvec + pk + 64, polyveccomp + et * N / 8, mu * N / 8};
+}
+}  // namespace saber
+
+enum Op : int { OP_KEYPAIR = 0, OP_ENC = 1, OP_DEC = 2 };
+enum Form : int { FORM_DP4A = 0, FORM_INT32 = 1, FORM_TC = 2 };
+
+struct FrodoBatch {
+  int n;
+  const uint8_t *coins;  // keypair [n][64] = s||seedSE||z; enc [n][24] = mu
+  uint8_t *pk;           // [n][15632]
+  uint8_t *sk;           // [n][31296]
+  uint8_t *ct;           // [n][15744]
+  uint8_t *ss;           // [n][24]
+  uint16_t *rw;          // scratch [n][15680]: sampled S'|E'|E'' (keypair: S^T|E)
+  uint8_t *kk;           // scratch [n][24]: k (enc) or k' (dec)
+  uint8_t *mu;           // scratch [n][24]: decoded mu' (dec)
+  uint32_t *fail;        // scratch [n]: nonzero when the re-encryption differs (dec)
+  uint32_t *err;         // device error word (DEV_ERR_*)
+};
+
+struct SaberBatch {
+  int n, level;
+  const uint8_t *coins;  // keypair [n][96] = seedA||seed_s||z; enc [n][32]
+  uint8_t *pk, *sk, *ct, *ss;
+  uint8_t *scr;          // scratch [n][saber_scratch_bytes(level)]: XOF bytes, kr, m
+  uint32_t *fail;        // scratch [n]
+  uint32_t *err;         // device error word (DEV_ERR_*)
+};
+
+struct CoinsBatch {
+  int n;
+  int len;               // bytes per instance, <= 136
+  uint64_t first;        // index of the first instance
+  uint8_t tag[16];
+  int taglen;
+  uint8_t *out;          // [n][len]
+};
+
+cudaError_t frodo_keypair(const FrodoBatch &b, int form, cudaStream_t st);
+cudaError_t frodo_enc(const FrodoBatch &b, int form, cudaStream_t st);
+cudaError_t frodo_dec(const FrodoBatch &b, int form, cudaStream_t st);
+
+cudaError_t saber_keypair(const SaberBatch &b, int form, cudaStream_t st);
+cudaError_t saber_enc(const SaberBatch &b, int form, cudaStream_t st);
+cudaError_t saber_dec(const SaberBatch &b, int form, cudaStream_t st);
+size_t saber_scratch_bytes(int level);
+cudaError_t coins_generate(const CoinsBatch &b, cudaStream_t st);
+
+}  // namespace dpkem

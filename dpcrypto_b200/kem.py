@@ -1,0 +1,245 @@
+"""Host-side mirror of the reference's batched KEM interface over libdpkem.so.
+
+The reference exposes batched host functions (FrodoKEM976-GPU/include/cuda_kernel.cuh:7-9,
+SABER-GPU/include/cuda_kernel.cuh:6-7).  This module binds the C ABI with ctypes:
+
+* ``Engine`` wraps one ``dpkem_ctx`` and runs keypair / enc / dec over n instances.
+  numpy uint8 arrays run in host-pointer mode (copy in, compute, copy out); torch
+  CUDA uint8 tensors run in device-pointer mode on the current torch stream.
+* ``frodoKEMKeypair`` / ``frodoKEMEncap`` / ``frodoKEMDecap`` / ``saber_enc`` /
+  ``saber_dec`` call the reference-named C shims with numpy buffers.
+
+There is no CPU fallback: if the library or a CUDA device is missing, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdpkem.so")
+
+FRODO976, LIGHTSABER, SABER, FIRESABER = 0, 2, 3, 4
+SCHEMES = (FRODO976, LIGHTSABER, SABER, FIRESABER)
+FORM_DP4A, FORM_INT32, FORM_TC = 0, 1, 2
+FLAG_DEVICE_PTRS = 1
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, EUNSUPPORTED = 0, -1, -2, -3, -4, -5
+
+EXPORTS = {
+    "dpkem_ctx_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_size_t]),
+    "dpkem_ctx_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dpkem_sizes": (ctypes.c_int, [ctypes.c_int] + [ctypes.POINTER(ctypes.c_size_t)] * 6),
+    "dpkem_max_chunk": (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int]),
+    "dpkem_keypair_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_size_t,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint,
+                                           ctypes.c_void_p]),
+    "dpkem_enc_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_size_t,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_uint, ctypes.c_void_p]),
+    "dpkem_dec_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_size_t,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint,
+                                       ctypes.c_void_p]),
+    "dpkem_coins": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_uint64,
+                                   ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]),
+    "dpkem_sync": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "dpkem_strerror": (ctypes.c_char_p, [ctypes.c_int]),
+    "dpkem_last_status": (ctypes.c_int, []),
+    "dpkem_set_compat_batch": (None, [ctypes.c_size_t]),
+    "dpkem_set_compat_saber_level": (None, [ctypes.c_int]),
+    "dpkem_set_compat_form": (None, [ctypes.c_int]),
+    "frodoKEMKeypair": (None, [ctypes.c_void_p, ctypes.c_void_p]),
+    "frodoKEMEncap": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "frodoKEMDecap": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "saber_enc": (None, [ctypes.c_uint8, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "saber_dec": (None, [ctypes.c_uint8, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+}
+
+_lib = None
+
+
+class DpkemError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        msg = load().dpkem_strerror(status).decode() if _lib is not None else str(status)
+        super().__init__(f"{what}: {msg} ({status})" if what else f"{msg} ({status})")
+
+
+def load() -> ctypes.CDLL:
+    """Load libdpkem.so (built by dpcrypto_b200.build); raise if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m dpcrypto_b200.build`")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in EXPORTS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def sizes(scheme: int) -> dict:
+    vals = [ctypes.c_size_t() for _ in range(6)]
+    rc = load().dpkem_sizes(scheme, *[ctypes.byref(v) for v in vals])
+    if rc != OK:
+        raise DpkemError(rc, f"dpkem_sizes({scheme})")
+    return dict(zip(("pk", "sk", "ct", "ss", "kp_coins", "enc_coins"), (v.value for v in vals)))
+
+
+def _is_torch_cuda(x) -> bool:
+    return hasattr(x, "is_cuda") and x.is_cuda
+
+
+def _ptr(x):
+    if _is_torch_cuda(x):
+        return ctypes.c_void_p(x.data_ptr())
+    assert isinstance(x, np.ndarray) and x.dtype == np.uint8 and x.flags["C_CONTIGUOUS"], "uint8 C-contiguous array"
+    return ctypes.c_void_p(x.ctypes.data)
+
+
+class Engine:
+    """One dpkem context (device scratch arena + stream) on a CUDA device."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self._lib = load()
+        h = ctypes.c_void_p()
+        rc = self._lib.dpkem_ctx_create(ctypes.byref(h), device, hbm_budget)
+        if rc != OK:
+            raise DpkemError(rc, "dpkem_ctx_create (is a CUDA device visible?)")
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.dpkem_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- helpers ---------------------------------------------------------------
+    def _alloc(self, like, n: int, size: int):
+        if _is_torch_cuda(like):
+            import torch
+
+            return torch.empty((n, size), dtype=torch.uint8, device=like.device)
+        return np.empty((n, size), dtype=np.uint8)
+
+    def _mode(self, *arrs):
+        dev = [_is_torch_cuda(a) for a in arrs]
+        if any(dev) and not all(dev):
+            raise ValueError("mix of host and device buffers")
+        if all(dev):
+            import torch
+
+            return FLAG_DEVICE_PTRS, ctypes.c_void_p(torch.cuda.current_stream(arrs[0].device).cuda_stream)
+        return 0, None
+
+    @staticmethod
+    def _rows(x, size: int, what: str) -> int:
+        shape = tuple(x.shape)
+        if len(shape) != 2 or shape[1] != size:
+            raise ValueError(f"{what}: expected shape (n, {size}), got {shape}")
+        return shape[0]
+
+    def _check(self, rc: int, what: str):
+        if rc != OK:
+            raise DpkemError(rc, what)
+
+    # -- operations ------------------------------------------------------------
+    def keypair(self, scheme: int, coins, form: int = FORM_TC, out=None):
+        z = sizes(scheme)
+        n = self._rows(coins, z["kp_coins"], "coins")
+        pk, sk = out if out is not None else (self._alloc(coins, n, z["pk"]), self._alloc(coins, n, z["sk"]))
+        flags, st = self._mode(coins, pk, sk)
+        self._check(self._lib.dpkem_keypair_batch(self._h, scheme, form, n, _ptr(coins), _ptr(pk), _ptr(sk), flags,
+                                                  st), "keypair")
+        return pk, sk
+
+    def enc(self, scheme: int, pk, coins, form: int = FORM_TC, out=None):
+        z = sizes(scheme)
+        n = self._rows(pk, z["pk"], "pk")
+        if self._rows(coins, z["enc_coins"], "coins") != n:
+            raise ValueError("pk and coins batch sizes differ")
+        ct, ss = out if out is not None else (self._alloc(pk, n, z["ct"]), self._alloc(pk, n, z["ss"]))
+        flags, st = self._mode(pk, coins, ct, ss)
+        self._check(self._lib.dpkem_enc_batch(self._h, scheme, form, n, _ptr(coins), _ptr(pk), _ptr(ct), _ptr(ss),
+                                              flags, st), "enc")
+        return ct, ss
+
+    def dec(self, scheme: int, ct, sk, form: int = FORM_TC, out=None):
+        z = sizes(scheme)
+        n = self._rows(ct, z["ct"], "ct")
+        if self._rows(sk, z["sk"], "sk") != n:
+            raise ValueError("ct and sk batch sizes differ")
+        ss = out if out is not None else self._alloc(ct, n, z["ss"])
+        flags, st = self._mode(ct, sk, ss)
+        self._check(self._lib.dpkem_dec_batch(self._h, scheme, form, n, _ptr(ct), _ptr(sk), _ptr(ss), flags, st),
+                    "dec")
+        return ss
+
+    def coins(self, n: int, length: int, tag: str, first: int = 0, out=None):
+        out = out if out is not None else np.empty((n, length), np.uint8)
+        flags, st = self._mode(out)
+        self._check(self._lib.dpkem_coins(self._h, n, length, first, tag.encode(), _ptr(out), flags, st), "coins")
+        return out
+
+    def sync(self, stream=None):
+        self._check(self._lib.dpkem_sync(self._h, stream), "sync")
+
+    def max_chunk(self, scheme: int) -> int:
+        return int(self._lib.dpkem_max_chunk(self._h, scheme))
+
+
+# ---- reference-named entry points (batch from set_compat_batch, default 768) ----
+def set_compat(batch: int | None = None, saber_level: int | None = None, form: int | None = None):
+    lib = load()
+    if batch is not None:
+        lib.dpkem_set_compat_batch(batch)
+    if saber_level is not None:
+        lib.dpkem_set_compat_saber_level(saber_level)
+    if form is not None:
+        lib.dpkem_set_compat_form(form)
+
+
+def _last(what: str):
+    rc = load().dpkem_last_status()
+    if rc != OK:
+        raise DpkemError(rc, what)
+
+
+def frodoKEMKeypair(h_pk: np.ndarray, h_sk: np.ndarray) -> None:
+    load().frodoKEMKeypair(_ptr(h_pk), _ptr(h_sk))
+    _last("frodoKEMKeypair")
+
+
+def frodoKEMEncap(ct: np.ndarray, ss: np.ndarray, pk: np.ndarray) -> None:
+    load().frodoKEMEncap(_ptr(ct), _ptr(ss), _ptr(pk))
+    _last("frodoKEMEncap")
+
+
+def frodoKEMDecap(ss: np.ndarray, ct: np.ndarray, sk: np.ndarray) -> None:
+    load().frodoKEMDecap(_ptr(ss), _ptr(ct), _ptr(sk))
+    _last("frodoKEMDecap")
+
+
+def saber_enc(mode: int, h_k: np.ndarray, h_pk: np.ndarray, h_c: np.ndarray) -> None:
+    load().saber_enc(mode, _ptr(h_k), _ptr(h_pk), _ptr(h_c))
+    _last("saber_enc")
+
+
+def saber_dec(mode: int, h_c: np.ndarray, h_pk: np.ndarray, h_sk: np.ndarray, h_k: np.ndarray) -> None:
+    load().saber_dec(mode, _ptr(h_c), _ptr(h_pk), _ptr(h_sk), _ptr(h_k))
+    _last("saber_dec")

@@ -1,0 +1,108 @@
+/*
+ * dpkem: batched FrodoKEM-976-SHAKE and Saber (LightSaber / Saber / FireSaber) KEM
+ * engine for NVIDIA B200 (sm_100a).  C ABI of libdpkem.so.
+ *
+ * Drop-in boundary for the reference (benlwk/DPCrypto) batched entry points:
+ *   - frodoKEMKeypair / frodoKEMEncap / frodoKEMDecap replace
+ *     FrodoKEM976-GPU/include/cuda_kernel.cuh:7-9 (batch = compile-time BLOCK there,
+ *     dpkem_set_compat_batch() here);
+ *   - saber_enc / saber_dec replace SABER-GPU/include/cuda_kernel.cuh:6-7
+ *     (mode 0 = DP / dp4a form, 1 = INT32 in the reference; here 1 is unsupported and
+ *     2 selects the int8 tensor-core form).
+ *   - dpkem_{keypair,enc,dec}_batch are the batched form of the PQClean-style API the
+ *     reference's headers declare (FrodoKEM976-GPU/include/api.h:14-18), with explicit
+ *     coins so every call is reproducible.
+ * Byte layouts are the reference's: arrays of n contiguous instances, stride = object size.
+ *   Frodo-976: pk 15632 = seedA(16) || BE16(B); sk 31296 = s || pk || LE16(S^T) || H(pk);
+ *              ct 15744 = BE16(B') || BE16(C); ss 24          (FrodoKEM976-GPU/include/api.h:7-10)
+ *   Saber l:   pk 320l+32, sk 416l + pk + 64, ct 320l + eT*32, ss 32 (SABER-GPU/include/params.h:27-48)
+ * Coins: Frodo keypair 64 B = s || seedSE || z, Frodo enc 24 B = mu;
+ *        Saber keypair 96 B = seed_A || seed_s || z, Saber enc 32 B.
+ */
+#ifndef DPKEM_H
+#define DPKEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* Status codes (the reference returns void and checks no CUDA error). */
+enum {
+  DPKEM_OK = 0,
+  DPKEM_EINVAL = -1,       /* bad scheme/form/size/pointer/alignment */
+  DPKEM_ENOMEM = -2,       /* allocation failed or the request exceeds the HBM budget */
+  DPKEM_ECUDA = -3,        /* a CUDA runtime call failed */
+  DPKEM_ETIMEOUT = -4,     /* a bounded device wait expired (the kernel unwound) */
+  DPKEM_EUNSUPPORTED = -5  /* valid request this build does not implement */
+};
+
+/* Schemes: the value of a Saber scheme is its module rank l. */
+enum { DPKEM_FRODO976 = 0, DPKEM_LIGHTSABER = 2, DPKEM_SABER = 3, DPKEM_FIRESABER = 4 };
+
+/* Product forms. */
+enum { DPKEM_FORM_DP4A = 0, DPKEM_FORM_INT32 = 1, DPKEM_FORM_TC = 2 };
+
+/* Flags. */
+#define DPKEM_FLAG_DEVICE_PTRS 1u /* all buffers are device pointers (8-byte aligned); call is async */
+
+typedef struct dpkem_ctx dpkem_ctx;
+
+/* Create a context on `device` whose scratch arena may use at most `hbm_budget_bytes`
+ * (0 = default 8 GiB).  Batches larger than the budget allows run in chunks. */
+int dpkem_ctx_create(dpkem_ctx **out, int device, size_t hbm_budget_bytes);
+int dpkem_ctx_destroy(dpkem_ctx *ctx);
+
+/* Object sizes in bytes; any pointer may be NULL. */
+int dpkem_sizes(int scheme, size_t *pk, size_t *sk, size_t *ct, size_t *ss, size_t *kp_coins, size_t *enc_coins);
+
+/* Largest batch one launch chain processes under the context's budget (host-pointer mode). */
+size_t dpkem_max_chunk(dpkem_ctx *ctx, int scheme);
+
+/* Batched operations.  `stream` is a cudaStream_t (NULL = the context's stream).
+ * Host-pointer mode (flags 0): copies in, computes, copies out, returns when done.
+ * Device-pointer mode: enqueues on `stream` and returns; call dpkem_sync() for the
+ * device error word.  Decaps failure is not an error (implicit rejection). */
+int dpkem_keypair_batch(dpkem_ctx *ctx, int scheme, int form, size_t n, const uint8_t *coins, uint8_t *pk,
+                        uint8_t *sk, unsigned flags, void *stream);
+int dpkem_enc_batch(dpkem_ctx *ctx, int scheme, int form, size_t n, const uint8_t *coins, const uint8_t *pk,
+                    uint8_t *ct, uint8_t *ss, unsigned flags, void *stream);
+int dpkem_dec_batch(dpkem_ctx *ctx, int scheme, int form, size_t n, const uint8_t *ct, const uint8_t *sk,
+                    uint8_t *ss, unsigned flags, void *stream);
+
+/* Seeded synthetic coins: out[i] = SHAKE256(00 01 .. 1F || LE64(first + i) || tag, len), len <= 136,
+ * strlen(tag) <= 16.  Same flag semantics as the batched operations. */
+int dpkem_coins(dpkem_ctx *ctx, size_t n, size_t len, uint64_t first, const char *tag, uint8_t *out,
+                unsigned flags, void *stream);
+
+/* Wait for `stream` (NULL = context stream) and report a device-side timeout, if any. */
+int dpkem_sync(dpkem_ctx *ctx, void *stream);
+
+const char *dpkem_strerror(int status);
+/* Status of the last call made by this thread (the compatibility shims return void). */
+int dpkem_last_status(void);
+
+/* ---- Reference-compatible shims (process-wide default context on device 0) ---- */
+void dpkem_set_compat_batch(size_t n);     /* default 768, the reference's BLOCK / BATCH */
+void dpkem_set_compat_saber_level(int l);  /* default 3, the reference's SABER_L */
+void dpkem_set_compat_form(int form);      /* default DPKEM_FORM_TC */
+/* Keypair coins come from dpkem_coins(i, "kp"), encaps coins from dpkem_coins(i, "enc"). */
+void frodoKEMKeypair(uint8_t *h_pk, uint8_t *h_sk);
+void frodoKEMEncap(uint8_t *ct, uint8_t *ss, const uint8_t *pk);
+void frodoKEMDecap(uint8_t *ss, const uint8_t *ct, const uint8_t *sk);
+/* Reference: keys from tv.h, overwriting h_pk / h_sk.  Here caller data is used as given. */
+void saber_enc(uint8_t mode, uint8_t *h_k, uint8_t *h_pk, uint8_t *h_c);
+void saber_dec(uint8_t mode, uint8_t *h_c, uint8_t *h_pk, uint8_t *h_sk, uint8_t *h_k);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif

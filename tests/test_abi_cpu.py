@@ -1,0 +1,59 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol the header
+declares, reports sizes, and fails loudly (no CPU fallback) without a device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    text = open(os.path.join(ROOT, "include", "dpkem.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*([A-Za-z_][A-Za-z_0-9]*)\s*\(", text, flags=re.M))
+    return {n for n in names if n not in ("if", "defined")}
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from dpcrypto_b200 import build
+
+    path = build.build()
+    return ctypes.CDLL(path)
+
+
+def test_exports_every_declared_symbol(lib):
+    names = _declared()
+    assert len(names) >= 19
+    for n in sorted(names):
+        assert hasattr(lib, n), n
+
+
+def test_binding_covers_header():
+    from dpcrypto_b200 import EXPORTS
+
+    assert _declared() == set(EXPORTS)
+
+
+def test_sizes():
+    import dpcrypto_b200 as d
+
+    assert d.sizes(0) == dict(pk=15632, sk=31296, ct=15744, ss=24, kp_coins=64, enc_coins=24)
+    assert (d.sizes(2)["pk"], d.sizes(2)["sk"], d.sizes(2)["ct"]) == (672, 1568, 736)
+    assert (d.sizes(3)["pk"], d.sizes(3)["sk"], d.sizes(3)["ct"]) == (992, 2304, 1088)
+    assert (d.sizes(4)["pk"], d.sizes(4)["sk"], d.sizes(4)["ct"]) == (1312, 3040, 1472)
+    with pytest.raises(d.DpkemError):
+        d.sizes(1)
+
+
+def test_no_silent_fallback_without_device():
+    import torch
+
+    import dpcrypto_b200 as d
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(d.DpkemError):
+        d.Engine(0)

@@ -1,0 +1,94 @@
+"""C-ABI behaviour on the GPU: status codes, device-pointer mode, chunking under a small
+HBM budget, device coin stream, and the reference-named shims."""
+import numpy as np
+import pytest
+import torch
+
+import dpcrypto_b200 as d
+
+pytestmark = pytest.mark.gpu
+
+
+def test_status_codes(engine, oracle):
+    kc = oracle.coins(2, 96, "kp")
+    with pytest.raises(d.DpkemError) as e:
+        engine.keypair(d.SABER, kc, d.FORM_INT32)
+    assert e.value.status == d.kem.EUNSUPPORTED
+    with pytest.raises(d.DpkemError) as e:
+        engine.keypair(7, kc, d.FORM_TC)
+    assert e.value.status == d.kem.EINVAL
+    with pytest.raises(ValueError):
+        engine.keypair(d.SABER, kc[:, :95].copy(), d.FORM_TC)
+    empty = np.zeros((0, 96), np.uint8)
+    pk, sk = engine.keypair(d.SABER, empty, d.FORM_TC)
+    assert pk.shape == (0, 992) and sk.shape == (0, 2304)
+
+
+def test_device_coins_match_oracle(engine, oracle):
+    for length, tag in ((64, "kp"), (24, "enc"), (96, "kp"), (32, "enc"), (5, "x")):
+        host = engine.coins(37, length, tag, first=3)
+        assert (host == oracle.coins(37, length, tag, first=3)).all()
+        dev = torch.empty((37, length), dtype=torch.uint8, device="cuda")
+        engine.coins(37, length, tag, first=3, out=dev)
+        torch.cuda.synchronize()
+        assert (dev.cpu().numpy() == host).all()
+
+
+@pytest.mark.parametrize("scheme", [d.FRODO976, d.SABER])
+def test_device_pointer_mode(engine, oracle, scheme):
+    z = d.sizes(scheme)
+    n = 40
+    kc = torch.from_numpy(oracle.coins(n, z["kp_coins"], "kp")).cuda()
+    ec = torch.from_numpy(oracle.coins(n, z["enc_coins"], "enc")).cuda()
+    pk, sk = engine.keypair(scheme, kc, d.FORM_TC)
+    ct, ss = engine.enc(scheme, pk, ec, d.FORM_TC)
+    ss2 = engine.dec(scheme, ct, sk, d.FORM_TC)
+    engine.sync(ctypes_stream(torch.cuda.current_stream()))
+    assert torch.equal(ss, ss2)
+    pk_h, _ = engine.keypair(scheme, kc.cpu().numpy(), d.FORM_DP4A)
+    assert (pk.cpu().numpy() == pk_h).all()
+
+
+def ctypes_stream(s):
+    import ctypes
+
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+@pytest.mark.parametrize("scheme", [d.FRODO976, d.SABER])
+def test_chunking_under_small_budget(oracle, scheme):
+    z = d.sizes(scheme)
+    budget = (2 << 20) if scheme == d.FRODO976 else (256 << 10)
+    with d.Engine(0, hbm_budget=budget) as small:
+        assert small.max_chunk(scheme) < 40
+        n = 40
+        kc, ec = oracle.coins(n, z["kp_coins"], "kp"), oracle.coins(n, z["enc_coins"], "enc")
+        pk, sk = small.keypair(scheme, kc, d.FORM_TC)
+        ct, ss = small.enc(scheme, pk, ec, d.FORM_TC)
+        assert (small.dec(scheme, ct, sk, d.FORM_TC) == ss).all()
+    with d.Engine(0) as big:
+        pk2, _ = big.keypair(scheme, kc, d.FORM_TC)
+        assert (pk2 == pk).all()
+
+
+def test_reference_named_shims(oracle):
+    n = 4
+    d.set_compat(batch=n, saber_level=3, form=d.FORM_TC)
+    pk, sk = np.zeros((n, 15632), np.uint8), np.zeros((n, 31296), np.uint8)
+    d.frodoKEMKeypair(pk, sk)
+    pk_o, sk_o = oracle.keypair(0, oracle.coins(n, 64, "kp"), threads=4)
+    assert (pk == pk_o).all() and (sk == sk_o).all()
+    ct, ssb, ssa = np.zeros((n, 15744), np.uint8), np.zeros((n, 24), np.uint8), np.zeros((n, 24), np.uint8)
+    d.frodoKEMEncap(ct, ssb, pk)
+    d.frodoKEMDecap(ssa, ct, sk)
+    assert (ssa == ssb).all()
+    spk, ssk = oracle.keypair(3, oracle.coins(n, 96, "kp"), threads=4)
+    k_enc, c = np.zeros((n, 32), np.uint8), np.zeros((n, 1088), np.uint8)
+    for mode in (0, 2):
+        d.saber_enc(mode, k_enc, spk, c)
+        k_dec = np.zeros((n, 32), np.uint8)
+        d.saber_dec(mode, c, spk, ssk, k_dec)
+        assert (k_dec == k_enc).all()
+    with pytest.raises(d.DpkemError):
+        d.saber_enc(1, k_enc, spk, c)
+    d.set_compat(batch=768)
