@@ -1,0 +1,377 @@
+#!/usr/bin/env python3
+"""Benchmark: FrodoKEM-976-SHAKE encaps+decaps per second at batch 8192 per GPU.
+
+One step = encaps of the batch followed by decaps of the resulting ciphertexts
+(independent keypairs per instance, generated once before timing).  The headline
+form is the int8 tcgen05 product; the dp4a form and Saber (l=3, batch 4096) are
+measured on the same GPU and reported beside it.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU (torchrun, one rank per GPU): every rank runs its own batch (weak scaling,
+no data-path collective); value = instances of all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "KEM encaps+decaps/sec at batch 8192 (int8 TC vs dp4a, bit-exact); p99 latency"
+UNIT = "encaps+decaps/s"
+# 32-bit LOP3/SHF operations of one Keccak-f[1600] in its minimal form: per round theta
+# 20 (column parities) + 10 (rot1) + 50 (3-input XOR into the lanes), rho 48, chi 50,
+# iota 2 = 180; x 24 rounds.
+KECCAK_INT_OPS = 4320
+FRODO_ROWS, FRODO_BLOCKS = 976, 12      # A rows per instance, SHAKE128 blocks per row
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "frodo_sa_tc_traffic.json")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--batch", type=int, default=8192)
+    p.add_argument("--form", default="tc", choices=["tc", "dp4a"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-secondary", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def config(args, world):
+    return {
+        "workload": f"FrodoKEM-976-SHAKE encaps+decaps, batch {args.batch} per GPU, {args.form} product form",
+        "scheme": "FrodoKEM-976-SHAKE", "batch_per_gpu": args.batch, "global_batch": args.batch * world,
+        "form": args.form, "parallelism": f"instances sharded, {world} replica(s)",
+        "l2": "inputs larger than L2 (pk+sk+ct per step = %d MB per GPU)" % (args.batch * (15632 + 31296 + 15744) >> 20),
+    }
+
+
+# ---------------------------------------------------------------- CPU (oracle) arms
+def cpu_sample(n_inst: int, threads: int):
+    """Time the oracle's encaps+decaps on n_inst instances over `threads` host threads."""
+    from oracle import oracle as O
+
+    pk, sk = O.keypair(0, O.coins(n_inst, 64, "kp"), threads=threads)
+    ec = O.coins(n_inst, 24, "enc")
+    t0 = time.perf_counter()
+    ct, ss = O.enc(0, pk, ec, threads=threads)
+    ss2 = O.dec(0, ct, sk, threads=threads)
+    dt = time.perf_counter() - t0
+    assert (ss == ss2).all()
+    return n_inst / dt, dt
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+
+    O.build()
+    threads = os.cpu_count() or 1
+    per_step = 2 * threads
+    for _ in range(args.warmup):
+        cpu_sample(per_step, threads)
+    times = []
+    for _ in range(args.steps):
+        _, dt = cpu_sample(per_step, threads)
+        times.append(dt)
+    total = sum(times)
+    value = per_step * args.steps / total
+    sample = f"{per_step} FrodoKEM-976 encaps+decaps per step (2 per host thread), oracle C port, pthreads"
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64/u16 (CPU)",
+        "data": "synthetic (seeded SHAKE256 coins)", "config": config(args, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU helpers
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.rows.append(f)
+
+    def summary(self):
+        rows = getattr(self, "rows", [])
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1])]
+        smax = max((num(r[2]) for r in rows if num(r[2])), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows), "power_w_max": max((num(r[3]) or 0) for r in rows)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+
+    import numpy as np
+    import torch
+
+    import dpcrypto_b200 as d
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        pg = dist
+    eng = d.Engine(local)
+    form = d.FORM_TC if args.form == "tc" else d.FORM_DP4A
+    B = args.batch
+    stream = torch.cuda.current_stream()
+
+    # ---- inputs: keypairs and coins generated on the device, untimed ----
+    first = rank * B
+    kc = torch.empty((B, 64), dtype=torch.uint8, device="cuda")
+    ec = torch.empty((B, 24), dtype=torch.uint8, device="cuda")
+    eng.coins(B, 64, "kp", first=first, out=kc)
+    eng.coins(B, 24, "enc", first=first, out=ec)
+    pk, sk = eng.keypair(d.FRODO976, kc, d.FORM_TC)
+    ct = torch.empty((B, 15744), dtype=torch.uint8, device="cuda")
+    ss = torch.empty((B, 24), dtype=torch.uint8, device="cuda")
+    ss2 = torch.empty((B, 24), dtype=torch.uint8, device="cuda")
+
+    def step(f):
+        eng.enc(d.FRODO976, pk, ec, f, out=(ct, ss))
+        eng.dec(d.FRODO976, ct, sk, f, out=ss2)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+
+    def timed(f, steps, profile=False):
+        """Device time of `steps` steps on torch's stream (max over ranks) + per-stage times."""
+        stages = {"enc": [], "dec": []}
+        eng.profile(profile)
+        barrier()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(steps):
+            eng.enc(d.FRODO976, pk, ec, f, out=(ct, ss))
+            if profile:
+                stages["enc"].append(eng.stage_times())
+            eng.dec(d.FRODO976, ct, sk, f, out=ss2)
+            if profile:
+                stages["dec"].append(eng.stage_times())
+        t1.record(stream)
+        barrier()
+        eng.profile(False)
+        ms = t0.elapsed_time(t1)
+        if pg is not None:
+            x = torch.tensor([ms], device="cuda")
+            pg.all_reduce(x, op=pg.ReduceOp.MAX)
+            ms = float(x.item())
+        return ms, stages
+
+    for _ in range(args.warmup):
+        step(form)
+    barrier()
+    sampler = ClockSampler(local)
+    with sampler:
+        ms, stages = timed(form, args.steps, profile=True)
+    clocks = sampler.summary()
+    eng.sync()
+    ok = bool(torch.equal(ss, ss2))
+    value = world * B * args.steps / (ms * 1e-3)
+
+    # ---- roofline of the dominant kernel (the fused A-generation + S'A product) ----
+    sa_ms = [s[1] for s in stages["enc"]] + [s[2] for s in stages["dec"]]
+    sa_avg = statistics.mean(sa_ms)
+    ops_per_launch = B * FRODO_ROWS * FRODO_BLOCKS * KECCAK_INT_OPS
+    int_peak, keccak_peak = eng.probe_int_peaks()
+    achieved = ops_per_launch / (sa_avg * 1e-3) / 1e9
+    traffic = None
+    if os.path.exists(TRAFFIC_FILE):
+        with open(TRAFFIC_FILE) as f:
+            traffic = json.load(f)["dram_bytes_per_instance"] * B
+    stage_names = {"enc": ["prologue", "sa_product", "final_hash"], "dec": ["w_decode", "prologue", "sa_product",
+                                                                             "final_hash"]}
+    stage_ms = {op: dict(zip(stage_names[op], [statistics.mean(x) for x in zip(*stages[op])])) for op in stages}
+    kernel_total = sum(sum(v.values()) for v in stage_ms.values())
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8xs8->s32 (tcgen05 kind::i8), u64 Keccak lanes" if form == d.FORM_TC else "s16xs8->s32 (dp2a)",
+        "data": "synthetic (seeded SHAKE256 coins, keypairs generated on the GPU)", "config": config(args, world),
+        "bit_exact_roundtrip": ok, "gpu_launches": 7 * args.steps,
+        "roofline": {
+            "kernel": "sa_tc_kernel (SHAKE128 A rows in registers -> int8 tcgen05 S'A)" if form == d.FORM_TC
+            else "sa_dp4a_kernel", "bound": "int", "unit": "Gop/s",
+            "achieved": achieved, "peak": int_peak / 1e9, "frac": achieved * 1e9 / int_peak,
+            "peak_source": "measured in-process: LOP3/SHF issue rate in Keccak's mix (dpkem_probe_int_peaks)",
+            "algorithmic": f"{KECCAK_INT_OPS} int32 ops per Keccak-f x 12 per A row x 976 rows x batch",
+            "avg_launch_ms": sa_avg, "traffic": traffic,
+            "keccak_per_s": B * FRODO_ROWS * FRODO_BLOCKS / (sa_avg * 1e-3),
+            "keccak_peak_per_s": keccak_peak,
+        },
+        "stage_ms": stage_ms, "stage_share_of_step": {k: sum(v.values()) / kernel_total for k, v in stage_ms.items()},
+        "clocks": clocks,
+    }
+
+    # ---- comparison form (dp4a vs tc) on the same GPU ----
+    if not args.no_secondary:
+        other = d.FORM_DP4A if form == d.FORM_TC else d.FORM_TC
+        for _ in range(2):
+            step(other)
+        oms, ostages = timed(other, max(3, args.steps // 2), profile=True)
+        ovalue = world * B * max(3, args.steps // 2) / (oms * 1e-3)
+        o_sa = statistics.mean([s[1] for s in ostages["enc"]] + [s[2] for s in ostages["dec"]])
+        line["forms"] = {
+            "tc": value if form == d.FORM_TC else ovalue, "dp4a": ovalue if form == d.FORM_TC else value,
+            "sa_kernel_ms": {"tc": sa_avg if form == d.FORM_TC else o_sa, "dp4a": o_sa if form == d.FORM_TC else sa_avg},
+        }
+        line["forms"]["tc_over_dp4a"] = line["forms"]["tc"] / line["forms"]["dp4a"]
+        line["forms"]["product_stage_tc_over_dp4a"] = line["forms"]["sa_kernel_ms"]["dp4a"] / line["forms"]["sa_kernel_ms"]["tc"]
+        # Saber l=3, batch 4096 (configs' second workload)
+        SB = 4096
+        skc = torch.empty((SB, 96), dtype=torch.uint8, device="cuda")
+        sec = torch.empty((SB, 32), dtype=torch.uint8, device="cuda")
+        eng.coins(SB, 96, "kp", first=first, out=skc)
+        eng.coins(SB, 32, "enc", first=first, out=sec)
+        spk, ssk = eng.keypair(d.SABER, skc, d.FORM_TC)
+        sct = torch.empty((SB, 1088), dtype=torch.uint8, device="cuda")
+        sss = torch.empty((SB, 32), dtype=torch.uint8, device="cuda")
+        sss2 = torch.empty((SB, 32), dtype=torch.uint8, device="cuda")
+        sres = {}
+        for name, f in (("tc", d.FORM_TC), ("dp4a", d.FORM_DP4A)):
+            for _ in range(3):
+                eng.enc(d.SABER, spk, sec, f, out=(sct, sss))
+                eng.dec(d.SABER, sct, ssk, f, out=sss2)
+            barrier()
+            reps = 50
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for _ in range(reps):
+                eng.enc(d.SABER, spk, sec, f, out=(sct, sss))
+                eng.dec(d.SABER, sct, ssk, f, out=sss2)
+            t1.record(stream)
+            barrier()
+            sres[name] = SB * reps / (t0.elapsed_time(t1) * 1e-3)
+            sres[name + "_roundtrip_ok"] = bool(torch.equal(sss, sss2))
+        sres["tc_over_dp4a"] = sres["tc"] / sres["dp4a"]
+        line["saber_l3_batch4096"] = dict(sres, unit=UNIT)
+
+    # ---- end to end through the public API with pinned host buffers ----
+    if not args.no_e2e:
+        pin = lambda t: t.cpu().pin_memory().numpy()  # noqa: E731
+        h_pk, h_sk, h_ec = pin(pk), pin(sk), pin(ec)
+        h_ct = torch.empty((B, 15744), dtype=torch.uint8).pin_memory().numpy()
+        h_ss = torch.empty((B, 24), dtype=torch.uint8).pin_memory().numpy()
+        h_ss2 = torch.empty((B, 24), dtype=torch.uint8).pin_memory().numpy()
+        for _ in range(max(1, args.warmup)):
+            eng.enc(d.FRODO976, h_pk, h_ec, form, out=(h_ct, h_ss))
+            eng.dec(d.FRODO976, h_ct, h_sk, form, out=h_ss2)
+        barrier()
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            eng.enc(d.FRODO976, h_pk, h_ec, form, out=(h_ct, h_ss))
+            eng.dec(d.FRODO976, h_ct, h_sk, form, out=h_ss2)
+        el = time.perf_counter() - t
+        if pg is not None:
+            x = torch.tensor([el], device="cuda", dtype=torch.float64)
+            pg.all_reduce(x, op=pg.ReduceOp.MAX)
+            el = float(x.item())
+        line["e2e"] = {"value": world * B * args.steps / el, "unit": UNIT,
+                       "h2d_bytes_per_step": B * (15632 + 24 + 15744 + 31296),
+                       "d2h_bytes_per_step": B * (15744 + 24 + 24),
+                       "roundtrip_ok": bool((h_ss == h_ss2).all())}
+
+    # ---- CPU baseline: the oracle on the host cores, rank 0 at N=1 ----
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        n_inst = 4 * threads
+        cv, dt = cpu_sample(n_inst, threads)
+        line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{n_inst} FrodoKEM-976 encaps+decaps (4 per host thread), "
+                                          f"oracle C restatement, {dt:.1f} s wall",
+                                "note": "reported baseline, not the target"}
+
+    peaks, src = measured_peaks()
+    line["peaks_file"] = src
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    eng.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

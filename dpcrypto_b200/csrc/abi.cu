@@ -28,6 +28,9 @@ struct dpkem_ctx {
   uint8_t *arena = nullptr;
   size_t arena_bytes = 0;
   uint32_t *d_err = nullptr;
+  bool profile = false;
+  StageTimer timer;
+  int timer_stages = 0;
   std::mutex mu;
 };
 
@@ -202,6 +205,13 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
       d_in0 = a;
       d_in1 = b;
     }
+    StageTimer *tm = nullptr;
+    if (c->profile) {
+      c->timer.n = 0;
+      tm = &c->timer;
+    }
+    fb.timer = tm;
+    sb.timer = tm;
     if (scheme == DPKEM_FRODO976) {
       fb.n = (int)m;
       fb.err = c->d_err;
@@ -239,6 +249,7 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
       }
     }
     if (e != cudaSuccess) return cuda_status(e);
+    if (tm) c->timer_stages = tm->n - 1;
     if (!dev) {
       if ((e = cudaMemcpyAsync(out0 + first * out0_sz, d_out0, m * out0_sz, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return cuda_status(e);
@@ -279,6 +290,7 @@ int dpkem_ctx_create(dpkem_ctx **out, int device, size_t hbm_budget_bytes) {
   dpkem_ctx *c = new dpkem_ctx();
   c->device = device;
   c->budget = hbm_budget_bytes ? hbm_budget_bytes : kDefaultBudget;
+  for (int k = 0; k <= StageTimer::kMax; k++) cudaEventCreate(&c->timer.ev[k]);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->last, cudaEventDisableTiming) != cudaSuccess ||
       cudaMalloc(&c->d_err, 4) != cudaSuccess || cudaMemset(c->d_err, 0, 4) != cudaSuccess) {
@@ -298,6 +310,8 @@ int dpkem_ctx_destroy(dpkem_ctx *c) {
   if (c->arena) cudaFree(c->arena);
   if (c->d_err) cudaFree(c->d_err);
   if (c->last) cudaEventDestroy(c->last);
+  for (int k = 0; k <= StageTimer::kMax; k++)
+    if (c->timer.ev[k]) cudaEventDestroy(c->timer.ev[k]);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return set_status(DPKEM_OK);
@@ -391,6 +405,34 @@ int dpkem_sync(dpkem_ctx *c, void *stream) {
     return set_status(DPKEM_ETIMEOUT);
   }
   return set_status(DPKEM_OK);
+}
+
+int dpkem_profile(dpkem_ctx *c, int enable) {
+  if (!c) return set_status(DPKEM_EINVAL);
+  std::lock_guard<std::mutex> lock(c->mu);
+  c->profile = enable != 0;
+  c->timer_stages = 0;
+  return set_status(DPKEM_OK);
+}
+
+int dpkem_profile_read(dpkem_ctx *c, float *stage_ms, int max_stages) {
+  if (!c || (!stage_ms && max_stages > 0)) return set_status(DPKEM_EINVAL);
+  std::lock_guard<std::mutex> lock(c->mu);
+  cudaSetDevice(c->device);
+  const int n = c->timer_stages;
+  if (n <= 0) return 0;
+  if (cudaEventSynchronize(c->timer.ev[n]) != cudaSuccess) return set_status(cuda_status(cudaErrorUnknown));
+  for (int k = 0; k < n && k < max_stages; k++)
+    if (cudaEventElapsedTime(&stage_ms[k], c->timer.ev[k], c->timer.ev[k + 1]) != cudaSuccess)
+      return set_status(cuda_status(cudaErrorUnknown));
+  return n;
+}
+
+int dpkem_probe_int_peaks(dpkem_ctx *c, double *int_ops_per_s, double *keccak_per_s) {
+  if (!c || !int_ops_per_s || !keccak_per_s) return set_status(DPKEM_EINVAL);
+  std::lock_guard<std::mutex> lock(c->mu);
+  cudaSetDevice(c->device);
+  return set_status(cuda_status(probe_int_peaks(c->stream, int_ops_per_s, keccak_per_s)));
 }
 
 const char *dpkem_strerror(int s) {

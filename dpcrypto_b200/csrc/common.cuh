@@ -36,6 +36,17 @@ __host__ __device__ constexpr Params params(int level) {
 }  // namespace saber
 
 enum Op : int { OP_KEYPAIR = 0, OP_ENC = 1, OP_DEC = 2 };
+
+// Optional per-stage timing: when non-null, a launcher records ev[k] on its stream
+// before its k-th stage and ev[nstages] after the last one.
+struct StageTimer {
+  static constexpr int kMax = 8;
+  cudaEvent_t ev[kMax + 1];
+  int n = 0;
+  void mark(cudaStream_t st) {
+    if (n <= kMax) cudaEventRecord(ev[n++], st);
+  }
+};
 enum Form : int { FORM_DP4A = 0, FORM_INT32 = 1, FORM_TC = 2 };
 
 struct FrodoBatch {
@@ -50,6 +61,7 @@ struct FrodoBatch {
   uint8_t *mu;           // scratch [n][24]: decoded mu' (dec)
   uint32_t *fail;        // scratch [n]: nonzero when the re-encryption differs (dec)
   uint32_t *err;         // device error word (DEV_ERR_*)
+  StageTimer *timer;     // optional
 };
 
 struct SaberBatch {
@@ -59,6 +71,7 @@ struct SaberBatch {
   uint8_t *scr;          // scratch [n][saber_scratch_bytes(level)]: XOF bytes, kr, m
   uint32_t *fail;        // scratch [n]
   uint32_t *err;         // device error word (DEV_ERR_*)
+  StageTimer *timer;     // optional
 };
 
 struct CoinsBatch {
@@ -79,5 +92,6 @@ cudaError_t saber_enc(const SaberBatch &b, int form, cudaStream_t st);
 cudaError_t saber_dec(const SaberBatch &b, int form, cudaStream_t st);
 size_t saber_scratch_bytes(int level);
 cudaError_t coins_generate(const CoinsBatch &b, cudaStream_t st);
+cudaError_t probe_int_peaks(cudaStream_t st, double *int_ops_per_s, double *keccak_per_s);
 
 }  // namespace dpkem

@@ -569,31 +569,48 @@ cudaError_t launch_sa(const FrodoBatch &b, int form, cudaStream_t st) {
 
 }  // namespace
 
+inline void mark(const FrodoBatch &b, cudaStream_t st) {
+  if (b.timer) b.timer->mark(st);
+}
+
 cudaError_t frodo_keypair(const FrodoBatch &b, int form, cudaStream_t st) {
   if (b.n <= 0) return cudaSuccess;
-  kp_prologue_kernel<<<blocks_for(b.n, 64), 64, 0, st>>>(b);
-  kp_as_dp4a_kernel<<<b.n, 256, 0, st>>>(b);
-  pk_hash_kernel<<<blocks_for(b.n, 64), 64, 0, st>>>(b);
   (void)form;
+  mark(b, st);
+  kp_prologue_kernel<<<blocks_for(b.n, 64), 64, 0, st>>>(b);
+  mark(b, st);
+  kp_as_dp4a_kernel<<<b.n, 256, 0, st>>>(b);
+  mark(b, st);
+  pk_hash_kernel<<<blocks_for(b.n, 64), 64, 0, st>>>(b);
+  mark(b, st);
   return cudaGetLastError();
 }
 
 cudaError_t frodo_enc(const FrodoBatch &b, int form, cudaStream_t st) {
   if (b.n <= 0) return cudaSuccess;
+  mark(b, st);
   prologue_kernel<OP_ENC><<<blocks_for(b.n, 64), 64, 0, st>>>(b);
+  mark(b, st);
   cudaError_t e = launch_sa<OP_ENC>(b, form, st);
   if (e != cudaSuccess) return e;
+  mark(b, st);
   ss_kernel<OP_ENC><<<blocks_for(b.n, 64), 64, 0, st>>>(b);
+  mark(b, st);
   return cudaGetLastError();
 }
 
 cudaError_t frodo_dec(const FrodoBatch &b, int form, cudaStream_t st) {
   if (b.n <= 0) return cudaSuccess;
+  mark(b, st);
   dec_w_kernel<<<b.n, 256, 0, st>>>(b);
+  mark(b, st);
   prologue_kernel<OP_DEC><<<blocks_for(b.n, 64), 64, 0, st>>>(b);
+  mark(b, st);
   cudaError_t e = launch_sa<OP_DEC>(b, form, st);
   if (e != cudaSuccess) return e;
+  mark(b, st);
   ss_kernel<OP_DEC><<<blocks_for(b.n, 64), 64, 0, st>>>(b);
+  mark(b, st);
   return cudaGetLastError();
 }
 

@@ -554,28 +554,41 @@ cudaError_t launch_product(const SaberBatch &b, int form, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+inline void mark(const SaberBatch &b, cudaStream_t st) {
+  if (b.timer) b.timer->mark(st);
+}
+
 template <int L>
 cudaError_t run(const SaberBatch &b, int op, int form, cudaStream_t st) {
   const int pb = (b.n + 31) / 32, fb = (b.n + 63) / 64;
   cudaError_t e;
+  mark(b, st);
   switch (op) {
     case OP_KEYPAIR:
       prologue_kernel<L, OP_KEYPAIR><<<pb, 64, 0, st>>>(b);
+      mark(b, st);
       if ((e = launch_product<L, PM_KEYPAIR>(b, form, st)) != cudaSuccess) return e;
+      mark(b, st);
       finish_kernel<L, OP_KEYPAIR><<<fb, 64, 0, st>>>(b);
       break;
     case OP_ENC:
       prologue_kernel<L, OP_ENC><<<pb, 64, 0, st>>>(b);
+      mark(b, st);
       if ((e = launch_product<L, PM_ENC>(b, form, st)) != cudaSuccess) return e;
+      mark(b, st);
       finish_kernel<L, OP_ENC><<<fb, 64, 0, st>>>(b);
       break;
     default:
       if ((e = launch_product<L, PM_DEC_INNER>(b, form, st)) != cudaSuccess) return e;
+      mark(b, st);
       prologue_kernel<L, OP_DEC><<<pb, 64, 0, st>>>(b);
+      mark(b, st);
       if ((e = launch_product<L, PM_DEC_CMP>(b, form, st)) != cudaSuccess) return e;
+      mark(b, st);
       finish_kernel<L, OP_DEC><<<fb, 64, 0, st>>>(b);
       break;
   }
+  mark(b, st);
   return cudaGetLastError();
 }
 

@@ -44,6 +44,10 @@ EXPORTS = {
     "dpkem_coins": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_uint64,
                                    ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]),
     "dpkem_sync": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "dpkem_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "dpkem_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
+    "dpkem_probe_int_peaks": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_double)]),
     "dpkem_strerror": (ctypes.c_char_p, [ctypes.c_int]),
     "dpkem_last_status": (ctypes.c_int, []),
     "dpkem_set_compat_batch": (None, [ctypes.c_size_t]),
@@ -198,6 +202,23 @@ class Engine:
 
     def sync(self, stream=None):
         self._check(self._lib.dpkem_sync(self._h, stream), "sync")
+
+    def profile(self, enable: bool = True):
+        self._check(self._lib.dpkem_profile(self._h, int(enable)), "profile")
+
+    def stage_times(self) -> list:
+        """Per-stage device times (ms) of the last batched call, when profiling is on."""
+        buf = (ctypes.c_float * 8)()
+        n = self._lib.dpkem_profile_read(self._h, buf, 8)
+        if n < 0:
+            raise DpkemError(n, "profile_read")
+        return [float(buf[k]) for k in range(n)]
+
+    def probe_int_peaks(self):
+        """(32-bit LOP3/SHF ops per second in Keccak's mix, Keccak-f[1600] per second)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self._lib.dpkem_probe_int_peaks(self._h, ctypes.byref(a), ctypes.byref(b)), "probe")
+        return a.value, b.value
 
     def max_chunk(self, scheme: int) -> int:
         return int(self._lib.dpkem_max_chunk(self._h, scheme))

@@ -83,6 +83,18 @@ int dpkem_coins(dpkem_ctx *ctx, size_t n, size_t len, uint64_t first, const char
 /* Wait for `stream` (NULL = context stream) and report a device-side timeout, if any. */
 int dpkem_sync(dpkem_ctx *ctx, void *stream);
 
+/* Stage timing: when enabled, each batched call records CUDA events on its stream
+ * between the kernels of its launch chain; dpkem_profile_read() waits for them and
+ * returns the number of stages of the last call (its last chunk), filling stage_ms.
+ * Frodo enc: prologue, S'A product, final hash; dec: W/decode, prologue, product, hash.
+ * Saber enc: prologue, product, finish; dec: inner product, prologue, product, finish. */
+int dpkem_profile(dpkem_ctx *ctx, int enable);
+int dpkem_profile_read(dpkem_ctx *ctx, float *stage_ms, int max_stages);
+
+/* Integer-pipe roofline probes on the context's device: 32-bit LOP3/SHF ops per second
+ * in Keccak's instruction mix, and register-resident Keccak-f[1600] permutations per second. */
+int dpkem_probe_int_peaks(dpkem_ctx *ctx, double *int_ops_per_s, double *keccak_per_s);
+
 const char *dpkem_strerror(int status);
 /* Status of the last call made by this thread (the compatibility shims return void). */
 int dpkem_last_status(void);
