@@ -148,7 +148,10 @@ class Engine:
         if all(dev):
             import torch
 
-            return FLAG_DEVICE_PTRS, ctypes.c_void_p(torch.cuda.current_stream(arrs[0].device).cuda_stream)
+            h = torch.cuda.current_stream(arrs[0].device).cuda_stream
+            # torch's default stream is the legacy NULL stream; the C ABI reads NULL as "the
+            # context's own stream", so name the legacy stream explicitly (cudaStreamLegacy).
+            return FLAG_DEVICE_PTRS, ctypes.c_void_p(h if h else 1)
         return 0, None
 
     @staticmethod
