@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdpkem.so")
-SOURCES = ["frodo.cu", "saber.cu", "coins.cu", "peak.cu", "abi.cu"]
+SOURCES = ["frodo.cu", "saber.cu", "coins.cu", "peak.cu", "abi.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "-Xptxas", "-warn-spills"]

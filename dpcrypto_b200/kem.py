@@ -48,6 +48,9 @@ EXPORTS = {
     "dpkem_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
     "dpkem_probe_int_peaks": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_double)]),
+    "dpkem_saber_enc_batch_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
+                                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_void_p]),
     "dpkem_strerror": (ctypes.c_char_p, [ctypes.c_int]),
     "dpkem_last_status": (ctypes.c_int, []),
     "dpkem_set_compat_batch": (None, [ctypes.c_size_t]),

@@ -95,6 +95,21 @@ int dpkem_profile_read(dpkem_ctx *ctx, float *stage_ms, int max_stages);
  * in Keccak's instruction mix, and register-resident Keccak-f[1600] permutations per second. */
 int dpkem_probe_int_peaks(dpkem_ctx *ctx, double *int_ops_per_s, double *keccak_per_s);
 
+/* Saber encapsulation that allocates no device memory (no counterpart in the reference).
+ * For callers that may not call cudaMalloc on their request path (allocator calls are
+ * forbidden there, all device memory belongs to a host framework, or a fixed memory
+ * quota applies).  Scratch is a fixed __device__ array inside the library, sized for
+ * DPKEM_SABER_ENC_STATIC_MAX instances (about 3.9 MB, held on every GPU that loads the
+ * library until exit); n above that returns DPKEM_EINVAL.  coins, pk, ct, ss are device
+ * pointers (8-byte aligned), laid out as in dpkem_enc_batch; stream NULL is the legacy
+ * default stream.  The call returns when the work has finished.  The first call on each
+ * device resolves the array's address (make it before any stream capture).  All calls on
+ * a device share the array: the library serialises its own calls, and work that overlaps
+ * them on the GPU would race. */
+#define DPKEM_SABER_ENC_STATIC_MAX 512
+int dpkem_saber_enc_batch_static(int scheme, int form, size_t n, const uint8_t *coins, const uint8_t *pk,
+                                 uint8_t *ct, uint8_t *ss, void *stream);
+
 const char *dpkem_strerror(int status);
 /* Status of the last call made by this thread (the compatibility shims return void). */
 int dpkem_last_status(void);
