@@ -133,7 +133,8 @@ size_t arena_need(int scheme, int op, size_t chunk, bool host) {
   return s;
 }
 
-bool aligned8(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 7u) == 0; }
+// Device buffers must be 16-byte aligned: the Frodo stages move 16-byte vectors of pk/ct.
+bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 int cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return DPKEM_OK;
@@ -155,7 +156,7 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
   if (n > (size_t)INT32_MAX) return DPKEM_EINVAL;
   if (!in0 || !out0 || (op != OP_KEYPAIR && !in1) || (op != OP_DEC && !out1)) return DPKEM_EINVAL;
   const bool dev = (flags & DPKEM_FLAG_DEVICE_PTRS) != 0;
-  if (dev && !(aligned8(in0) && aligned8(out0) && (!in1 || aligned8(in1)) && (!out1 || aligned8(out1))))
+  if (dev && !(aligned16(in0) && aligned16(out0) && (!in1 || aligned16(in1)) && (!out1 || aligned16(out1))))
     return DPKEM_EINVAL;
   std::lock_guard<std::mutex> lock(c->mu);
   if (cudaSetDevice(c->device) != cudaSuccess) return cuda_status(cudaErrorInvalidDevice);

@@ -1,0 +1,543 @@
+// FrodoKEM-976-SHAKE device routines, written per instance so that the batched kernels
+// (frodo.cu) and the persistent mixed-batch kernel (mixed.cu) run the same code.
+//
+// Stages per operation (all instances independent):
+//   keypair: kp_prologue (thread: seedA, 0x5F stream -> S^T,E)  ->  kp_as_dp4a (CTA: A rows
+//            generated in registers, B = A S + E)  ->  pk_hash (thread: H(pk) into sk)
+//   encaps:  prologue (thread: pkh, G2 = SHAKE256(pkh||mu), 0x96 stream -> S',E',E'')
+//            -> sa_{dp4a,tc} (CTA: B' = S'A + E' with A never leaving the SM, V = S'B + E'',
+//               C = V + Encode(mu), ct written)  ->  ss (thread: SHAKE256(ct||k))
+//   decaps:  dec_w (CTA: W = C - B'S, mu' = Decode(W)) -> prologue -> sa_{dp4a,tc} in compare
+//            mode -> ss with the implicit-reject select.
+//
+// Replaces the reference's ~20-35 launches per operation
+// (FrodoKEM976-GPU/src/cuda_kernel.cu:21-335) whose A matrix made a 1.9 MB HBM round trip
+// per instance (shake128_ser, shake.cu:619-644; DoDP4Av5s, matrix_kernel.cu:183-241).
+#pragma once
+#include "common.cuh"
+#include "keccak.cuh"
+#include "tc.cuh"
+
+namespace dpkem {
+namespace fdev {
+
+using namespace frodo;
+
+// Pointers of one instance, already offset into the caller's arrays and the scratch arena.
+struct Inst {
+  const uint8_t *coins;  // keypair 64 B = s||seedSE||z; enc 24 B = mu
+  uint8_t *pk, *sk, *ct, *ss;
+  uint16_t *rw;          // RW sampled words
+  uint8_t *kk, *mu;      // 24 B each
+  uint32_t *fail;
+};
+
+__device__ __forceinline__ Inst inst_of(const FrodoBatch &b, int i, int op) {
+  Inst v;
+  v.coins = b.coins ? b.coins + (size_t)i * (op == OP_KEYPAIR ? KP_COINS : ENC_COINS) : nullptr;
+  v.pk = b.pk ? b.pk + (size_t)i * PK : nullptr;
+  v.sk = b.sk ? b.sk + (size_t)i * SK : nullptr;
+  v.ct = b.ct ? b.ct + (size_t)i * CT : nullptr;
+  v.ss = b.ss ? b.ss + (size_t)i * SS : nullptr;
+  v.rw = b.rw + (size_t)i * RW;
+  v.kk = b.kk + (size_t)i * LENSE;
+  v.mu = b.mu + (size_t)i * LENMU;
+  v.fail = b.fail + i;
+  return v;
+}
+
+__device__ __forceinline__ uint32_t sample16(uint32_t v) {
+  // Constant-time CDF sampler (FrodoKEM976-GPU/src/sample_pack.cu:13-46, table params.h:24-25).
+  constexpr uint32_t cdf[10] = {5638, 15915, 23689, 28571, 31116, 32217, 32613, 32731, 32760, 32766};
+  const uint32_t t = (v & 0xFFFFu) >> 1, sign = v & 1u;
+  uint32_t s = 0;
+#pragma unroll
+  for (int c = 0; c < 10; c++) s += (cdf[c] - t) >> 31;
+  return (((0u - sign) ^ s) + sign) & 0xFFFFu;
+}
+
+__device__ __forceinline__ uint2 sample_lane(uint2 w) {
+  return make_uint2(sample16(w.x) | (sample16(w.x >> 16) << 16), sample16(w.y) | (sample16(w.y >> 16) << 16));
+}
+
+// Message lanes of 0x5F/0x96 || seed (24 bytes), i.e. the 25-byte sampling-stream input.
+__device__ __forceinline__ void seed_stream_init(uint2 (&a)[25], uint32_t dom, uint2 s0, uint2 s1, uint2 s2) {
+  keccak_zero(a);
+  const uint64_t x0 = ((uint64_t)s0.y << 32) | s0.x, x1 = ((uint64_t)s1.y << 32) | s1.x,
+                 x2 = ((uint64_t)s2.y << 32) | s2.x;
+  const uint64_t l0 = dom | (x0 << 8), l1 = (x0 >> 56) | (x1 << 8), l2 = (x1 >> 56) | (x2 << 8), l3 = x2 >> 56;
+  a[0] = make_uint2((uint32_t)l0, (uint32_t)(l0 >> 32));
+  a[1] = make_uint2((uint32_t)l1, (uint32_t)(l1 >> 32));
+  a[2] = make_uint2((uint32_t)l2, (uint32_t)(l2 >> 32));
+  a[3] = make_uint2((uint32_t)l3, 0u);
+  absorb_finish<136>(a, 25, 0x1Fu);
+}
+
+// Squeeze `words` sampled 16-bit values of the stream into dst (8-byte aligned);
+// when dst_le is non-null the first `le_words` values are also written there (sk's S^T).
+__device__ __forceinline__ void sample_stream(uint2 (&a)[25], uint16_t *dst, int words, uint8_t *dst_le,
+                                              int le_words) {
+  const int nblk = (words + 67) / 68;
+  for (int blk = 0; blk < nblk; blk++) {
+    if (blk) keccak_f1600(a);
+#pragma unroll
+    for (int q = 0; q < 17; q++) {
+      const int w = blk * 68 + 4 * q;
+      if (w < words) {
+        const uint2 v = sample_lane(a[q]);
+        *reinterpret_cast<uint2 *>(dst + w) = v;
+        if (dst_le && w < le_words) *reinterpret_cast<uint2 *>(dst_le + 2 * w) = v;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- thread-level stages
+__device__ __forceinline__ void kp_prologue_inst(const Inst &v) {
+  uint2 a[25];
+  // seedA = SHAKE256(z, 16)
+  keccak_zero(a);
+  a[0] = ld_lane(v.coins + 48);
+  a[1] = ld_lane(v.coins + 56);
+  absorb_finish<136>(a, 16, 0x1Fu);
+  *reinterpret_cast<uint2 *>(v.pk) = a[0];
+  *reinterpret_cast<uint2 *>(v.pk + 8) = a[1];
+  *reinterpret_cast<uint2 *>(v.sk + LENS) = a[0];
+  *reinterpret_cast<uint2 *>(v.sk + LENS + 8) = a[1];
+#pragma unroll
+  for (int q = 0; q < 3; q++) *reinterpret_cast<uint2 *>(v.sk + 8 * q) = ld_lane(v.coins + 8 * q);
+  // S^T || E = sample(SHAKE256(0x5F || seedSE))
+  seed_stream_init(a, 0x5Fu, ld_lane(v.coins + 24), ld_lane(v.coins + 32), ld_lane(v.coins + 40));
+  sample_stream(a, v.rw, 2 * N * NBAR, v.sk + SK_S, N * NBAR);
+}
+
+// H(pk) = SHAKE256(pk, 24) into sk.
+__device__ __forceinline__ void pk_hash_inst(const Inst &v) {
+  uint2 a[25];
+  keccak_zero(a);
+  const int pos = absorb_aligned<136>(a, 0, v.pk, PK);
+  absorb_finish<136>(a, pos, 0x1Fu);
+#pragma unroll
+  for (int q = 0; q < 3; q++) *reinterpret_cast<uint2 *>(v.sk + SK_PKH + 8 * q) = a[q];
+}
+
+template <int MODE>
+__device__ __forceinline__ void prologue_inst(const Inst &v) {
+  uint2 a[25], pkh[3], mu[3];
+  if (MODE == OP_ENC) {
+    keccak_zero(a);
+    const int pos = absorb_aligned<136>(a, 0, v.pk, PK);
+    absorb_finish<136>(a, pos, 0x1Fu);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      pkh[q] = a[q];
+      mu[q] = ld_lane(v.coins + 8 * q);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      pkh[q] = ld_lane(v.sk + SK_PKH + 8 * q);
+      mu[q] = ld_lane(v.mu + 8 * q);
+    }
+  }
+  // G2 = SHAKE256(pkh || mu, 48) = seedSE || k
+  keccak_zero(a);
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    a[q] = pkh[q];
+    a[3 + q] = mu[q];
+  }
+  absorb_finish<136>(a, 48, 0x1Fu);
+#pragma unroll
+  for (int q = 0; q < 3; q++) *reinterpret_cast<uint2 *>(v.kk + 8 * q) = a[3 + q];
+  seed_stream_init(a, 0x96u, a[0], a[1], a[2]);
+  sample_stream(a, v.rw, RW, nullptr, 0);
+}
+
+// ss = SHAKE256(ct || k); decaps selects k' or s in constant time (util.cu:193-226).
+template <int MODE>
+__device__ __forceinline__ void ss_inst(const Inst &v) {
+  uint2 kh[3];
+  if (MODE == OP_ENC) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) kh[q] = ld_lane(v.kk + 8 * q);
+  } else {
+    const uint32_t m = 0u - (uint32_t)(*v.fail != 0u);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const uint2 x = ld_lane(v.kk + 8 * q), y = ld_lane(v.sk + 8 * q);
+      kh[q] = make_uint2((x.x & ~m) | (y.x & m), (x.y & ~m) | (y.y & m));
+    }
+  }
+  uint2 a[25];
+  keccak_zero(a);
+  int pos = absorb_aligned<136>(a, 0, v.ct, CT);
+#pragma unroll
+  for (int q = 0; q < 3; q++) pos = absorb_word<136>(a, pos, kh[q]);
+  absorb_finish<136>(a, pos, 0x1Fu);
+#pragma unroll
+  for (int q = 0; q < 3; q++) *reinterpret_cast<uint2 *>(v.ss + 8 * q) = a[q];
+}
+
+// ---------------------------------------------------------------- CTA-level stages (256 threads)
+constexpr int DEC_W_SMEM = 2 * PKB + 4 * 64 * 4 + 64 * 2;
+
+// decaps: W = C - B'S, mu' = Decode(W).
+__device__ __forceinline__ void dec_w_cta(const Inst &v, uint8_t *smem) {
+  uint16_t *bp = reinterpret_cast<uint16_t *>(smem);
+  uint16_t *st = reinterpret_cast<uint16_t *>(smem + PKB);
+  uint32_t(*red)[64] = reinterpret_cast<uint32_t(*)[64]>(smem + 2 * PKB);
+  uint16_t *w = reinterpret_cast<uint16_t *>(smem + 2 * PKB + 4 * 64 * 4);
+  const int tid = threadIdx.x;
+  const uint8_t *ct = v.ct, *sk = v.sk + SK_S;
+  for (int q = tid; q < PKB / 16; q += 256) {
+    const uint4 x = *reinterpret_cast<const uint4 *>(ct + 16 * q);  // 8 big-endian words
+    *reinterpret_cast<uint4 *>(bp + 8 * q) =
+        make_uint4(prmt(x.x, 0, 0x2301), prmt(x.y, 0, 0x2301), prmt(x.z, 0, 0x2301), prmt(x.w, 0, 0x2301));
+  }
+  for (int q = tid; q < PKB / 8; q += 256) *reinterpret_cast<uint2 *>(st + 4 * q) = ld_lane(sk + 8 * q);
+  __syncthreads();
+  const int o = tid & 63, q = tid >> 6, k = o >> 3, l = o & 7;
+  uint32_t acc = 0;
+  for (int j = 244 * q; j < 244 * q + 244; j++) acc += (uint32_t)bp[k * N + j] * st[l * N + j];
+  red[q][o] = acc;
+  __syncthreads();
+  if (tid < 64) {
+    const uint32_t c = ((uint32_t)ct[PKB + 2 * tid] << 8) | ct[PKB + 2 * tid + 1];
+    w[tid] = (uint16_t)(c - (red[0][tid] + red[1][tid] + red[2][tid] + red[3][tid]));
+  }
+  __syncthreads();
+  if (tid < NBAR) {  // Decode row tid: 8 x 3 bits (encode_decode.cu:31-53)
+    uint32_t t = 0;
+#pragma unroll
+    for (int c = 0; c < NBAR; c++) t |= ((((uint32_t)w[tid * NBAR + c] + (1u << 12)) >> 13) & 7u) << (3 * c);
+    v.mu[3 * tid] = (uint8_t)t;
+    v.mu[3 * tid + 1] = (uint8_t)(t >> 8);
+    v.mu[3 * tid + 2] = (uint8_t)(t >> 16);
+  }
+  __syncthreads();
+}
+
+// Row j of A: state after absorbing LE16(j) || seedA with SHAKE128 padding.
+__device__ __forceinline__ void row_init(uint2 (&a)[25], uint32_t j, uint2 sa0, uint2 sa1) {
+  keccak_zero(a);
+  a[0] = make_uint2(j | (sa0.x << 16), (sa0.x >> 16) | (sa0.y << 16));
+  a[1] = make_uint2((sa0.y >> 16) | (sa1.x << 16), (sa1.x >> 16) | (sa1.y << 16));
+  a[2] = make_uint2((sa1.y >> 16) | (0x1Fu << 16), 0u);
+  a[20].y = 0x80000000u;
+}
+
+__device__ __forceinline__ uint32_t bswap16x2(uint32_t v0, uint32_t v1) { return prmt(v0, v1, 0x4501); }
+
+// V = S'B + E'' + Encode(mu): 64 outputs over 976 terms, 256 threads.  sval(k, j) yields
+// S'[k][j] sign-extended; C is written to ct (encaps) or compared with it (decaps).
+template <int MODE, typename SVal>
+__device__ __forceinline__ uint32_t finish_c(const Inst &v, SVal sval, uint32_t (*red)[64]) {
+  const int tid = threadIdx.x, o = tid & 63, q = tid >> 6, k = o >> 3, l = o & 7;
+  const uint8_t *bsrc = MODE == OP_ENC ? v.pk + SEEDA : v.sk + LENS + SEEDA;
+  uint32_t acc = 0;
+  for (int j = 244 * q; j < 244 * q + 244; j++) {
+    const uint32_t bv = ((uint32_t)bsrc[2 * (NBAR * j + l)] << 8) | bsrc[2 * (NBAR * j + l) + 1];
+    acc += (uint32_t)sval(k, j) * bv;
+  }
+  red[q][o] = acc;
+  __syncthreads();
+  uint32_t diff = 0;
+  if (tid < 64) {
+    const uint16_t *epp = v.rw + 2 * N * NBAR;
+    const uint8_t *mu = MODE == OP_ENC ? v.coins : v.mu;
+    const int kr = tid >> 3, lc = tid & 7;
+    const uint32_t t3 = mu[3 * kr] | ((uint32_t)mu[3 * kr + 1] << 8) | ((uint32_t)mu[3 * kr + 2] << 16);
+    const uint32_t enc = ((t3 >> (3 * lc)) & 7u) << 13;
+    const uint32_t c = (red[0][tid] + red[1][tid] + red[2][tid] + red[3][tid] + epp[tid] + enc) & 0xFFFFu;
+    uint8_t *dst = v.ct + PKB + 2 * tid;
+    if (MODE == OP_ENC) {
+      dst[0] = (uint8_t)(c >> 8);
+      dst[1] = (uint8_t)c;
+    } else {
+      diff = c ^ (((uint32_t)dst[0] << 8) | dst[1]);
+    }
+  }
+  return diff;
+}
+
+// ---------------------------------------------------------------- B' = S'A + E', dp2a form
+// Each warp owns 32-row chunks of A (lane = row).  After every squeeze the warp's
+// 32 x 84 tile goes to shared memory and the warp forms row-pair x S' dot products with
+// dp2a (16-bit A halves x 8-bit S'), flushing column partial sums with shared atomics.
+constexpr int DP4A_SMEM = 83200 + 4 * 64 * 4;
+
+template <int MODE>
+__device__ __forceinline__ void sa_dp4a_cta(const Inst &v, uint8_t *smem) {
+  uint32_t *acc = reinterpret_cast<uint32_t *>(smem);             // [8][976]
+  uint32_t *sp8 = reinterpret_cast<uint32_t *>(smem + 31232);     // [248 quads][8 k]: S'[k][4q..4q+3]
+  uint32_t *tile = reinterpret_cast<uint32_t *>(smem + 39168);    // [8 warps][32 rows][43]
+  uint32_t(*red)[64] = reinterpret_cast<uint32_t(*)[64]>(smem + 83200);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint16_t *rw = v.rw;
+  const uint8_t *seed = MODE == OP_ENC ? v.pk : v.sk + LENS;
+  for (int q = tid; q < N * NBAR; q += 256) acc[q] = 0;
+  for (int q = tid; q < (ROWS_PAD / 4) * NBAR; q += 256) {
+    const int qd = q >> 3, k = q & 7;
+    uint32_t s = 0;
+    if (4 * qd < N) {
+      const uint2 x = *reinterpret_cast<const uint2 *>(rw + k * N + 4 * qd);
+      s = prmt(x.x, x.y, 0x6420);
+    }
+    sp8[q] = s;
+  }
+  const uint2 sa0 = ld_lane(seed), sa1 = ld_lane(seed + 8);
+  __syncthreads();
+  uint32_t *mt = tile + warp * 32 * 43;
+  for (int c = warp; c < ROWS_PAD / 32; c += 8) {
+    uint2 a[25];
+    row_init(a, 32 * c + lane, sa0, sa1);
+    for (int blk = 0; blk < 12; blk++) {
+      keccak_f1600(a);
+#pragma unroll
+      for (int q = 0; q < 21; q++) {
+        mt[lane * 43 + 2 * q] = a[q].x;
+        mt[lane * 43 + 2 * q + 1] = a[q].y;
+      }
+      __syncwarp();
+      const int ncw = blk < 11 ? 42 : 26;
+      for (int w = lane; w < ncw; w += 32) {
+        int alo[8], ahi[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) alo[k] = ahi[k] = 0;
+#pragma unroll 2
+        for (int rq = 0; rq < 8; rq++) {
+          const uint32_t x0 = mt[(4 * rq) * 43 + w], x1 = mt[(4 * rq + 1) * 43 + w];
+          const uint32_t x2 = mt[(4 * rq + 2) * 43 + w], x3 = mt[(4 * rq + 3) * 43 + w];
+          const int p01l = prmt(x0, x1, 0x5410), p01h = prmt(x0, x1, 0x7632);
+          const int p23l = prmt(x2, x3, 0x5410), p23h = prmt(x2, x3, 0x7632);
+          const uint4 s0 = *reinterpret_cast<const uint4 *>(sp8 + (8 * c + rq) * 8);
+          const uint4 s1 = *reinterpret_cast<const uint4 *>(sp8 + (8 * c + rq) * 8 + 4);
+          const int sv[8] = {(int)s0.x, (int)s0.y, (int)s0.z, (int)s0.w, (int)s1.x, (int)s1.y, (int)s1.z, (int)s1.w};
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            alo[k] = dp2a_hi(p23l, sv[k], dp2a_lo(p01l, sv[k], alo[k]));
+            ahi[k] = dp2a_hi(p23h, sv[k], dp2a_lo(p01h, sv[k], ahi[k]));
+          }
+        }
+        const int i0 = 84 * blk + 2 * w;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          atomicAdd(&acc[k * N + i0], (uint32_t)alo[k]);
+          atomicAdd(&acc[k * N + i0 + 1], (uint32_t)ahi[k]);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  uint32_t diff = 0;
+  for (int p = tid; p < N * NBAR / 2; p += 256) {
+    const uint32_t v0 = acc[2 * p] + rw[N * NBAR + 2 * p], v1 = acc[2 * p + 1] + rw[N * NBAR + 2 * p + 1];
+    const uint32_t packed = bswap16x2(v0, v1);
+    if (MODE == OP_ENC) *reinterpret_cast<uint32_t *>(v.ct + 4 * p) = packed;
+    else diff |= packed ^ *reinterpret_cast<const uint32_t *>(v.ct + 4 * p);
+  }
+  auto sval = [&](int k, int j) -> int32_t {
+    return (int32_t)(int8_t)(uint8_t)(sp8[(j >> 2) * 8 + k] >> (8 * (j & 3)));
+  };
+  diff |= finish_c<MODE>(v, sval, red);
+  const int any = __syncthreads_or(diff != 0);
+  if (MODE == OP_DEC && tid == 0) *v.fail = (uint32_t)any;
+}
+
+// ---------------------------------------------------------------- B' = S'A + E', tcgen05 form
+// A (976 x 976, u16) is consumed as u8 hi/lo limb planes.  GEMM view per squeeze block
+// blk (columns 84*blk .. +83 of A):  D_blk,limb[m][k] += sum_j limb(A[j][84 blk + m]) S'[k][j],
+// M = 128 (84 valid), N = 8, K = 32 rows per MMA.  The limb tile is MN-major (row j of
+// A is contiguous along M) in the canonical no-swizzle layout: byte (m, j) at
+// (m/16)*512 + (j/8)*128 + (j%8)*16 + m%16.  S'^T is the K-major B operand: byte (j, k) at
+// (j/16)*128 + k*16 + j%16.  24 accumulators (12 blocks x 2 limbs) x 8 columns in TMEM;
+// B' = lo + 256 hi (mod 2^16).  Every producer warp issues its own MMAs and commits
+// them to its stage barrier; the tile ring has NST stages per warp.
+constexpr int TC_SP_BYTES = 62 * 128;
+constexpr int TC_STAGE = 6144;  // lo plane (6 x 512) + hi plane (6 x 512)
+constexpr int TC_TMEM_COLS = 256;
+
+template <int NST>
+struct TcLayout {
+  static constexpr int ring = TC_SP_BYTES;
+  static constexpr int bars = ring + 8 * NST * TC_STAGE + 1024;  // +1 KB: MMA reads M rows 96..127 past the last plane
+  static constexpr int tslot = bars + (8 * NST + 1) * 8;
+  static constexpr int red = (tslot + 4 + 15) & ~15;
+  static constexpr int total = red + 4 * 64 * 4;
+};
+
+// TMEM columns [tbase, tbase + 192) must be allocated by the caller.  Returns false if a
+// bounded wait expired (the error word is set; the CTA still leaves TMEM idle).
+template <int MODE, int NST>
+__device__ __forceinline__ bool sa_tc_cta(const Inst &v, uint8_t *smem, uint32_t tbase, uint32_t *err) {
+  using L = TcLayout<NST>;
+  uint8_t *sp = smem;
+  uint8_t *ring = smem + L::ring;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bars);
+  uint32_t(*red)[64] = reinterpret_cast<uint32_t(*)[64]>(smem + L::red);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint16_t *rw = v.rw;
+  const uint8_t *seed = MODE == OP_ENC ? v.pk : v.sk + LENS;
+
+  for (int q = tid; q < 62 * NBAR; q += 256) {
+    const int g = q >> 3, k = q & 7;
+    uint4 o = make_uint4(0, 0, 0, 0);
+    if (16 * g < N) {
+      const uint4 x0 = *reinterpret_cast<const uint4 *>(rw + k * N + 16 * g);
+      const uint4 x1 = *reinterpret_cast<const uint4 *>(rw + k * N + 16 * g + 8);
+      o = make_uint4(prmt(x0.x, x0.y, 0x6420), prmt(x0.z, x0.w, 0x6420), prmt(x1.x, x1.y, 0x6420),
+                     prmt(x1.z, x1.w, 0x6420));
+    }
+    *reinterpret_cast<uint4 *>(sp + g * 128 + k * 16) = o;
+  }
+  if (tid == 0) {
+    for (int q = 0; q < 8 * NST; q++) mbar_init(&bars[q], 1);
+    mbar_init(&bars[8 * NST], 8);
+    fence_mbar_init();
+  }
+  const uint2 sa0 = ld_lane(seed), sa1 = ld_lane(seed + 8);
+  if (warp < 4) {
+#pragma unroll
+    for (int col = 0; col < 192; col += 16) tmem_st16_zero(tbase + ((uint32_t)(warp * 32) << 16) + col);
+    tmem_wait_st();
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+
+  constexpr uint32_t idesc = idesc_i8(128, 8, false, true, true, false);
+  const uint32_t sp_addr = smem_u32(sp);
+  const int roff = (lane >> 3) * 128 + (lane & 7) * 16;
+  bool ok = true;
+  uint32_t u = 0;
+  for (int c = warp; c < ROWS_PAD / 32; c += 8) {
+    uint2 a[25];
+    row_init(a, 32 * c + lane, sa0, sa1);
+    const uint64_t bdesc = sdesc(sp_addr + 256 * c, 128, 1024);
+    for (int blk = 0; blk < 12; blk++, u++) {
+      keccak_f1600(a);
+      uint32_t lo[21], hi[21];
+#pragma unroll
+      for (int q = 0; q < 21; q++) {
+        lo[q] = prmt(a[q].x, a[q].y, 0x6420);
+        hi[q] = prmt(a[q].x, a[q].y, 0x7531);
+      }
+      const int s = u % NST;
+      if (u >= NST && ok) ok = mbar_wait(&bars[warp * NST + s], ((u / NST) - 1) & 1);
+      ok = __all_sync(0xffffffffu, ok);
+      uint8_t *stg = ring + (warp * NST + s) * TC_STAGE;
+#pragma unroll
+      for (int cc = 0; cc < 5; cc++) {
+        *reinterpret_cast<uint4 *>(stg + cc * 512 + roff) = make_uint4(lo[4 * cc], lo[4 * cc + 1], lo[4 * cc + 2], lo[4 * cc + 3]);
+        *reinterpret_cast<uint4 *>(stg + 3072 + cc * 512 + roff) =
+            make_uint4(hi[4 * cc], hi[4 * cc + 1], hi[4 * cc + 2], hi[4 * cc + 3]);
+      }
+      *reinterpret_cast<uint32_t *>(stg + 5 * 512 + roff) = lo[20];
+      *reinterpret_cast<uint32_t *>(stg + 3072 + 5 * 512 + roff) = hi[20];
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0 && ok) {
+        tc_fence_after();
+        const uint32_t sa = smem_u32(stg);
+        mma_i8(tbase + blk * 16, sdesc(sa, 128, 512), bdesc, idesc, 1u);
+        mma_i8(tbase + blk * 16 + 8, sdesc(sa + 3072, 128, 512), bdesc, idesc, 1u);
+        mma_commit(&bars[warp * NST + s]);
+      }
+      __syncwarp();
+    }
+  }
+  if (lane == 0) mma_commit(&bars[8 * NST]);
+  bool fin = mbar_wait(&bars[8 * NST], 0);
+  // Drain: observe each stage barrier's last phase, so no arrival is still pending
+  // when the barriers are initialised again for the next instance.
+  for (int s = 0; s < NST; s++)
+    if (ok && u > (uint32_t)s) fin &= mbar_wait(&bars[warp * NST + s], ((u - 1 - s) / NST) & 1);
+  if ((!fin || !ok) && lane == 0) atomicOr(err, DEV_ERR_TIMEOUT);
+  tc_fence_after();
+
+  // Epilogue: B'[k][84 blk + m] = lo + 256 hi + E' (mod 2^16).
+  uint32_t diff = 0;
+  const int qd = warp & 3, m = qd * 32 + lane, b0 = warp < 4 ? 0 : 6;
+  for (int blk = b0; blk < b0 + 6; blk++) {
+    uint32_t r[16];
+    tmem_ld16(tbase + ((uint32_t)(qd * 32) << 16) + blk * 16, r);
+    tmem_wait_ld();
+    if (m < (blk < 11 ? 84 : 52)) {
+      const int col = 84 * blk + m;
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const uint32_t x = (r[k] + (r[8 + k] << 8) + rw[N * NBAR + k * N + col]) & 0xFFFFu;
+        uint8_t *d = v.ct + 2 * (k * N + col);
+        if (MODE == OP_ENC) {
+          *reinterpret_cast<uint16_t *>(d) = (uint16_t)((x >> 8) | (x << 8));
+        } else {
+          diff |= x ^ (((uint32_t)d[0] << 8) | d[1]);
+        }
+      }
+    }
+  }
+  auto sval = [&](int k, int j) -> int32_t {
+    return (int32_t)(int8_t)sp[(j >> 4) * 128 + k * 16 + (j & 15)];
+  };
+  tc_fence_before();
+  __syncthreads();
+  diff |= finish_c<MODE>(v, sval, red);
+  const int any = __syncthreads_or(diff != 0);
+  if (MODE == OP_DEC && tid == 0) *v.fail = (uint32_t)any;
+  return ok && fin;
+}
+
+// ---------------------------------------------------------------- B = A S + E (keypair), dp2a form
+// Thread = row of A: after each squeeze the thread dots its 84 fresh columns with the
+// 8 rows of S^T (broadcast from shared memory), so B[j][k] accumulates in registers.
+constexpr int KP_AS_SMEM = 12 * 21 * 8 * 4;
+
+__device__ __forceinline__ void kp_as_dp4a_cta(const Inst &v, uint8_t *smem) {
+  uint32_t *st8 = reinterpret_cast<uint32_t *>(smem);  // [blk][q][k]: S^T[k][84 blk + 4q .. +3]
+  const int tid = threadIdx.x;
+  const uint16_t *rw = v.rw;
+  for (int x = tid; x < 12 * 21 * 8; x += 256) {
+    const int k = x & 7, q = (x >> 3) % 21, blk = x / 168, j = 84 * blk + 4 * q;
+    uint32_t s = 0;
+    if (j < N) {
+      const uint2 y = *reinterpret_cast<const uint2 *>(rw + k * N + j);
+      s = prmt(y.x, y.y, 0x6420);
+    }
+    st8[x] = s;
+  }
+  const uint2 sa0 = ld_lane(v.pk), sa1 = ld_lane(v.pk + 8);
+  __syncthreads();
+  for (int j = tid; j < N; j += 256) {
+    uint2 a[25];
+    row_init(a, j, sa0, sa1);
+    int acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc[k] = 0;
+    for (int blk = 0; blk < 12; blk++) {
+      keccak_f1600(a);
+#pragma unroll
+      for (int q = 0; q < 21; q++) {
+        const uint4 s0 = *reinterpret_cast<const uint4 *>(st8 + (blk * 21 + q) * 8);
+        const uint4 s1 = *reinterpret_cast<const uint4 *>(st8 + (blk * 21 + q) * 8 + 4);
+        const int sv[8] = {(int)s0.x, (int)s0.y, (int)s0.z, (int)s0.w, (int)s1.x, (int)s1.y, (int)s1.z, (int)s1.w};
+#pragma unroll
+        for (int k = 0; k < 8; k++) acc[k] = dp2a_hi((int)a[q].y, sv[k], dp2a_lo((int)a[q].x, sv[k], acc[k]));
+      }
+    }
+    uint32_t x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = (uint32_t)acc[k] + rw[N * NBAR + NBAR * j + k];
+    const uint4 o = make_uint4(bswap16x2(x[0], x[1]), bswap16x2(x[2], x[3]), bswap16x2(x[4], x[5]),
+                               bswap16x2(x[6], x[7]));
+    *reinterpret_cast<uint4 *>(v.pk + SEEDA + 16 * j) = o;
+    *reinterpret_cast<uint2 *>(v.sk + LENS + SEEDA + 16 * j) = make_uint2(o.x, o.y);
+    *reinterpret_cast<uint2 *>(v.sk + LENS + SEEDA + 16 * j + 8) = make_uint2(o.z, o.w);
+  }
+  __syncthreads();
+}
+
+}  // namespace fdev
+}  // namespace dpkem

@@ -1,536 +1,58 @@
-// Saber (LightSaber l=2, Saber l=3, FireSaber l=4) batched keypair / encaps / decaps
-// for sm_100a.
-//
-// Kernel chain per operation:
-//   prologue  (64 threads = 32 instances: warp 0 runs the hash chain and GenSecret's
-//              SHAKE128, warp 1 runs GenMatrix's SHAKE128, in parallel; raw XOF bytes
-//              go to the scratch arena)
-//   product   (CTA/instance: CBD sampling, 13/10-bit unpacking, the negacyclic
-//              matrix-vector and inner products, rounding, packing / comparison)
-//   finish    (thread/instance: SHA3-256(c), final key, or H(pk) for keypair)
-// Decaps runs the product kernel twice: first the inner product v = b'^T s with the
-// secret from sk (-> m'), then the re-encryption in compare mode.
-//
-// Two product forms:
-//   dp4a: thread = output coefficient; dp2a(16-bit public pair, 8-bit secret pair)
-//         over a reversed, sign-extended secret window (no branch on the wrap).
-//   tc:   tcgen05.mma kind::i8, D[coef][(out, limb)] = sum_K H_j[coef][K] * P[K][(out,limb)].
-//         The public polynomials are written in reversed coefficient order along K,
-//         which turns the negacyclic Toeplitz block of each secret into a Hankel block:
-//         T'[i][k'] = s_ext[i + k' - 255].  Its core matrix (8 rows x 16 bytes) at
-//         (mi, ki) depends only on t = mi + 2 ki, so the whole 256 x 256 block is 62
-//         distinct 128-byte core matrices (SBO = 128, LBO = 256) instead of 64 KB.
-//         Public coefficients are split into u8 limbs (lo 8 bits, hi bits) along N.
-//
-// Replaces the reference's per-stage launches (SABER-GPU/src/cuda_kernel.cu:19-299),
-// its dp4a-shaped DoDP4Av7/_inner products over HBM rotation tables
-// (SABER-GPU/src/poly.cu:26-206) and its FO helpers (pack.cu:215-255), following the
-// round-3 specification order (cmov of z before the final hash).
-#include "common.cuh"
-#include "keccak.cuh"
-#include "tc.cuh"
+// Saber (LightSaber l=2, Saber l=3, FireSaber l=4) batched keypair / encaps / decaps: one
+// launch per stage over n instances.  The stage bodies live in saber_dev.cuh (shared with
+// the persistent mixed-batch kernel); these wrappers only map blockIdx/threadIdx to instances.
+#include "saber_dev.cuh"
 
 namespace dpkem {
 namespace {
 
-using saber::EP;
-using saber::EQ;
-constexpr int SN = saber::N;
+using sdev::inst_of;
+using sdev::PL;
+using sdev::Scr;
 
-enum PMode : int { PM_KEYPAIR = 0, PM_ENC = 1, PM_DEC_CMP = 2, PM_DEC_INNER = 3 };
-
-template <int L>
-struct SP {
-  static constexpr saber::Params p = saber::params(L);
-  static constexpr int MU = p.mu, ET = p.et;
-  static constexpr int POLYVEC = p.polyvec, POLYVECCOMP = p.polyveccomp, PK = p.pk, SK = p.sk, CT = p.ct;
-  static constexpr int ARAW = L * L * EQ * SN / 8;  // GenMatrix bytes
-  static constexpr int SRAW = L * MU * SN / 8;      // GenSecret bytes
-  static constexpr uint32_t H1 = 1u << (EQ - EP - 1);
-  static constexpr uint32_t H2 = (1u << (EP - 2)) - (1u << (EP - ET - 1)) + (1u << (EQ - EP - 1));
-};
-
-// Scratch offsets within one instance's record (all multiples of 16).
-template <int L>
-struct Scr {
-  static constexpr int ARAW = 0;
-  static constexpr int SRAW = (SP<L>::ARAW + 15) & ~15;
-  static constexpr int KR = SRAW + ((SP<L>::SRAW + 15) & ~15);
-  static constexpr int MTXT = KR + 64;
-  static constexpr int BYTES = MTXT + 32;
-};
-
-__device__ __forceinline__ void store_lanes(uint8_t *dst, const uint2 (&a)[25], int nlanes) {
-  for (int q = 0; q < nlanes; q++) *reinterpret_cast<uint2 *>(dst + 8 * q) = a[q];
-}
-
-// SHAKE128 of a 32-byte seed held in 4 lanes, squeezing `len` bytes (len % 8 == 0) to dst.
-__device__ __forceinline__ void shake128_seed32(const uint2 (&seed)[4], uint8_t *dst, int len) {
-  uint2 a[25];
-  keccak_zero(a);
-#pragma unroll
-  for (int q = 0; q < 4; q++) a[q] = seed[q];
-  absorb_finish<168>(a, 32, 0x1Fu);
-  for (int off = 0;; off += 168) {
-#pragma unroll
-    for (int q = 0; q < 21; q++)
-      if (off + 8 * q < len) *reinterpret_cast<uint2 *>(dst + off + 8 * q) = a[q];
-    if (off + 168 >= len) break;
-    keccak_f1600(a);
-  }
-}
-
-// SHA3-256 of a whole byte string (length multiple of 8, 8-byte aligned).
-__device__ __forceinline__ void sha3_256_msg(const uint8_t *p, int len, uint2 (&out)[4]) {
-  uint2 a[25];
-  keccak_zero(a);
-  const int pos = absorb_aligned<136>(a, 0, p, len);
-  absorb_finish<136>(a, pos, 0x06u);
-#pragma unroll
-  for (int q = 0; q < 4; q++) out[q] = a[q];
-}
-
-// SHA3-256 / SHA3-512 of 64 bytes held in lanes.
-__device__ __forceinline__ void sha3_256_64(const uint2 (&m)[8], uint2 (&out)[4]) {
-  uint2 a[25];
-  keccak_zero(a);
-#pragma unroll
-  for (int q = 0; q < 8; q++) a[q] = m[q];
-  absorb_finish<136>(a, 64, 0x06u);
-#pragma unroll
-  for (int q = 0; q < 4; q++) out[q] = a[q];
-}
-__device__ __forceinline__ void sha3_512_64(const uint2 (&m)[8], uint2 (&out)[8]) {
-  uint2 a[25];
-  keccak_zero(a);
-#pragma unroll
-  for (int q = 0; q < 8; q++) a[q] = m[q];
-  absorb_finish<72>(a, 64, 0x06u);
-#pragma unroll
-  for (int q = 0; q < 8; q++) out[q] = a[q];
-}
-
-// ---------------------------------------------------------------- prologue
 // blockDim 64: warp 0 = hash chain + GenSecret XOF, warp 1 = GenMatrix XOF, 32 instances.
 template <int L, int OP>
 __global__ void __launch_bounds__(64) prologue_kernel(SaberBatch b) {
-  using P = SP<L>;
-  using S = Scr<L>;
-  const int warp = threadIdx.x >> 5;
   const int i = blockIdx.x * 32 + (threadIdx.x & 31);
-  if (i >= b.n) return;
-  uint8_t *scr = b.scr + (size_t)i * S::BYTES;
-  if (warp == 1) {
-    uint2 seed[4];
-    if (OP == OP_KEYPAIR) {
-      // seed_A = SHAKE128(coins[0:32], 32), published in pk.
-      uint2 a[25];
-      keccak_zero(a);
-#pragma unroll
-      for (int q = 0; q < 4; q++) a[q] = ld_lane(b.coins + (size_t)i * 96 + 8 * q);
-      absorb_finish<168>(a, 32, 0x1Fu);
-      uint8_t *pk = b.pk + (size_t)i * P::PK + P::POLYVECCOMP;
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        seed[q] = a[q];
-        *reinterpret_cast<uint2 *>(pk + 8 * q) = a[q];
-      }
-    } else {
-      const uint8_t *src = OP == OP_ENC ? b.pk + (size_t)i * P::PK + P::POLYVECCOMP
-                                        : b.sk + (size_t)i * P::SK + P::POLYVEC + P::POLYVECCOMP;
-#pragma unroll
-      for (int q = 0; q < 4; q++) seed[q] = ld_lane(src + 8 * q);
-    }
-    shake128_seed32(seed, scr + S::ARAW, P::ARAW);
-    return;
-  }
-  uint2 seed[4];
-  if (OP == OP_KEYPAIR) {
-#pragma unroll
-    for (int q = 0; q < 4; q++) seed[q] = ld_lane(b.coins + (size_t)i * 96 + 32 + 8 * q);
-  } else {
-    uint2 buf[8], kr[8];
-    if (OP == OP_ENC) {
-      // m = SHA3-256(coins), H(pk), kr = SHA3-512(m || H(pk))  (cuda_kernel.cu:68-70)
-      uint2 c8[8], h[4];
-#pragma unroll
-      for (int q = 0; q < 4; q++) c8[q] = ld_lane(b.coins + (size_t)i * 32 + 8 * q);
-#pragma unroll
-      for (int q = 4; q < 8; q++) c8[q] = make_uint2(0, 0);
-      uint2 a[25];
-      keccak_zero(a);
-#pragma unroll
-      for (int q = 0; q < 4; q++) a[q] = c8[q];
-      absorb_finish<136>(a, 32, 0x06u);
-#pragma unroll
-      for (int q = 0; q < 4; q++) buf[q] = a[q];
-      sha3_256_msg(b.pk + (size_t)i * P::PK, P::PK, h);
-#pragma unroll
-      for (int q = 0; q < 4; q++) buf[4 + q] = h[q];
-    } else {
-      // m' from the inner-product pass, H(pk) stored in sk (cuda_kernel.cu:231-232)
-      const uint8_t *hpk = b.sk + (size_t)i * P::SK + P::SK - 64;
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        buf[q] = ld_lane(scr + S::MTXT + 8 * q);
-        buf[4 + q] = ld_lane(hpk + 8 * q);
-      }
-    }
-    sha3_512_64(buf, kr);
-    uint8_t *krp = scr + S::KR;
-#pragma unroll
-    for (int q = 0; q < 8; q++) *reinterpret_cast<uint2 *>(krp + 8 * q) = kr[q];
-    if (OP == OP_ENC) {
-#pragma unroll
-      for (int q = 0; q < 4; q++) *reinterpret_cast<uint2 *>(scr + S::MTXT + 8 * q) = buf[q];
-    }
-#pragma unroll
-    for (int q = 0; q < 4; q++) seed[q] = kr[4 + q];
-  }
-  shake128_seed32(seed, scr + S::SRAW, P::SRAW);
+  if (i < b.n) sdev::prologue_inst<L, OP>(inst_of<L>(b, i, OP), threadIdx.x >> 5);
 }
 
-// ---------------------------------------------------------------- finish
 template <int L, int OP>
 __global__ void __launch_bounds__(64) finish_kernel(SaberBatch b) {
-  using P = SP<L>;
-  using S = Scr<L>;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= b.n) return;
-  if (OP == OP_KEYPAIR) {
-    const uint8_t *pk = b.pk + (size_t)i * P::PK;
-    uint8_t *sk = b.sk + (size_t)i * P::SK;
-    for (int off = 0; off < P::PK; off += 8) *reinterpret_cast<uint2 *>(sk + P::POLYVEC + off) = ld_lane(pk + off);
-    uint2 h[4];
-    sha3_256_msg(pk, P::PK, h);
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      *reinterpret_cast<uint2 *>(sk + P::SK - 64 + 8 * q) = h[q];
-      *reinterpret_cast<uint2 *>(sk + P::SK - 32 + 8 * q) = ld_lane(b.coins + (size_t)i * 96 + 64 + 8 * q);
-    }
-    return;
-  }
-  const uint8_t *scr = b.scr + (size_t)i * S::BYTES;
-  uint2 m[8], hc[4], k[4];
-  sha3_256_msg(b.ct + (size_t)i * P::CT, P::CT, hc);
-  const uint32_t msk = OP == OP_DEC ? 0u - (uint32_t)(b.fail[i] != 0u) : 0u;
-  const uint8_t *z = b.sk + (size_t)i * P::SK + P::SK - 32;
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    uint2 x = ld_lane(scr + S::KR + 8 * q);
-    if (OP == OP_DEC) {  // cmov(kr, z, fail) before the final hash
-      const uint2 y = ld_lane(z + 8 * q);
-      x = make_uint2((x.x & ~msk) | (y.x & msk), (x.y & ~msk) | (y.y & msk));
-    }
-    m[q] = x;
-    m[4 + q] = hc[q];
-  }
-  sha3_256_64(m, k);
-#pragma unroll
-  for (int q = 0; q < 4; q++) *reinterpret_cast<uint2 *>(b.ss + (size_t)i * 32 + 8 * q) = k[q];
+  if (i < b.n) sdev::finish_inst<L, OP>(inst_of<L>(b, i, OP));
 }
 
-// ---------------------------------------------------------------- bit packing helpers
-__device__ __forceinline__ uint32_t unpack_coef(const uint8_t *src, int nbytes, int c, int bits) {
-  const int bit = c * bits, by = bit >> 3, sh = bit & 7;
-  uint32_t w = src[by];
-  if (by + 1 < nbytes) w |= (uint32_t)src[by + 1] << 8;
-  if (by + 2 < nbytes) w |= (uint32_t)src[by + 2] << 16;
-  return (w >> sh) & ((1u << bits) - 1u);
+__host__ __device__ constexpr int op_of(int mode) {
+  return mode == sdev::PM_KEYPAIR ? OP_KEYPAIR : mode == sdev::PM_ENC ? OP_ENC : OP_DEC;
 }
 
-__device__ __forceinline__ uint32_t pack_byte(const uint16_t *v, int q, int bits) {
-  const int bit0 = 8 * q;
-  int c = bit0 / bits;
-  const int off = bit0 - c * bits;
-  const uint32_t mask = (1u << bits) - 1u;
-  uint32_t acc = (v[c] & mask) >> off;
-  int have = bits - off;
-  while (have < 8) {
-    c++;
-    acc |= (uint32_t)(v[c] & mask) << have;
-    have += bits;
-  }
-  return acc & 0xFFu;
-}
-
-// CBD_mu: coefficient c = popcount(bits [mu c, mu c + mu/2)) - popcount(next mu/2 bits).
-template <int MU>
-__device__ __forceinline__ int cbd_coef(const uint8_t *raw, int c) {
-  const uint32_t v = unpack_coef(raw, MU * SN / 8, c, MU);
-  constexpr uint32_t hm = (1u << (MU / 2)) - 1u;
-  return __popc(v & hm) - __popc((v >> (MU / 2)) & hm);
-}
-
-// ---------------------------------------------------------------- product kernel
-// Shared-memory layout common to both forms.
-template <int L>
-struct PL {
-  static constexpr int NO_MAX = L + 1;
-  static constexpr int A16 = 0;                               // u16 [L*L][256]
-  static constexpr int B16 = A16 + L * L * SN * 2;            // u16 [L][256] public b / b'
-  static constexpr int SEC = B16 + L * SN * 2;                // s8  [L][256]
-  static constexpr int RES = SEC + L * SN;                    // u16 [L+1][256]
-  static constexpr int CM = RES + NO_MAX * SN * 2;            // u16 [256]
-  static constexpr int SEQ = CM + SN * 2;                     // s8  [L][528] secret sequences
-  static constexpr int SEQ_STRIDE = 528;
-  static constexpr int COMMON = SEQ + L * SEQ_STRIDE;
-  // tcgen05 form
-  static constexpr int HANK = (COMMON + 127) & ~127;          // [L][62][128]
-  static constexpr int HANK_STRIDE = 62 * 128;
-  static constexpr int BOP = HANK + L * HANK_STRIDE;          // [NPAD/8][K/16][8][16]
-  static constexpr int NPAD = 2 * NO_MAX <= 8 ? 8 : 16;
-  static constexpr int BOP_GROUP = L * SN / 16 * 128;         // bytes per 8-row N group
-  static constexpr int BAR = BOP + (NPAD / 8) * BOP_GROUP;
-  static constexpr int TSLOT = BAR + 8;
-  static constexpr int TC_TOTAL = TSLOT + 8;
-};
-
-template <int L, int MODE>
-__device__ __forceinline__ constexpr int n_out() {
-  return MODE == PM_KEYPAIR ? L : MODE == PM_DEC_INNER ? 1 : L + 1;
-}
-
-// Phase 1: secrets and public polynomials into shared memory.
-template <int L, int MODE>
-__device__ __forceinline__ void load_operands(const SaberBatch &b, int i, uint8_t *sm) {
-  using P = SP<L>;
-  using S = Scr<L>;
-  using Y = PL<L>;
-  const int tid = threadIdx.x;
-  const uint8_t *scr = b.scr + (size_t)i * S::BYTES;
-  int8_t *sec = reinterpret_cast<int8_t *>(sm + Y::SEC);
-  uint16_t *a16 = reinterpret_cast<uint16_t *>(sm + Y::A16);
-  uint16_t *b16 = reinterpret_cast<uint16_t *>(sm + Y::B16);
-  uint16_t *cm = reinterpret_cast<uint16_t *>(sm + Y::CM);
-  if (MODE == PM_DEC_INNER) {
-    const uint8_t *sk = b.sk + (size_t)i * P::SK;
-    const uint8_t *ct = b.ct + (size_t)i * P::CT;
-    for (int c = tid; c < L * SN; c += blockDim.x) {
-      const uint32_t v = unpack_coef(sk, P::POLYVEC, c, EQ);
-      sec[c] = (int8_t)(int32_t)(((v ^ 0x1000u) - 0x1000u));  // centred 13-bit secret
-      b16[c] = (uint16_t)unpack_coef(ct, P::POLYVECCOMP, c, EP);
-    }
-    for (int c = tid; c < SN; c += blockDim.x)
-      cm[c] = (uint16_t)unpack_coef(ct + P::POLYVECCOMP, P::ET * SN / 8, c, P::ET);
-  } else {
-    const uint8_t *sraw = scr + S::SRAW, *araw = scr + S::ARAW;
-    for (int c = tid; c < L * SN; c += blockDim.x) sec[c] = (int8_t)cbd_coef<P::MU>(sraw + (c / SN) * (P::MU * SN / 8), c % SN);
-    for (int c = tid; c < L * L * SN; c += blockDim.x)
-      a16[c] = (uint16_t)unpack_coef(araw + (c / SN) * (EQ * SN / 8), EQ * SN / 8, c % SN, EQ);
-    if (MODE != PM_KEYPAIR) {
-      const uint8_t *pk = MODE == PM_ENC ? b.pk + (size_t)i * P::PK : b.sk + (size_t)i * P::SK + P::POLYVEC;
-      for (int c = tid; c < L * SN; c += blockDim.x) b16[c] = (uint16_t)unpack_coef(pk, P::POLYVECCOMP, c, EP);
-    }
-  }
-}
-
-// Public polynomial multiplied by secret j for output o.
-template <int L, int MODE>
-__device__ __forceinline__ const uint16_t *pub_poly(const uint8_t *sm, int o, int j) {
-  using Y = PL<L>;
-  const uint16_t *a16 = reinterpret_cast<const uint16_t *>(sm + Y::A16);
-  const uint16_t *b16 = reinterpret_cast<const uint16_t *>(sm + Y::B16);
-  if (MODE == PM_DEC_INNER) return b16 + j * SN;
-  if (MODE == PM_KEYPAIR) return a16 + (j * L + o) * SN;  // transposed: b = A^T s
-  return o < L ? a16 + (o * L + j) * SN : b16 + j * SN;
-}
-
-// Phase 3: rounding, packing / comparison.  res holds the products mod 2^16.
-template <int L, int MODE>
-__device__ __forceinline__ void epilogue(const SaberBatch &b, int i, uint8_t *sm) {
-  using P = SP<L>;
-  using S = Scr<L>;
-  using Y = PL<L>;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  uint16_t *res = reinterpret_cast<uint16_t *>(sm + Y::RES);
-  uint8_t *scr = b.scr + (size_t)i * S::BYTES;
-  if (MODE == PM_DEC_INNER) {
-    const uint16_t *cm = reinterpret_cast<const uint16_t *>(sm + Y::CM);
-    for (int c = tid; c < SN; c += nt)
-      res[c] = (uint16_t)(((uint32_t)res[c] + P::H2 - ((uint32_t)cm[c] << (EP - P::ET))) >> (EP - 1)) & 1u;
-    __syncthreads();
-    if (tid < 32) scr[S::MTXT + tid] = (uint8_t)pack_byte(res, tid, 1);
-    return;
-  }
-  for (int c = tid; c < L * SN; c += nt) res[c] = (uint16_t)((((uint32_t)res[c] + P::H1) >> (EQ - EP)) & 0x3FFu);
-  if (MODE != PM_KEYPAIR) {
-    const uint8_t *mt = scr + S::MTXT;
-    for (int c = tid; c < SN; c += nt) {
-      const uint32_t mb = (mt[c >> 3] >> (c & 7)) & 1u;
-      res[L * SN + c] = (uint16_t)((((uint32_t)res[L * SN + c] - (mb << (EP - 1)) + P::H1) >> (EP - P::ET)) &
-                                   ((1u << P::ET) - 1u));
-    }
-  }
-  __syncthreads();
-  if (MODE == PM_KEYPAIR) {
-    uint8_t *pk = b.pk + (size_t)i * P::PK;
-    uint8_t *sk = b.sk + (size_t)i * P::SK;
-    const int8_t *sec = reinterpret_cast<const int8_t *>(sm + Y::SEC);
-    for (int q = tid; q < P::POLYVECCOMP; q += nt) pk[q] = (uint8_t)pack_byte(res, q, EP);
-    uint16_t *s13 = reinterpret_cast<uint16_t *>(sm + Y::A16);  // A no longer needed
-    for (int c = tid; c < L * SN; c += nt) s13[c] = (uint16_t)((int32_t)sec[c] & 0x1FFF);
-    __syncthreads();
-    for (int q = tid; q < P::POLYVEC; q += nt) sk[q] = (uint8_t)pack_byte(s13, q, EQ);
-    return;
-  }
-  uint8_t *ct = b.ct + (size_t)i * P::CT;
-  uint32_t diff = 0;
-  for (int q = tid; q < P::CT; q += nt) {
-    const uint32_t v = q < P::POLYVECCOMP ? pack_byte(res, q, EP) : pack_byte(res + L * SN, q - P::POLYVECCOMP, P::ET);
-    if (MODE == PM_ENC) ct[q] = (uint8_t)v;
-    else diff |= v ^ ct[q];
-  }
-  if (MODE == PM_DEC_CMP) {
-    const int any = __syncthreads_or(diff != 0);
-    if (tid == 0) b.fail[i] = (uint32_t)any;
-  }
-}
-
-// ---------------------------------------------------------------- dp4a form
-// Secret j's reversed sign-extended window R_j[t] = s_ext[255 - t], t in [0, 512), with
-// s_ext[d] = s[d] (d >= 0), -s[d + 256] (d < 0): coefficient i of s*P is
-// sum_m P[m] R_j[255 - i + m].
 template <int L, int MODE>
 __global__ void __launch_bounds__(256) product_dp4a_kernel(SaberBatch b) {
-  using Y = PL<L>;
-  constexpr int NO = n_out<L, MODE>();
   extern __shared__ __align__(1024) uint8_t sm[];
-  const int i = blockIdx.x, tid = threadIdx.x;
-  load_operands<L, MODE>(b, i, sm);
-  __syncthreads();
-  const int8_t *sec = reinterpret_cast<const int8_t *>(sm + Y::SEC);
-  for (int v = tid; v < L * Y::SEQ_STRIDE; v += 256) {
-    const int j = v / Y::SEQ_STRIDE, t = v % Y::SEQ_STRIDE;
-    int8_t r = 0;
-    if (t < 256) r = sec[j * SN + 255 - t];
-    else if (t < 512) r = (int8_t)(-sec[j * SN + 511 - t]);
-    reinterpret_cast<int8_t *>(sm + Y::SEQ)[v] = r;
-  }
-  __syncthreads();
-  const int base = 255 - tid, wb = base >> 2, sh = 8 * (base & 3);
-  int acc[NO];
-#pragma unroll
-  for (int o = 0; o < NO; o++) acc[o] = 0;
-  for (int j = 0; j < L; j++) {
-    const uint32_t *rw = reinterpret_cast<const uint32_t *>(sm + Y::SEQ + j * Y::SEQ_STRIDE);
-    const uint2 *pp[NO];
-#pragma unroll
-    for (int o = 0; o < NO; o++) pp[o] = reinterpret_cast<const uint2 *>(pub_poly<L, MODE>(sm, o, j));
-    uint32_t w0 = rw[wb];
-#pragma unroll 4
-    for (int mq = 0; mq < SN / 4; mq++) {
-      const uint32_t w1 = rw[wb + mq + 1];
-      const int win = (int)__funnelshift_r(w0, w1, sh);
-      w0 = w1;
-#pragma unroll
-      for (int o = 0; o < NO; o++) {
-        const uint2 pw = pp[o][mq];
-        acc[o] = dp2a_hi((int)pw.y, win, dp2a_lo((int)pw.x, win, acc[o]));
-      }
-    }
-  }
-  uint16_t *res = reinterpret_cast<uint16_t *>(sm + Y::RES);
-#pragma unroll
-  for (int o = 0; o < NO; o++) res[o * SN + tid] = (uint16_t)acc[o];
-  __syncthreads();
-  epilogue<L, MODE>(b, i, sm);
+  sdev::product_dp4a_cta<L, MODE>(inst_of<L>(b, blockIdx.x, op_of(MODE)), sm);
 }
 
-// ---------------------------------------------------------------- tcgen05 form
 template <int L, int MODE>
 __global__ void __launch_bounds__(256) product_tc_kernel(SaberBatch b) {
   using Y = PL<L>;
-  constexpr int NO = n_out<L, MODE>();
-  constexpr int NPAD = 2 * NO <= 8 ? 8 : 16;
   extern __shared__ __align__(1024) uint8_t sm[];
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Y::BAR);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + Y::TSLOT);
-  const int i = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (warp == 0) {
+  if (threadIdx.x < 32) {
     tmem_alloc(tslot, 32);
     tmem_relinquish();
   }
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    fence_mbar_init();
-  }
-  load_operands<L, MODE>(b, i, sm);
-  __syncthreads();
-  // E_j[e] = s_ext[e - 255], e in [0, 511): the Hankel generating sequence.
-  const int8_t *sec = reinterpret_cast<const int8_t *>(sm + Y::SEC);
-  int8_t *seq = reinterpret_cast<int8_t *>(sm + Y::SEQ);
-  for (int v = tid; v < L * Y::SEQ_STRIDE; v += 256) {
-    const int j = v / Y::SEQ_STRIDE, e = v % Y::SEQ_STRIDE;
-    int8_t r = 0;
-    if (e >= 255 && e < 511) r = sec[j * SN + e - 255];
-    else if (e < 255) r = (int8_t)(-sec[j * SN + e + 1]);
-    seq[v] = r;
-  }
-  __syncthreads();
-  // Hankel core matrices: H_j[t][r][c] = E_j[8t + r + c].
-  for (int v = tid; v < L * 62 * 8; v += 256) {
-    const int j = v / (62 * 8), t = (v / 8) % 62, r = v & 7, e0 = 8 * t + r;
-    const uint32_t *sw = reinterpret_cast<const uint32_t *>(seq + j * Y::SEQ_STRIDE);
-    const int wb = e0 >> 2, sh = 8 * (e0 & 3);
-    const uint32_t x0 = sw[wb], x1 = sw[wb + 1], x2 = sw[wb + 2], x3 = sw[wb + 3], x4 = sw[wb + 4];
-    *reinterpret_cast<uint4 *>(sm + Y::HANK + j * Y::HANK_STRIDE + t * 128 + r * 16) =
-        make_uint4(__funnelshift_r(x0, x1, sh), __funnelshift_r(x1, x2, sh), __funnelshift_r(x2, x3, sh),
-                   __funnelshift_r(x3, x4, sh));
-  }
-  // B operand: row n = o + NO*limb, K = 256 j + k', value = limb(P_{o,j}[255 - k']).
-  for (int v = tid; v < NPAD * L * (SN / 16); v += 256) {
-    const int n = v / (L * SN / 16), kc = v % (L * SN / 16), j = kc / (SN / 16), k0 = 16 * (kc % (SN / 16));
-    uint32_t w[4] = {0, 0, 0, 0};
-    if (n < 2 * NO) {
-      const int o = n % NO, limb = n / NO;
-      const uint16_t *pp = pub_poly<L, MODE>(sm, o, j);
-#pragma unroll
-      for (int c = 0; c < 16; c++) {
-        const uint32_t x = pp[255 - (k0 + c)];
-        const uint32_t byte = limb ? (x >> 8) : (x & 0xFFu);
-        w[c >> 2] |= byte << (8 * (c & 3));
-      }
-    }
-    *reinterpret_cast<uint4 *>(sm + Y::BOP + (n >> 3) * Y::BOP_GROUP + kc * 128 + (n & 7) * 16) =
-        make_uint4(w[0], w[1], w[2], w[3]);
-  }
-  fence_proxy_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = *tslot;
-  if (tid == 0) {
-    constexpr uint32_t idesc = idesc_i8(128, NPAD, true, false, false, false);
-    const uint32_t h0 = smem_u32(sm + Y::HANK), b0 = smem_u32(sm + Y::BOP);
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++)
-      for (int j = 0; j < L; j++)
-#pragma unroll
-        for (int ks = 0; ks < 8; ks++) {
-          const uint64_t ad = sdesc(h0 + j * Y::HANK_STRIDE + (16 * mt + 4 * ks) * 128, 256, 128);
-          const uint64_t bd = sdesc(b0 + (16 * j + 2 * ks) * 128, 128, Y::BOP_GROUP);
-          mma_i8(tbase + mt * NPAD, ad, bd, idesc, (j | ks) ? 1u : 0u);
-        }
-    mma_commit(bar);
-  }
-  const bool ok = mbar_wait(bar, 0);
-  if (!ok && lane == 0) atomicOr(b.err, DEV_ERR_TIMEOUT);
-  tc_fence_after();
-  // Warp w reads TMEM lanes 32 (w % 4) .. of M tile w / 4: coefficient = tid.
-  uint32_t r[16];
-  tmem_ld16(tbase + ((uint32_t)((warp & 3) * 32) << 16) + (warp >> 2) * NPAD, r);
-  tmem_wait_ld();
-  uint16_t *res = reinterpret_cast<uint16_t *>(sm + Y::RES);
-#pragma unroll
-  for (int o = 0; o < NO; o++) res[o * SN + tid] = (uint16_t)(r[o] + (r[NO + o] << 8));
+  sdev::product_tc_cta<L, MODE>(inst_of<L>(b, blockIdx.x, op_of(MODE)), sm, tbase, b.err);
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) {
+  if (threadIdx.x < 32) {
     tc_fence_after();
     tmem_dealloc(tbase, 32);
   }
-  epilogue<L, MODE>(b, i, sm);
 }
 
 template <typename K>
@@ -567,23 +89,23 @@ cudaError_t run(const SaberBatch &b, int op, int form, cudaStream_t st) {
     case OP_KEYPAIR:
       prologue_kernel<L, OP_KEYPAIR><<<pb, 64, 0, st>>>(b);
       mark(b, st);
-      if ((e = launch_product<L, PM_KEYPAIR>(b, form, st)) != cudaSuccess) return e;
+      if ((e = launch_product<L, sdev::PM_KEYPAIR>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
       finish_kernel<L, OP_KEYPAIR><<<fb, 64, 0, st>>>(b);
       break;
     case OP_ENC:
       prologue_kernel<L, OP_ENC><<<pb, 64, 0, st>>>(b);
       mark(b, st);
-      if ((e = launch_product<L, PM_ENC>(b, form, st)) != cudaSuccess) return e;
+      if ((e = launch_product<L, sdev::PM_ENC>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
       finish_kernel<L, OP_ENC><<<fb, 64, 0, st>>>(b);
       break;
     default:
-      if ((e = launch_product<L, PM_DEC_INNER>(b, form, st)) != cudaSuccess) return e;
+      if ((e = launch_product<L, sdev::PM_DEC_INNER>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
       prologue_kernel<L, OP_DEC><<<pb, 64, 0, st>>>(b);
       mark(b, st);
-      if ((e = launch_product<L, PM_DEC_CMP>(b, form, st)) != cudaSuccess) return e;
+      if ((e = launch_product<L, sdev::PM_DEC_CMP>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
       finish_kernel<L, OP_DEC><<<fb, 64, 0, st>>>(b);
       break;

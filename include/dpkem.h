@@ -49,7 +49,7 @@ enum { DPKEM_FRODO976 = 0, DPKEM_LIGHTSABER = 2, DPKEM_SABER = 3, DPKEM_FIRESABE
 enum { DPKEM_FORM_DP4A = 0, DPKEM_FORM_INT32 = 1, DPKEM_FORM_TC = 2 };
 
 /* Flags. */
-#define DPKEM_FLAG_DEVICE_PTRS 1u /* all buffers are device pointers (8-byte aligned); call is async */
+#define DPKEM_FLAG_DEVICE_PTRS 1u /* all buffers are device pointers (16-byte aligned); call is async */
 
 typedef struct dpkem_ctx dpkem_ctx;
 
