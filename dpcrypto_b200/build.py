@@ -17,7 +17,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdpkem.so")
-SOURCES = ["frodo.cu", "saber.cu", "coins.cu", "peak.cu", "abi.cu", "noalloc.cu"]
+SOURCES = ["frodo.cu", "saber.cu", "coins.cu", "peak.cu", "abi.cu", "noalloc.cu", "mixed.cu"]
+# The persistent mixed-batch kernel reads data other CTAs wrote in the same launch: its
+# global loads bypass the (non-coherent) L1.
+EXTRA = {"mixed.cu": ["-Xptxas", "-dlcm=cg"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "-Xptxas", "-warn-spills"]
@@ -46,7 +49,7 @@ def build(verbose: bool = False) -> str:
     for s in SOURCES:
         src, obj = os.path.join(CSRC, s), os.path.join(OBJ, s + ".o")
         if _stale(src, obj):
-            jobs.append([cc, *FLAGS, *ARCH, "-c", src, "-o", obj])
+            jobs.append([cc, *FLAGS, *EXTRA.get(s, []), *ARCH, "-c", src, "-o", obj])
 
     def run(cmd):
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -133,8 +133,19 @@ size_t arena_need(int scheme, int op, size_t chunk, bool host) {
   return s;
 }
 
-// Device buffers must be 16-byte aligned: the Frodo stages move 16-byte vectors of pk/ct.
+// Device buffers: pk and ct arrays must be 16-byte aligned (the Frodo stages move 16-byte
+// vectors of them), coins, sk and ss arrays 8-byte aligned (64-bit lane loads/stores).
 bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+bool aligned8(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 7u) == 0; }
+
+// Alignment check of an operation's buffers in argument order (see run_op).
+bool op_aligned(int op, const void *in0, const void *in1, const void *out0, const void *out1) {
+  switch (op) {
+    case OP_KEYPAIR: return aligned8(in0) && aligned16(out0) && aligned8(out1);             // coins, pk, sk
+    case OP_ENC: return aligned8(in0) && aligned16(in1) && aligned16(out0) && aligned8(out1);  // coins, pk, ct, ss
+    default: return aligned16(in0) && aligned8(in1) && aligned8(out0);                     // ct, sk, ss
+  }
+}
 
 int cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return DPKEM_OK;
@@ -156,8 +167,7 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
   if (n > (size_t)INT32_MAX) return DPKEM_EINVAL;
   if (!in0 || !out0 || (op != OP_KEYPAIR && !in1) || (op != OP_DEC && !out1)) return DPKEM_EINVAL;
   const bool dev = (flags & DPKEM_FLAG_DEVICE_PTRS) != 0;
-  if (dev && !(aligned16(in0) && aligned16(out0) && (!in1 || aligned16(in1)) && (!out1 || aligned16(out1))))
-    return DPKEM_EINVAL;
+  if (dev && !op_aligned(op, in0, in1, out0, out1)) return DPKEM_EINVAL;
   std::lock_guard<std::mutex> lock(c->mu);
   if (cudaSetDevice(c->device) != cudaSuccess) return cuda_status(cudaErrorInvalidDevice);
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
@@ -350,6 +360,118 @@ int dpkem_enc_batch(dpkem_ctx *c, int scheme, int form, size_t n, const uint8_t 
 int dpkem_dec_batch(dpkem_ctx *c, int scheme, int form, size_t n, const uint8_t *ct, const uint8_t *sk, uint8_t *ss,
                     unsigned flags, void *stream) {
   return set_status(run_op(c, scheme, form, OP_DEC, n, ct, sk, ss, nullptr, flags, stream));
+}
+
+static_assert(sizeof(dpkem_request) == sizeof(mixed::Req), "request layout");
+
+static int check_requests(size_t n, const dpkem_request *reqs) {
+  if (!reqs || n == 0 || n > (size_t)INT32_MAX) return DPKEM_EINVAL;
+  for (size_t i = 0; i < n; i++) {
+    const dpkem_request &r = reqs[i];
+    Sizes z;
+    if (!scheme_sizes(r.scheme, &z) || r.op < 0 || r.op > 2) return DPKEM_EINVAL;
+    const bool two_out = r.op != OP_DEC;
+    if (!r.in0 || !r.out0 || (r.op != OP_KEYPAIR && !r.in1) || (two_out && !r.out1)) return DPKEM_EINVAL;
+    if (!op_aligned(r.op, r.in0, r.in1, r.out0, r.out1)) return DPKEM_EINVAL;
+  }
+  return DPKEM_OK;
+}
+
+int dpkem_mixed_batch(dpkem_ctx *c, int form, size_t n, const dpkem_request *reqs, void *stream) {
+  if (!c) return set_status(DPKEM_EINVAL);
+  if (form == DPKEM_FORM_INT32) return set_status(DPKEM_EUNSUPPORTED);
+  if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC) return set_status(DPKEM_EINVAL);
+  if (n == 0) return set_status(DPKEM_OK);
+  int rc = check_requests(n, reqs);
+  if (rc) return set_status(rc);
+  std::lock_guard<std::mutex> lock(c->mu);
+  cudaSetDevice(c->device);
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  const mixed::Req *mr = reinterpret_cast<const mixed::Req *>(reqs);
+  const size_t need = mixed::plan_bytes(mr, n, nullptr);
+  if ((rc = ensure_arena(c, need)) != DPKEM_OK) return set_status(rc);
+  cudaError_t e = cudaStreamWaitEvent(st, c->last, 0);
+  int grid = 0;
+  if (e == cudaSuccess) e = mixed::kernel_setup(&grid);
+  std::vector<uint8_t> plan(mixed::plan_struct_bytes());
+  if (e == cudaSuccess)
+    e = mixed::plan_build(mr, n, form, grid, c->arena, c->arena_bytes, c->d_err, st, plan.data());
+  if (e == cudaSuccess) e = mixed::plan_launch(plan.data(), n, grid, st);
+  if (e == cudaSuccess) e = cudaEventRecord(c->last, st);
+  return set_status(cuda_status(e));
+}
+
+struct dpkem_graph {
+  dpkem_ctx *ctx = nullptr;
+  uint8_t *mem = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+int dpkem_mixed_graph_destroy(dpkem_graph *g) {
+  if (!g) return set_status(DPKEM_EINVAL);
+  if (g->ctx) cudaSetDevice(g->ctx->device);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  if (g->mem) {
+    cudaDeviceSynchronize();
+    cudaFree(g->mem);
+  }
+  delete g;
+  return set_status(DPKEM_OK);
+}
+
+int dpkem_mixed_graph_create(dpkem_ctx *c, int form, size_t n, const dpkem_request *reqs, dpkem_graph **out) {
+  if (!c || !out) return set_status(DPKEM_EINVAL);
+  *out = nullptr;
+  if (form == DPKEM_FORM_INT32) return set_status(DPKEM_EUNSUPPORTED);
+  if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC) return set_status(DPKEM_EINVAL);
+  int rc = check_requests(n, reqs);
+  if (rc) return set_status(rc);
+  std::lock_guard<std::mutex> lock(c->mu);
+  cudaSetDevice(c->device);
+  const mixed::Req *mr = reinterpret_cast<const mixed::Req *>(reqs);
+  const size_t need = mixed::plan_bytes(mr, n, nullptr);
+  dpkem_graph *g = new dpkem_graph();
+  g->ctx = c;
+  cudaError_t e = cudaMalloc(&g->mem, need);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete g;
+    return set_status(DPKEM_ENOMEM);
+  }
+  int grid = 0;
+  std::vector<uint8_t> plan(mixed::plan_struct_bytes());
+  cudaStream_t cap = nullptr;
+  e = mixed::kernel_setup(&grid);
+  if (e == cudaSuccess) e = mixed::plan_build(mr, n, form, grid, g->mem, need, c->d_err, c->stream, plan.data());
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaError_t le = mixed::plan_launch(plan.data(), n, grid, cap);
+    e = cudaStreamEndCapture(cap, &g->graph);
+    if (le != cudaSuccess) e = le;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  if (cap) cudaStreamDestroy(cap);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    dpkem_mixed_graph_destroy(g);
+    return set_status(DPKEM_ECUDA);
+  }
+  *out = g;
+  return set_status(DPKEM_OK);
+}
+
+int dpkem_mixed_graph_launch(dpkem_graph *g, void *stream) {
+  if (!g || !g->exec) return set_status(DPKEM_EINVAL);
+  dpkem_ctx *c = g->ctx;
+  std::lock_guard<std::mutex> lock(c->mu);
+  cudaSetDevice(c->device);
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  cudaError_t e = cudaGraphLaunch(g->exec, st);
+  if (e == cudaSuccess) e = cudaEventRecord(c->last, st);
+  return set_status(cuda_status(e));
 }
 
 int dpkem_coins(dpkem_ctx *c, size_t n, size_t len, uint64_t first, const char *tag, uint8_t *out, unsigned flags,

@@ -94,4 +94,19 @@ size_t saber_scratch_bytes(int level);
 cudaError_t coins_generate(const CoinsBatch &b, cudaStream_t st);
 cudaError_t probe_int_peaks(cudaStream_t st, double *int_ops_per_s, double *keccak_per_s);
 
+namespace mixed {
+struct Req {
+  int32_t scheme, op;
+  const uint8_t *in0, *in1;
+  uint8_t *out0, *out1;
+};
+size_t plan_bytes(const Req *reqs, size_t n, size_t *ntasks_out);
+size_t plan_struct_bytes();
+cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *arena, size_t arena_bytes,
+                       uint32_t *err, cudaStream_t st, void *plan_out);
+cudaError_t kernel_setup(int *grid);
+cudaError_t plan_launch(const void *plan, size_t n, int grid, cudaStream_t st);
+int slots_for_device();
+}  // namespace mixed
+
 }  // namespace dpkem

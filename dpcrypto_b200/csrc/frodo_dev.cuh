@@ -484,6 +484,8 @@ __device__ __forceinline__ bool sa_tc_cta(const Inst &v, uint8_t *smem, uint32_t
   };
   tc_fence_before();
   __syncthreads();
+  if (tid == 0 && ok && fin)  // all arrivals observed: the barrier memory may be reused by the next task
+    for (int q = 0; q < 8 * NST + 1; q++) mbar_inval(&bars[q]);
   diff |= finish_c<MODE>(v, sval, red);
   const int any = __syncthreads_or(diff != 0);
   if (MODE == OP_DEC && tid == 0) *v.fail = (uint32_t)any;

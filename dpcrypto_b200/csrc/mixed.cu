@@ -1,0 +1,490 @@
+// Persistent mixed-scheme, mixed-operation batch: one launch of 2 CTAs per SM that pull
+// tasks from a device work queue until it is empty.
+//
+// A request is one KEM operation (FrodoKEM-976 or Saber l = 2/3/4; keypair, encaps or
+// decaps) on caller device buffers.  Each operation is a short chain of stages (the same
+// per-instance / per-CTA routines the batched kernels use): thread-level stages (hash
+// chains, XOF prologues) run up to 256 instances per task, one per thread; CTA-level
+// stages (Frodo A-generation + product, Saber products, Frodo W) run one instance per
+// task.  The host orders the task list by simulating list scheduling on the GPU's CTA
+// slots (so every task is preceded by the tasks it depends on) and each task waits, with
+// a bounded spin, for its instances' previous stages through per-request stage counters
+// (release: __threadfence + atomicAdd; acquire: ld.acquire.gpu).
+//
+// This translation unit is compiled with -Xptxas -dlcm=cg: global loads bypass L1, because
+// L1 is not coherent within a launch and requests may share 128-byte lines that a later
+// stage of a neighbouring request is still writing.
+//
+// The reference has no equivalent: each of its operations is a fixed chain of launches
+// over a compile-time batch of one scheme (FrodoKEM976-GPU/src/cuda_kernel.cu,
+// SABER-GPU/src/cuda_kernel.cu).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <queue>
+#include <vector>
+
+#include "frodo_dev.cuh"
+#include "saber_dev.cuh"
+
+namespace dpkem {
+namespace mixed {
+namespace {
+
+// ---- stage codes: scheme * 64 + op * 16 + stage * 2 + form ----
+__host__ __device__ constexpr int code_of(int scheme, int op, int stage, int form) {
+  return scheme * 64 + op * 16 + stage * 2 + (form == FORM_TC ? 1 : 0);
+}
+__host__ __device__ constexpr int scheme_of(int code) { return code >> 6; }
+__host__ __device__ constexpr int op_of(int code) { return (code >> 4) & 3; }
+__host__ __device__ constexpr int stage_of(int code) { return (code >> 1) & 7; }
+__host__ __device__ constexpr bool tc_of(int code) { return code & 1; }
+
+// Stage kinds: 0 = thread (one instance per thread), 2 = thread with two roles
+// (Saber prologue: instance t on threads t and t + 128), 1 = CTA (one instance per task).
+enum Kind : int { K_THREAD = 0, K_CTA = 1, K_THREAD2 = 2 };
+
+__host__ __device__ constexpr int nstages(int scheme, int op) { return op == OP_DEC ? 4 : 3; }
+
+__host__ __device__ constexpr int kind_of(int scheme, int op, int stage) {
+  if (scheme == 0) {
+    if (op == OP_DEC) return stage == 0 || stage == 2 ? K_CTA : K_THREAD;
+    return stage == 1 ? K_CTA : K_THREAD;
+  }
+  if (op == OP_DEC) return stage == 1 ? K_THREAD2 : stage == 3 ? K_THREAD : K_CTA;
+  return stage == 0 ? K_THREAD2 : stage == 1 ? K_CTA : K_THREAD;
+}
+
+// Completed-role count an instance must show before `stage` may start.
+__host__ __device__ constexpr uint32_t threshold(int scheme, int op, int stage) {
+  uint32_t t = 0;
+  for (int s = 0; s < stage; s++) t += kind_of(scheme, op, s) == K_THREAD2 ? 2u : 1u;
+  return t;
+}
+
+// ---- per-request scratch records (256-byte multiples so no line is shared) ----
+constexpr size_t kFrodoRec = 31488;  // rw 31,360 | k 24 | mu 24 | fail 4
+constexpr size_t kFrodoK = frodo::RW * 2, kFrodoMu = kFrodoK + 24, kFrodoFail = kFrodoMu + 24;
+
+__host__ __device__ inline size_t saber_rec_bytes(int level) {
+  const size_t b = level == 2 ? sdev::Scr<2>::BYTES : level == 3 ? sdev::Scr<3>::BYTES : sdev::Scr<4>::BYTES;
+  return (b + 4 + 255) & ~(size_t)255;
+}
+
+struct DevReq {
+  int32_t scheme, op;
+  const uint8_t *in0, *in1;
+  uint8_t *out0, *out1;
+  uint8_t *scr;
+};
+
+struct Task {
+  uint16_t code;
+  uint16_t count;
+  uint32_t first;  // index into idx[]
+};
+
+struct Plan {
+  const DevReq *req;
+  const Task *tasks;
+  const uint32_t *idx;
+  uint32_t ntasks;
+  uint32_t *head;
+  uint32_t *done;
+  uint32_t *err;
+};
+
+__device__ __forceinline__ fdev::Inst frodo_view(const DevReq &r) {
+  fdev::Inst v{};
+  const bool kp = r.op == OP_KEYPAIR, enc = r.op == OP_ENC;
+  v.coins = kp || enc ? r.in0 : nullptr;
+  v.pk = kp ? r.out0 : enc ? const_cast<uint8_t *>(r.in1) : nullptr;
+  v.sk = kp ? r.out1 : enc ? nullptr : const_cast<uint8_t *>(r.in1);
+  v.ct = enc ? r.out0 : kp ? nullptr : const_cast<uint8_t *>(r.in0);
+  v.ss = enc ? r.out1 : kp ? nullptr : r.out0;
+  v.rw = reinterpret_cast<uint16_t *>(r.scr);
+  v.kk = r.scr + kFrodoK;
+  v.mu = r.scr + kFrodoMu;
+  v.fail = reinterpret_cast<uint32_t *>(r.scr + kFrodoFail);
+  return v;
+}
+
+template <int L>
+__device__ __forceinline__ sdev::Inst saber_view(const DevReq &r) {
+  sdev::Inst v{};
+  const bool kp = r.op == OP_KEYPAIR, enc = r.op == OP_ENC;
+  v.coins = kp || enc ? r.in0 : nullptr;
+  v.pk = kp ? r.out0 : enc ? const_cast<uint8_t *>(r.in1) : nullptr;
+  v.sk = kp ? r.out1 : enc ? nullptr : const_cast<uint8_t *>(r.in1);
+  v.ct = enc ? r.out0 : kp ? nullptr : const_cast<uint8_t *>(r.in0);
+  v.ss = enc ? r.out1 : kp ? nullptr : r.out0;
+  v.scr = r.scr;
+  v.fail = reinterpret_cast<uint32_t *>(r.scr + sdev::Scr<L>::BYTES);
+  return v;
+}
+
+// Wait limit for a dependency (a Frodo prologue task takes milliseconds; 20 s means broken).
+constexpr uint64_t kDepLimitNs = 20000000000ull;
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void wait_done(const Plan &p, uint32_t r, uint32_t need) {
+  if (ld_acquire(p.done + r) >= need) return;
+  const uint64_t t0 = globaltimer_ns();
+  while (ld_acquire(p.done + r) < need) {
+    __nanosleep(200);
+    if (globaltimer_ns() - t0 > kDepLimitNs) {
+      atomicOr(p.err, DEV_ERR_TIMEOUT);
+      return;
+    }
+  }
+}
+
+__device__ __forceinline__ void mark_done(const Plan &p, uint32_t r) {
+  __threadfence();
+  atomicAdd(p.done + r, 1u);
+}
+
+template <int L>
+__device__ __forceinline__ void saber_thread(int op, int stage, const DevReq &r, int role) {
+  const sdev::Inst v = saber_view<L>(r);
+  if (op == OP_KEYPAIR) {
+    if (stage == 0) sdev::prologue_inst<L, OP_KEYPAIR>(v, role);
+    else sdev::finish_inst<L, OP_KEYPAIR>(v);
+  } else if (op == OP_ENC) {
+    if (stage == 0) sdev::prologue_inst<L, OP_ENC>(v, role);
+    else sdev::finish_inst<L, OP_ENC>(v);
+  } else {
+    if (stage == 1) sdev::prologue_inst<L, OP_DEC>(v, role);
+    else sdev::finish_inst<L, OP_DEC>(v);
+  }
+}
+
+__device__ __forceinline__ void thread_stage(int code, const DevReq &r, int role) {
+  const int scheme = scheme_of(code), op = op_of(code), stage = stage_of(code);
+  if (scheme == 0) {
+    const fdev::Inst v = frodo_view(r);
+    if (op == OP_KEYPAIR) {
+      if (stage == 0) fdev::kp_prologue_inst(v);
+      else fdev::pk_hash_inst(v);
+    } else if (op == OP_ENC) {
+      if (stage == 0) fdev::prologue_inst<OP_ENC>(v);
+      else fdev::ss_inst<OP_ENC>(v);
+    } else {
+      if (stage == 1) fdev::prologue_inst<OP_DEC>(v);
+      else fdev::ss_inst<OP_DEC>(v);
+    }
+  } else if (scheme == 2) {
+    saber_thread<2>(op, stage, r, role);
+  } else if (scheme == 3) {
+    saber_thread<3>(op, stage, r, role);
+  } else {
+    saber_thread<4>(op, stage, r, role);
+  }
+}
+
+template <int L, int MODE>
+__device__ __forceinline__ void saber_product(bool tc, const sdev::Inst &v, uint8_t *smem, uint32_t tbase,
+                                              uint32_t *err) {
+  if (tc) sdev::product_tc_cta<L, MODE>(v, smem, tbase, err);
+  else sdev::product_dp4a_cta<L, MODE>(v, smem);
+}
+
+template <int L>
+__device__ __forceinline__ void saber_cta(int op, int stage, bool tc, const DevReq &r, uint8_t *smem, uint32_t tbase,
+                                          uint32_t *err) {
+  const sdev::Inst v = saber_view<L>(r);
+  if (op == OP_KEYPAIR) saber_product<L, sdev::PM_KEYPAIR>(tc, v, smem, tbase, err);
+  else if (op == OP_ENC) saber_product<L, sdev::PM_ENC>(tc, v, smem, tbase, err);
+  else if (stage == 0) saber_product<L, sdev::PM_DEC_INNER>(tc, v, smem, tbase, err);
+  else saber_product<L, sdev::PM_DEC_CMP>(tc, v, smem, tbase, err);
+}
+
+constexpr int kTcStages = 2;
+
+__device__ __forceinline__ void cta_stage(int code, const DevReq &r, uint8_t *smem, uint32_t tbase, uint32_t *err) {
+  const int scheme = scheme_of(code), op = op_of(code), stage = stage_of(code);
+  const bool tc = tc_of(code);
+  if (scheme == 0) {
+    const fdev::Inst v = frodo_view(r);
+    if (op == OP_KEYPAIR) {
+      fdev::kp_as_dp4a_cta(v, smem);
+    } else if (op == OP_ENC) {
+      if (tc) fdev::sa_tc_cta<OP_ENC, kTcStages>(v, smem, tbase, err);
+      else fdev::sa_dp4a_cta<OP_ENC>(v, smem);
+    } else if (stage == 0) {
+      fdev::dec_w_cta(v, smem);
+    } else {
+      if (tc) fdev::sa_tc_cta<OP_DEC, kTcStages>(v, smem, tbase, err);
+      else fdev::sa_dp4a_cta<OP_DEC>(v, smem);
+    }
+  } else if (scheme == 2) {
+    saber_cta<2>(op, stage, tc, r, smem, tbase, err);
+  } else if (scheme == 3) {
+    saber_cta<3>(op, stage, tc, r, smem, tbase, err);
+  } else {
+    saber_cta<4>(op, stage, tc, r, smem, tbase, err);
+  }
+}
+
+constexpr int kSmem = std::max({fdev::TcLayout<kTcStages>::total, fdev::DP4A_SMEM, fdev::DEC_W_SMEM,
+                                fdev::KP_AS_SMEM, sdev::PL<4>::TC_TOTAL, sdev::PL<3>::TC_TOTAL,
+                                sdev::PL<2>::TC_TOTAL});
+
+__global__ void __launch_bounds__(256, 2) mixed_kernel(Plan p) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint32_t s_task, s_tmem;
+  const int tid = threadIdx.x;
+  if (tid < 32) {
+    tmem_alloc(&s_tmem, fdev::TC_TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = s_tmem;
+  while (true) {
+    if (tid == 0) s_task = atomicAdd(p.head, 1u);
+    __syncthreads();
+    const uint32_t t = s_task;
+    __syncthreads();
+    if (t >= p.ntasks) break;
+    const Task tk = p.tasks[t];
+    const int code = tk.code, scheme = scheme_of(code), op = op_of(code), stage = stage_of(code);
+    const int kind = kind_of(scheme, op, stage);
+    const uint32_t need = threshold(scheme, op, stage);
+    if (kind == K_CTA) {
+      const uint32_t r = p.idx[tk.first];
+      if (tid == 0) wait_done(p, r, need);
+      __syncthreads();
+      cta_stage(code, p.req[r], smem, tbase, p.err);
+      __syncthreads();
+      if (tid == 0) mark_done(p, r);
+    } else {
+      const int per = kind == K_THREAD2 ? 128 : 256;
+      const int slot = tid % per, role = tid / per;
+      if (slot < tk.count) {
+        const uint32_t r = p.idx[tk.first + slot];
+        wait_done(p, r, need);
+        thread_stage(code, p.req[r], role);
+        mark_done(p, r);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (tid < 32) {
+    tc_fence_after();
+    tmem_dealloc(tbase, fdev::TC_TMEM_COLS);
+  }
+}
+
+// ---------------------------------------------------------------- host: task list
+// Estimated CTA-slot time of each stage (microseconds), used only to order tasks.
+double est_us(int scheme, int op, int stage, int count) {
+  const int kind = kind_of(scheme, op, stage);
+  if (scheme == 0) {
+    if (kind == K_CTA) return op == OP_DEC && stage == 0 ? 30.0 : 1700.0;
+    const bool prologue = (op == OP_DEC) ? stage == 1 : stage == 0;
+    if (!prologue) return 900.0;
+    return op == OP_ENC ? 3200.0 : op == OP_DEC ? 2400.0 : 2200.0;
+  }
+  if (kind == K_CTA) return 60.0;
+  if (kind == K_THREAD2) return 250.0;
+  (void)count;
+  return 120.0;
+}
+
+struct HostTask {
+  Task t;
+  double dur, ready = 0;
+  int pending = 0;
+  std::vector<int> dependents;
+  int prio;
+};
+
+}  // namespace
+
+// Bytes of device memory a plan for these requests needs (tables + scratch records).
+size_t plan_bytes(const Req *reqs, size_t n, size_t *ntasks_out) {
+  size_t scr = 0, ntasks = 0, nidx = 0;
+  size_t counts[5][3] = {};
+  for (size_t i = 0; i < n; i++) {
+    scr += reqs[i].scheme == 0 ? kFrodoRec : saber_rec_bytes(reqs[i].scheme);
+    counts[reqs[i].scheme][reqs[i].op]++;
+  }
+  for (int s = 0; s < 5; s++)
+    for (int op = 0; op < 3; op++) {
+      const size_t c = counts[s][op];
+      if (!c || s == 1) continue;
+      for (int st = 0; st < nstages(s, op); st++) {
+        const int kind = kind_of(s, op, st);
+        ntasks += kind == K_CTA ? c : (c + (kind == K_THREAD2 ? 127 : 255)) / (kind == K_THREAD2 ? 128 : 256);
+        nidx += c;
+      }
+    }
+  if (ntasks_out) *ntasks_out = ntasks;
+  auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  return up(n * sizeof(DevReq)) + up(ntasks * sizeof(Task)) + up(nidx * 4) + up(n * 4) + 256 + scr;
+}
+
+// Builds the plan in host memory, uploads it into `arena` and returns the launch descriptor.
+cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *arena, size_t arena_bytes,
+                       uint32_t *err, cudaStream_t st, void *plan_out) {
+  size_t ntasks = 0;
+  const size_t need = plan_bytes(reqs, n, &ntasks);
+  if (need > arena_bytes) return cudaErrorMemoryAllocation;
+  auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  uint8_t *d_req = arena;
+  uint8_t *d_tasks = d_req + up(n * sizeof(DevReq));
+  uint8_t *d_idx = d_tasks + up(ntasks * sizeof(Task));
+  // idx size = sum over groups and stages of c
+  size_t nidx = 0;
+  std::vector<std::vector<uint32_t>> groups(5 * 3);
+  for (size_t i = 0; i < n; i++) groups[reqs[i].scheme * 3 + reqs[i].op].push_back((uint32_t)i);
+  for (int g = 0; g < 15; g++)
+    if (!groups[g].empty()) nidx += groups[g].size() * nstages(g / 3, g % 3);
+  uint8_t *d_done = d_idx + up(nidx * 4);
+  uint8_t *d_head = d_done + up(n * 4);
+  uint8_t *d_scr = d_head + 256;
+
+  std::vector<DevReq> hreq(n);
+  size_t off = 0;
+  for (size_t i = 0; i < n; i++) {
+    const Req &r = reqs[i];
+    hreq[i] = DevReq{r.scheme, r.op, r.in0, r.in1, r.out0, r.out1, d_scr + off};
+    off += r.scheme == 0 ? kFrodoRec : saber_rec_bytes(r.scheme);
+  }
+  // Tasks per group and stage, with dependencies on the previous stage's tasks.
+  std::vector<HostTask> ht;
+  std::vector<uint32_t> idx;
+  idx.reserve(nidx);
+  for (int g = 0; g < 15; g++) {
+    const std::vector<uint32_t> &R = groups[g];
+    if (R.empty()) continue;
+    const int scheme = g / 3, op = g % 3;
+    std::vector<int> owner_prev(R.size(), -1);  // task index of each instance's previous stage
+    for (int stg = 0; stg < nstages(scheme, op); stg++) {
+      const int kind = kind_of(scheme, op, stg);
+      const int per = kind == K_CTA ? 1 : kind == K_THREAD2 ? 128 : 256;
+      const uint32_t base = (uint32_t)idx.size();
+      idx.insert(idx.end(), R.begin(), R.end());
+      std::vector<int> owner(R.size());
+      for (size_t a = 0; a < R.size(); a += per) {
+        const int cnt = (int)std::min<size_t>(per, R.size() - a);
+        HostTask t;
+        t.t = Task{(uint16_t)code_of(scheme, op, stg, form), (uint16_t)cnt, base + (uint32_t)a};
+        t.dur = est_us(scheme, op, stg, cnt);
+        t.prio = kind == K_CTA ? (t.dur > 500 ? 2 : 1) : 0;  // latency-bound thread stages first
+        const int id = (int)ht.size();
+        std::vector<int> deps;
+        for (int k = 0; k < cnt; k++) {
+          owner[a + k] = id;
+          if (owner_prev[a + k] >= 0) deps.push_back(owner_prev[a + k]);
+        }
+        std::sort(deps.begin(), deps.end());
+        deps.erase(std::unique(deps.begin(), deps.end()), deps.end());
+        t.pending = (int)deps.size();
+        ht.push_back(t);
+        for (int d : deps) ht[d].dependents.push_back(id);
+      }
+      owner_prev = owner;
+    }
+  }
+  // List scheduling on `slots` CTA slots: the fetch order is the simulated start order.
+  // `waiting` holds tasks whose dependencies are scheduled, keyed by ready time; `ready`
+  // holds those whose ready time has passed, keyed by priority then creation order.
+  struct ByReady {
+    double ready;
+    int id;
+    bool operator>(const ByReady &o) const { return ready != o.ready ? ready > o.ready : id > o.id; }
+  };
+  struct ByPrio {
+    int prio, id;
+    bool operator>(const ByPrio &o) const { return prio != o.prio ? prio > o.prio : id > o.id; }
+  };
+  std::priority_queue<ByReady, std::vector<ByReady>, std::greater<ByReady>> waiting;
+  std::priority_queue<ByPrio, std::vector<ByPrio>, std::greater<ByPrio>> ready;
+  std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
+  for (int s = 0; s < std::max(1, slots); s++) free_at.push(0.0);
+  for (size_t i = 0; i < ht.size(); i++)
+    if (ht[i].pending == 0) waiting.push({0.0, (int)i});
+  std::vector<Task> order;
+  order.reserve(ht.size());
+  while (!waiting.empty() || !ready.empty()) {
+    const double w = free_at.top();
+    free_at.pop();
+    while (!waiting.empty() && waiting.top().ready <= w) {
+      ready.push({ht[waiting.top().id].prio, waiting.top().id});
+      waiting.pop();
+    }
+    int id;
+    if (!ready.empty()) {
+      id = ready.top().id;
+      ready.pop();
+    } else {
+      id = waiting.top().id;
+      waiting.pop();
+    }
+    const double start = std::max(w, ht[id].ready), fin = start + ht[id].dur;
+    free_at.push(fin);
+    order.push_back(ht[id].t);
+    for (int d : ht[id].dependents) {
+      ht[d].ready = std::max(ht[d].ready, fin);
+      if (--ht[d].pending == 0) waiting.push({ht[d].ready, d});
+    }
+  }
+  if (order.size() != ntasks) return cudaErrorInvalidValue;
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(d_req, hreq.data(), n * sizeof(DevReq), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(d_tasks, order.data(), ntasks * sizeof(Task), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return e;
+  if ((e = cudaMemcpyAsync(d_idx, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+  // Pageable sources: make sure the copies have consumed them before the vectors go away.
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  Plan *p = static_cast<Plan *>(plan_out);
+  *p = Plan{reinterpret_cast<const DevReq *>(d_req), reinterpret_cast<const Task *>(d_tasks),
+            reinterpret_cast<const uint32_t *>(d_idx), (uint32_t)ntasks, reinterpret_cast<uint32_t *>(d_head),
+            reinterpret_cast<uint32_t *>(d_done), err};
+  return cudaSuccess;
+}
+
+size_t plan_struct_bytes() { return sizeof(Plan); }
+
+// Grid of the persistent kernel (2 CTAs per SM when they fit); sets its shared-memory limit.
+// Call outside stream capture.
+cudaError_t kernel_setup(int *grid) {
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem)) != cudaSuccess)
+    return e;
+  int dev = 0, sms = 0, occ = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mixed_kernel, 256, kSmem);
+  *grid = std::max(1, sms * std::max(1, std::min(occ, 2)));
+  return cudaSuccess;
+}
+
+// Reset the queue and stage counters, then launch the persistent kernel (capturable).
+cudaError_t plan_launch(const void *plan, size_t n, int grid, cudaStream_t st) {
+  const Plan &p = *static_cast<const Plan *>(plan);
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(p.done, 0, n * 4, st)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(p.head, 0, 4, st)) != cudaSuccess) return e;
+  mixed_kernel<<<grid, 256, kSmem, st>>>(p);
+  return cudaGetLastError();
+}
+
+int slots_for_device() {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return 2 * sms;
+}
+
+}  // namespace mixed
+}  // namespace dpkem

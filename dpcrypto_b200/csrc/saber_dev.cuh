@@ -537,6 +537,7 @@ __device__ __forceinline__ bool product_tc_cta(const Inst &v, uint8_t *sm, uint3
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
+  if (tid == 0 && ok) mbar_inval(bar);
   epilogue<L, MODE>(v, sm);
   __syncthreads();
   return ok;

@@ -27,6 +27,13 @@ FORM_DP4A, FORM_INT32, FORM_TC = 0, 1, 2
 FLAG_DEVICE_PTRS = 1
 OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, EUNSUPPORTED = 0, -1, -2, -3, -4, -5
 
+class Request(ctypes.Structure):
+    """dpkem_request: one operation of a mixed batch (device buffers, batched-call order)."""
+
+    _fields_ = [("scheme", ctypes.c_int32), ("op", ctypes.c_int32), ("in0", ctypes.c_void_p),
+                ("in1", ctypes.c_void_p), ("out0", ctypes.c_void_p), ("out1", ctypes.c_void_p)]
+
+
 EXPORTS = {
     "dpkem_ctx_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_size_t]),
     "dpkem_ctx_destroy": (ctypes.c_int, [ctypes.c_void_p]),
@@ -44,6 +51,12 @@ EXPORTS = {
     "dpkem_coins": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_uint64,
                                    ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]),
     "dpkem_sync": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "dpkem_mixed_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
+                                         ctypes.c_void_p]),
+    "dpkem_mixed_graph_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
+                                                ctypes.POINTER(ctypes.c_void_p)]),
+    "dpkem_mixed_graph_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "dpkem_mixed_graph_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "dpkem_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "dpkem_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
     "dpkem_probe_int_peaks": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
@@ -226,8 +239,65 @@ class Engine:
         self._check(self._lib.dpkem_probe_int_peaks(self._h, ctypes.byref(a), ctypes.byref(b)), "probe")
         return a.value, b.value
 
+    # -- mixed batches ---------------------------------------------------------
+    @staticmethod
+    def requests(items):
+        """items: iterable of (scheme, op, in0, in1, out0, out1) with torch CUDA tensors (or None)."""
+        items = list(items)
+        arr = (Request * len(items))()
+        for k, (scheme, op, a, b, c, e) in enumerate(items):
+            ptr = lambda t: t.data_ptr() if t is not None else None  # noqa: E731
+            arr[k] = Request(scheme, op, ptr(a), ptr(b), ptr(c), ptr(e))
+        return arr
+
+    def mixed(self, items, form: int = FORM_TC):
+        """Run a mixed-scheme, mixed-operation batch as one persistent launch (device buffers)."""
+        import torch
+
+        arr = self.requests(items)
+        st = torch.cuda.current_stream().cuda_stream or 1
+        self._check(self._lib.dpkem_mixed_batch(self._h, form, len(arr), ctypes.cast(arr, ctypes.c_void_p),
+                                                ctypes.c_void_p(st)), "mixed_batch")
+
+    def mixed_graph(self, items, form: int = FORM_TC) -> "MixedGraph":
+        return MixedGraph(self, items, form)
+
     def max_chunk(self, scheme: int) -> int:
         return int(self._lib.dpkem_max_chunk(self._h, scheme))
+
+
+class MixedGraph:
+    """A mixed batch captured once as a CUDA graph; launch() replays it on the torch stream."""
+
+    def __init__(self, engine: Engine, items, form: int = FORM_TC):
+        self._lib = engine._lib
+        self._engine = engine
+        arr = engine.requests(items)
+        h = ctypes.c_void_p()
+        rc = self._lib.dpkem_mixed_graph_create(engine._h, form, len(arr), ctypes.cast(arr, ctypes.c_void_p),
+                                                ctypes.byref(h))
+        if rc != OK:
+            raise DpkemError(rc, "mixed_graph_create")
+        self._h = h
+
+    def launch(self):
+        import torch
+
+        st = torch.cuda.current_stream().cuda_stream or 1
+        rc = self._lib.dpkem_mixed_graph_launch(self._h, ctypes.c_void_p(st))
+        if rc != OK:
+            raise DpkemError(rc, "mixed_graph_launch")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.dpkem_mixed_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---- reference-named entry points (batch from set_compat_batch, default 768) ----

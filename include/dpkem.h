@@ -49,7 +49,7 @@ enum { DPKEM_FRODO976 = 0, DPKEM_LIGHTSABER = 2, DPKEM_SABER = 3, DPKEM_FIRESABE
 enum { DPKEM_FORM_DP4A = 0, DPKEM_FORM_INT32 = 1, DPKEM_FORM_TC = 2 };
 
 /* Flags. */
-#define DPKEM_FLAG_DEVICE_PTRS 1u /* all buffers are device pointers (16-byte aligned); call is async */
+#define DPKEM_FLAG_DEVICE_PTRS 1u /* all buffers are device pointers (pk/ct arrays 16-byte, others 8-byte aligned); call is async */
 
 typedef struct dpkem_ctx dpkem_ctx;
 
@@ -74,6 +74,31 @@ int dpkem_enc_batch(dpkem_ctx *ctx, int scheme, int form, size_t n, const uint8_
                     uint8_t *ct, uint8_t *ss, unsigned flags, void *stream);
 int dpkem_dec_batch(dpkem_ctx *ctx, int scheme, int form, size_t n, const uint8_t *ct, const uint8_t *sk,
                     uint8_t *ss, unsigned flags, void *stream);
+
+/* ---- Mixed batches: one persistent launch over mixed schemes and operations ----
+ * Each request names a scheme, an operation and its device buffers (pk/ct 16-byte, others 8-byte aligned),
+ * in the argument order of the batched calls:
+ *   keypair: in0 = coins, out0 = pk, out1 = sk
+ *   encaps:  in0 = coins, in1 = pk, out0 = ct, out1 = ss
+ *   decaps:  in0 = ct,    in1 = sk, out0 = ss
+ * The requests run as one launch of persistent CTAs that pull stage tasks from a device
+ * work queue; results equal those of the batched calls on the same inputs.  No
+ * counterpart in the reference (one scheme per compiled program, fixed launch chains). */
+typedef struct {
+  int32_t scheme; /* DPKEM_FRODO976 / DPKEM_LIGHTSABER / DPKEM_SABER / DPKEM_FIRESABER */
+  int32_t op;     /* 0 keypair, 1 encaps, 2 decaps */
+  const uint8_t *in0, *in1;
+  uint8_t *out0, *out1;
+} dpkem_request;
+
+/* Enqueue on `stream` (NULL = context stream); dpkem_sync() reports device-side errors. */
+int dpkem_mixed_batch(dpkem_ctx *ctx, int form, size_t n, const dpkem_request *reqs, void *stream);
+
+/* The same batch captured once as a CUDA graph (its own device memory) and replayed. */
+typedef struct dpkem_graph dpkem_graph;
+int dpkem_mixed_graph_create(dpkem_ctx *ctx, int form, size_t n, const dpkem_request *reqs, dpkem_graph **out);
+int dpkem_mixed_graph_launch(dpkem_graph *g, void *stream);
+int dpkem_mixed_graph_destroy(dpkem_graph *g);
 
 /* Seeded synthetic coins: out[i] = SHAKE256(00 01 .. 1F || LE64(first + i) || tag, len), len <= 136,
  * strlen(tag) <= 16.  Same flag semantics as the batched operations. */
