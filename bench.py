@@ -327,6 +327,57 @@ def main():
         sres["tc_over_dp4a"] = sres["tc"] / sres["dp4a"]
         line["saber_l3_batch4096"] = dict(sres, unit=UNIT)
 
+    # ---- mixed persistent batch: 16384 requests, 4 schemes x 3 ops, one CUDA-graph launch ----
+    if not args.no_secondary:
+        from dpcrypto_b200.workloads import MixedBatch
+
+        mb = MixedBatch(eng, 16384, seed=0, first=rank * 1000000)
+        mres = {"requests": mb.n, "unit": "KEM ops/s", "counts": mb.counts}
+        for name, f in (("tc", d.FORM_TC), ("dp4a", d.FORM_DP4A)):
+            g = eng.mixed_graph(mb.items, f)
+            for _ in range(2):
+                g.launch()
+            barrier()
+            reps = 3
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for _ in range(reps):
+                g.launch()
+            t1.record(stream)
+            barrier()
+            mres[name] = mb.n * reps / (t0.elapsed_time(t1) * 1e-3)
+            mres[name + "_ms_per_launch"] = t0.elapsed_time(t1) / reps
+            eng.sync()
+            mres[name + "_bit_exact"] = mb.check()
+            mb.clear()
+            g.close()
+        # the same requests as separate batched calls per (scheme, op), for comparison
+        line["mixed_16384"] = mres
+
+    # ---- serving loop: Poisson arrivals, 60 % encaps / 40 % decaps, 50/50 Frodo / Saber l=3 ----
+    if not args.no_secondary and world == 1:
+        from dpcrypto_b200.serving import RequestPool, Server, poisson_arrivals
+
+        pool = RequestPool(eng, 16384, seed=0)
+        serving = {"requests_per_level": pool.n, "mix": "60% encaps / 40% decaps, 50/50 FrodoKEM-976 / Saber l=3",
+                   "slots": 4, "max_batch": 4096, "unit": "KEM ops/s"}
+        for name, f in (("tc", d.FORM_TC), ("dp4a", d.FORM_DP4A)):
+            srv = Server(slots=4, max_batch=4096, form=f)
+            try:
+                srv.run(pool, np.zeros(2048))  # warm-up
+                peak = srv.run(pool, np.zeros(pool.n))["ops_per_s"]
+                levels = []
+                for frac in (0.1, 0.25, 0.5, 0.75, 1.0):
+                    pool.clear()
+                    r = srv.run(pool, poisson_arrivals(pool.n, rate=frac * peak, seed=int(frac * 100)))
+                    levels.append({"load": frac, "offered_per_s": frac * peak, "ops_per_s": r["ops_per_s"],
+                                   "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "mean_batch": r["mean_batch"]})
+                torch.cuda.synchronize()
+                serving[name] = {"peak_ops_per_s": peak, "levels": levels, "bit_exact": pool.check()}
+            finally:
+                srv.close()
+        line["serving"] = serving
+
     # ---- end to end through the public API with pinned host buffers ----
     if not args.no_e2e:
         pin = lambda t: t.cpu().pin_memory().numpy()  # noqa: E731

@@ -123,8 +123,10 @@ __device__ __forceinline__ sdev::Inst saber_view(const DevReq &r) {
   return v;
 }
 
-// Wait limit for a dependency (a Frodo prologue task takes milliseconds; 20 s means broken).
-constexpr uint64_t kDepLimitNs = 20000000000ull;
+// Wait limit for a dependency: a dependency was fetched earlier and is running, so a
+// healthy wait is at most one task (milliseconds).  After any error every wait returns at
+// once, so a broken plan drains instead of accumulating timeouts.
+constexpr uint64_t kDepLimitNs = 2000000000ull;
 
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
   uint32_t v;
@@ -136,6 +138,7 @@ __device__ __forceinline__ void wait_done(const Plan &p, uint32_t r, uint32_t ne
   if (ld_acquire(p.done + r) >= need) return;
   const uint64_t t0 = globaltimer_ns();
   while (ld_acquire(p.done + r) < need) {
+    if (ld_acquire(p.err) != 0) return;
     __nanosleep(200);
     if (globaltimer_ns() - t0 > kDepLimitNs) {
       atomicOr(p.err, DEV_ERR_TIMEOUT);

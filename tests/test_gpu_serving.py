@@ -1,0 +1,23 @@
+"""Continuous-batching serving loop: requests arriving while others run are batched onto free
+slots and overlap on the device; every result equals the one computed alone (batched call)."""
+import numpy as np
+import pytest
+import torch
+
+import dpcrypto_b200 as d
+from dpcrypto_b200.serving import RequestPool, Server, poisson_arrivals
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("form", [d.FORM_TC, d.FORM_DP4A])
+def test_serving_results_equal_alone(engine, form):
+    pool = RequestPool(engine, 700, seed=3)
+    srv = Server(slots=3, max_batch=128, form=form, hbm_budget=256 << 20)
+    try:
+        res = srv.run(pool, poisson_arrivals(pool.n, rate=20000.0, seed=1))
+    finally:
+        srv.close()
+    torch.cuda.synchronize()
+    assert pool.check()
+    assert res["batches"] > 1 and np.isfinite(res["latency_ms"]).all() and (res["latency_ms"] > 0).all()
