@@ -71,6 +71,26 @@ __global__ void __launch_bounds__(256, 2) kp_as_dp4a_kernel(FrodoBatch b) {
   fdev::kp_as_dp4a_cta(inst_of(b, blockIdx.x, OP_KEYPAIR), smem);
 }
 
+__global__ void __launch_bounds__(256, 2) kp_as_tc_kernel(FrodoBatch b) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint32_t tslot;
+  if (threadIdx.x < 32) {
+    tmem_alloc(&tslot, 64);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = tslot;
+  fdev::kp_as_tc_cta(inst_of(b, blockIdx.x, OP_KEYPAIR), smem, tbase, b.err);
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    tc_fence_after();
+    tmem_dealloc(tbase, 64);
+  }
+}
+
 inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
 
 template <typename K>
@@ -102,11 +122,16 @@ inline void mark(const FrodoBatch &b, cudaStream_t st) {
 
 cudaError_t frodo_keypair(const FrodoBatch &b, int form, cudaStream_t st) {
   if (b.n <= 0) return cudaSuccess;
-  (void)form;
   mark(b, st);
   kp_prologue_kernel<OP_KEYPAIR><<<blocks_for(b.n, 64), 64, 0, st>>>(b);
   mark(b, st);
-  kp_as_dp4a_kernel<<<b.n, 256, fdev::KP_AS_SMEM, st>>>(b);
+  if (form == FORM_TC) {
+    cudaError_t e = set_smem(kp_as_tc_kernel, fdev::KptLayout::total);
+    if (e != cudaSuccess) return e;
+    kp_as_tc_kernel<<<b.n, 256, fdev::KptLayout::total, st>>>(b);
+  } else {
+    kp_as_dp4a_kernel<<<b.n, 256, fdev::KP_AS_SMEM, st>>>(b);
+  }
   mark(b, st);
   pk_hash_kernel<OP_KEYPAIR><<<blocks_for(b.n, 64), 64, 0, st>>>(b);
   mark(b, st);

@@ -541,5 +541,139 @@ __device__ __forceinline__ void kp_as_dp4a_cta(const Inst &v, uint8_t *smem) {
   __syncthreads();
 }
 
+
+// ---------------------------------------------------------------- B = A S + E (keypair), tcgen05 form
+// GEMM view: D[i][k] = sum_j limb(A[i][j]) S^T[k][j], M = 128 rows of A per tile (a
+// warpgroup, thread = row), N = 8, K = the 84 columns of one squeeze block padded to 96
+// (3 K steps; S^T is zero-padded so the pad bytes contribute nothing).  A limb tiles are
+// K-major (row i contiguous along K, as the sponge squeezes it): byte (i, kk) at
+// (i/8)*768 + (kk/16)*128 + (i%8)*16 + kk%16.  S^T per block is the K-major B operand:
+// byte (kk, k) at (kk/16)*128 + k*16 + kk%16.  The two warpgroups take M tiles g, g+2, g+4,
+// g+6 (tile 7 holds rows 896..1023; rows >= 976 are computed and discarded); each has its
+// own 2-stage ring, TMEM columns [32g, 32g+16) and named barrier 1+g.
+constexpr int KPT_ST_BLK = 6 * 128;                // S^T operand per block (96 K bytes x 8 rows)
+constexpr int KPT_PLANE = 16 * 768;                // one limb plane of a 128-row tile
+constexpr int KPT_STAGE = 2 * KPT_PLANE;
+constexpr int KPT_NST = 2;
+struct KptLayout {
+  static constexpr int st = 0;
+  static constexpr int ring = 12 * KPT_ST_BLK;                       // 9216
+  static constexpr int bars = ring + 2 * KPT_NST * KPT_STAGE;        // per warpgroup: NST stage + 1 tile
+  static constexpr int total = bars + 2 * (KPT_NST + 1) * 8;
+};
+
+__device__ __forceinline__ void wg_sync(int g) {
+  asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory");
+}
+
+// TMEM columns [tbase, tbase + 48) must be allocated by the caller.
+__device__ __forceinline__ bool kp_as_tc_cta(const Inst &v, uint8_t *smem, uint32_t tbase, uint32_t *err) {
+  using L = KptLayout;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = warp >> 2, l = tid & 127;
+  uint8_t *stop = smem + L::st;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bars) + g * (KPT_NST + 1);
+  const uint16_t *rw = v.rw;
+  // S^T operand of every block, zero-padded to 96 columns.
+  for (int x = tid; x < 12 * 8 * 6; x += 256) {
+    const int blk = x / 48, k = (x / 6) % 8, q = x % 6;
+    uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int c = 0; c < 16; c++) {
+      const int kk = 16 * q + c, j = 84 * blk + kk;
+      const uint32_t sv = (kk < 84 && j < N) ? (uint32_t)(rw[k * N + j] & 0xFFu) : 0u;
+      w[c >> 2] |= sv << (8 * (c & 3));
+    }
+    *reinterpret_cast<uint4 *>(stop + blk * KPT_ST_BLK + q * 128 + k * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+  if (l == 0) {
+    for (int q = 0; q < KPT_NST + 1; q++) mbar_init(&bars[q], 1);
+    fence_mbar_init();
+  }
+  const uint2 sa0 = ld_lane(v.pk), sa1 = ld_lane(v.pk + 8);
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+
+  constexpr uint32_t idesc = idesc_i8(128, 8, false, true, false, false);
+  const uint32_t st_addr = smem_u32(stop);
+  uint8_t *ring = smem + L::ring + g * KPT_NST * KPT_STAGE;
+  const uint32_t tcol = tbase + 32 * g;
+  const int roff = (l >> 3) * 768 + (l & 7) * 16;
+  bool ok = true;
+  uint32_t u = 0, tiles = 0;
+  for (int t = g; t < 8; t += 2, tiles++) {
+    const int i = 128 * t + l;
+    uint2 a[25];
+    row_init(a, i, sa0, sa1);
+    for (int blk = 0; blk < 12; blk++, u++) {
+      keccak_f1600(a);
+      uint32_t lo[21], hi[21];
+#pragma unroll
+      for (int q = 0; q < 21; q++) {
+        lo[q] = prmt(a[q].x, a[q].y, 0x6420);
+        hi[q] = prmt(a[q].x, a[q].y, 0x7531);
+      }
+      const int s = u % KPT_NST;
+      if (u >= KPT_NST && ok) ok = mbar_wait(&bars[s], ((u / KPT_NST) - 1) & 1);
+      uint8_t *stg = ring + s * KPT_STAGE;
+#pragma unroll
+      for (int q = 0; q < 5; q++) {
+        *reinterpret_cast<uint4 *>(stg + roff + q * 128) = make_uint4(lo[4 * q], lo[4 * q + 1], lo[4 * q + 2], lo[4 * q + 3]);
+        *reinterpret_cast<uint4 *>(stg + KPT_PLANE + roff + q * 128) =
+            make_uint4(hi[4 * q], hi[4 * q + 1], hi[4 * q + 2], hi[4 * q + 3]);
+      }
+      *reinterpret_cast<uint4 *>(stg + roff + 5 * 128) = make_uint4(lo[20], 0u, 0u, 0u);
+      *reinterpret_cast<uint4 *>(stg + KPT_PLANE + roff + 5 * 128) = make_uint4(hi[20], 0u, 0u, 0u);
+      fence_proxy_async_smem();
+      wg_sync(g);
+      if (l == 0 && ok) {
+        tc_fence_after();
+        const uint32_t sa = smem_u32(stg);
+#pragma unroll
+        for (int ks = 0; ks < 3; ks++) {
+          const uint64_t bd = sdesc(st_addr + blk * KPT_ST_BLK + ks * 256, 128, 1024);
+          const uint32_t acc = (blk | ks) ? 1u : 0u;
+          mma_i8(tcol, sdesc(sa + ks * 256, 128, 768), bd, idesc, acc);
+          mma_i8(tcol + 8, sdesc(sa + KPT_PLANE + ks * 256, 128, 768), bd, idesc, acc);
+        }
+        mma_commit(&bars[s]);
+      }
+    }
+    if (l == 0) mma_commit(&bars[KPT_NST]);
+    const bool fin = mbar_wait(&bars[KPT_NST], tiles & 1);
+    if (!fin) ok = false;
+    tc_fence_after();
+    uint32_t r[16];
+    tmem_ld16(tcol + ((uint32_t)((warp & 3) * 32) << 16), r);
+    tmem_wait_ld();
+    if (i < N) {
+      uint32_t x[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) x[k] = r[k] + (r[8 + k] << 8) + rw[N * NBAR + NBAR * i + k];
+      const uint2 o0 = make_uint2(bswap16x2(x[0], x[1]), bswap16x2(x[2], x[3]));
+      const uint2 o1 = make_uint2(bswap16x2(x[4], x[5]), bswap16x2(x[6], x[7]));
+      *reinterpret_cast<uint2 *>(v.pk + SEEDA + 16 * i) = o0;
+      *reinterpret_cast<uint2 *>(v.pk + SEEDA + 16 * i + 8) = o1;
+      *reinterpret_cast<uint2 *>(v.sk + LENS + SEEDA + 16 * i) = o0;
+      *reinterpret_cast<uint2 *>(v.sk + LENS + SEEDA + 16 * i + 8) = o1;
+    }
+    tc_fence_before();
+    wg_sync(g);  // TMEM read before the next tile overwrites the accumulators
+    tc_fence_after();
+  }
+  // Drain: observe each stage barrier's last phase before the barriers are invalidated.
+  bool fin = true;
+  for (int s = 0; s < KPT_NST; s++)
+    if (ok && u > (uint32_t)s) fin &= mbar_wait(&bars[s], ((u - 1 - s) / KPT_NST) & 1);
+  if ((!ok || !fin) && l == 0) atomicOr(err, DEV_ERR_TIMEOUT);
+  tc_fence_before();
+  __syncthreads();
+  if (l == 0 && ok && fin)
+    for (int q = 0; q < KPT_NST + 1; q++) mbar_inval(&bars[q]);
+  __syncthreads();
+  return ok && fin;
+}
+
 }  // namespace fdev
 }  // namespace dpkem

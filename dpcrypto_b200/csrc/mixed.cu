@@ -215,7 +215,8 @@ __device__ __forceinline__ void cta_stage(int code, const DevReq &r, uint8_t *sm
   if (scheme == 0) {
     const fdev::Inst v = frodo_view(r);
     if (op == OP_KEYPAIR) {
-      fdev::kp_as_dp4a_cta(v, smem);
+      if (tc) fdev::kp_as_tc_cta(v, smem, tbase, err);
+      else fdev::kp_as_dp4a_cta(v, smem);
     } else if (op == OP_ENC) {
       if (tc) fdev::sa_tc_cta<OP_ENC, kTcStages>(v, smem, tbase, err);
       else fdev::sa_dp4a_cta<OP_ENC>(v, smem);
@@ -235,7 +236,7 @@ __device__ __forceinline__ void cta_stage(int code, const DevReq &r, uint8_t *sm
 }
 
 constexpr int kSmem = std::max({fdev::TcLayout<kTcStages>::total, fdev::DP4A_SMEM, fdev::DEC_W_SMEM,
-                                fdev::KP_AS_SMEM, sdev::PL<4>::TC_TOTAL, sdev::PL<3>::TC_TOTAL,
+                                fdev::KP_AS_SMEM, fdev::KptLayout::total, sdev::PL<4>::TC_TOTAL, sdev::PL<3>::TC_TOTAL,
                                 sdev::PL<2>::TC_TOTAL});
 
 __global__ void __launch_bounds__(256, 2) mixed_kernel(Plan p) {
