@@ -1,0 +1,172 @@
+"""Autotuner: pick the build- and run-time knobs of libdpkem.so on the GPU at hand.
+
+Knobs:
+  keccak_unroll      rounds per iteration of the Keccak-f[1600] round loop (compile time)
+  thread_block       block size of the latency-bound thread-per-instance kernels
+  mixed_frodo_task   instances per Frodo thread-level task in the persistent mixed kernel
+  mixed_saber_task   instances per Saber prologue task (two threads per instance)
+  mixed_thread_task  instances per other thread-level task
+Not knobs, with the measured reason recorded in the output: the MMA tile shape (the int8
+MMAs are <1 % of the tensor pipe: M = 128 is the smallest tile that keeps one TMEM lane per
+output row) and Keccak lanes per thread (one state per thread; the kernels are bound by the
+integer pipe, and splitting a state across threads adds shuffles to the same pipe).
+
+    python -m dpcrypto_b200.autotune --build          # build variants (CPU, nvcc)
+    python -m dpcrypto_b200.autotune --measure        # on a B200: sweep, write tuning.json
+
+Each variant library is measured in its own process (DPKEM_LIB points kem.py at it).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+VARIANTS = os.path.join(HERE, "_build", "variants")
+OUT = os.path.join(HERE, "tuning.json")
+UNROLLS = (1, 2, 3, 4)
+
+
+def variant_lib(u: int) -> str:
+    return os.path.join(VARIANTS, f"unroll{u}", "libdpkem.so")
+
+
+def build_variants() -> None:
+    sys.path.insert(0, ROOT)
+    from dpcrypto_b200 import build as b
+
+    for u in UNROLLS:
+        t = time.time()
+        b.build(out=variant_lib(u), defines=[f"-DDPKEM_KECCAK_UNROLL={u}"])
+        print(f"built unroll={u} in {time.time() - t:.0f} s", flush=True)
+
+
+# ---------------------------------------------------------------- child: measure one library
+def _child(u: int) -> dict:
+    import numpy as np
+    import torch
+
+    sys.path.insert(0, ROOT)
+    import dpcrypto_b200 as d
+    from dpcrypto_b200 import kem
+    from dpcrypto_b200.workloads import MixedBatch
+
+    res = {"keccak_unroll": u}
+    eng = d.Engine(0)
+    res["int_ops_per_s"], res["keccak_per_s"] = eng.probe_int_peaks()
+
+    def frodo_time(B: int, reps: int = 3):
+        kc = torch.empty((B, 64), dtype=torch.uint8, device="cuda")
+        ec = torch.empty((B, 24), dtype=torch.uint8, device="cuda")
+        eng.coins(B, 64, "tune-kp", out=kc)
+        eng.coins(B, 24, "tune-enc", out=ec)
+        pk, sk = eng.keypair(d.FRODO976, kc, d.FORM_TC)
+        ct = torch.empty((B, 15744), dtype=torch.uint8, device="cuda")
+        ss = torch.empty((B, 24), dtype=torch.uint8, device="cuda")
+        for _ in range(2):
+            eng.enc(d.FRODO976, pk, ec, d.FORM_TC, out=(ct, ss))
+            eng.dec(d.FRODO976, ct, sk, d.FORM_TC)
+        torch.cuda.synchronize()
+        eng.profile(True)
+        stages = []
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            eng.enc(d.FRODO976, pk, ec, d.FORM_TC, out=(ct, ss))
+            e = eng.stage_times()
+            eng.dec(d.FRODO976, ct, sk, d.FORM_TC)
+            stages.append((e, eng.stage_times()))
+        torch.cuda.synchronize()
+        eng.profile(False)
+        wall = (time.perf_counter() - t0) / reps
+        dev = float(np.mean([sum(e) + sum(x) for e, x in stages]))
+        thread_ms = float(np.mean([e[0] + e[2] + x[1] + x[3] for e, x in stages]))
+        return wall, dev, thread_ms
+
+    B = 4096
+    res["frodo_b4096_ms"] = frodo_time(B)[1]
+    sweep = {}
+    for tb in (32, 64, 128):
+        kem.set_tuning("thread_block", tb)
+        sweep[tb] = frodo_time(B, reps=2)[2]
+    res["thread_block_ms"] = sweep
+    kem.set_tuning("thread_block", min(sweep, key=sweep.get))
+    # mixed batch task sizes
+    mb = MixedBatch(eng, 4096, seed=7)
+    msweep = {}
+    for ft, stt, tt in ((256, 128, 256), (128, 128, 256), (64, 64, 128), (32, 32, 64)):
+        kem.set_tuning("mixed_frodo_task", ft)
+        kem.set_tuning("mixed_saber_task", stt)
+        kem.set_tuning("mixed_thread_task", tt)
+        eng.mixed(mb.items, d.FORM_TC)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(2):
+            eng.mixed(mb.items, d.FORM_TC)
+        torch.cuda.synchronize()
+        msweep[f"{ft}/{stt}/{tt}"] = (time.perf_counter() - t0) / 2 * 1e3
+        eng.sync()
+        ok = mb.check()
+        mb.clear()
+        if not ok:
+            raise RuntimeError("mixed batch mismatch while tuning")
+    res["mixed_task_ms"] = msweep
+    return res
+
+
+def measure() -> dict:
+    results = []
+    for u in UNROLLS:
+        lib = variant_lib(u)
+        if not os.path.exists(lib):
+            print(f"missing {lib}; run --build first", file=sys.stderr)
+            continue
+        env = dict(os.environ, DPKEM_LIB=lib)
+        r = subprocess.run([sys.executable, "-m", "dpcrypto_b200.autotune", "--child", str(u)], cwd=ROOT, env=env,
+                           capture_output=True, text=True, timeout=900)
+        if r.returncode != 0:
+            raise RuntimeError(f"variant {u} failed:\n{r.stdout}\n{r.stderr}")
+        results.append(json.loads(r.stdout.strip().splitlines()[-1]))
+        print(json.dumps(results[-1]), flush=True)
+    best = min(results, key=lambda x: x["frodo_b4096_ms"])
+    tb = min(best["thread_block_ms"], key=lambda k: best["thread_block_ms"][k])
+    mk = min(best["mixed_task_ms"], key=best["mixed_task_ms"].get)
+    ft, stt, tt = (int(x) for x in mk.split("/"))
+    import torch
+
+    out = {
+        "device": torch.cuda.get_device_name(0),
+        "chosen": {"keccak_unroll": best["keccak_unroll"], "thread_block": int(tb), "mixed_frodo_task": ft,
+                   "mixed_saber_task": stt, "mixed_thread_task": tt},
+        "fixed": {"mma_tile": "M=128 (N=8 Frodo, N=8/16 Saber), K=32: int8 MMA <1% of the tensor pipe",
+                  "keccak_lanes_per_thread": 1},
+        "measurements": results,
+        "command": "python -m dpcrypto_b200.autotune --measure",
+        "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
+    }
+    with open(OUT, "w") as f:
+        json.dump(out, f, indent=1)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--build", action="store_true")
+    ap.add_argument("--measure", action="store_true")
+    ap.add_argument("--child", type=int)
+    a = ap.parse_args()
+    if a.child is not None:
+        print(json.dumps(_child(a.child)))
+        return
+    if a.build:
+        build_variants()
+    if a.measure:
+        print(json.dumps(measure()["chosen"]))
+
+
+if __name__ == "__main__":
+    main()

@@ -42,14 +42,33 @@ def _stale(src: str, obj: str) -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(verbose: bool = False) -> str:
-    os.makedirs(OBJ, exist_ok=True)
+TUNING = os.path.join(HERE, "tuning.json")
+
+
+def tuning_defines() -> list:
+    """Compile-time knobs chosen by the autotuner (dpcrypto_b200/tuning.json)."""
+    import json
+
+    if not os.path.exists(TUNING):
+        return []
+    with open(TUNING) as f:
+        chosen = json.load(f).get("chosen", {})
+    return [f"-DDPKEM_KECCAK_UNROLL={int(chosen['keccak_unroll'])}"] if "keccak_unroll" in chosen else []
+
+
+def build(verbose: bool = False, out: str | None = None, defines: list | None = None) -> str:
+    lib = out or LIB
+    defs = tuning_defines() if defines is None else defines
+    obj_dir = OBJ if out is None else os.path.join(os.path.dirname(os.path.abspath(out)), "_obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    stamp = os.path.join(obj_dir, "defines.txt")
+    stale_defs = not os.path.exists(stamp) or open(stamp).read() != " ".join(defs)
     cc = nvcc()
     jobs = []
     for s in SOURCES:
-        src, obj = os.path.join(CSRC, s), os.path.join(OBJ, s + ".o")
-        if _stale(src, obj):
-            jobs.append([cc, *FLAGS, *EXTRA.get(s, []), *ARCH, "-c", src, "-o", obj])
+        src, obj = os.path.join(CSRC, s), os.path.join(obj_dir, s + ".o")
+        if stale_defs or _stale(src, obj):
+            jobs.append([cc, *FLAGS, *defs, *EXTRA.get(s, []), *ARCH, "-c", src, "-o", obj])
 
     def run(cmd):
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -60,13 +79,15 @@ def build(verbose: bool = False) -> str:
 
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         list(ex.map(run, jobs))
-    objs = [os.path.join(OBJ, s + ".o") for s in SOURCES]
-    if jobs or not os.path.exists(LIB):
-        link = [cc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+    with open(stamp, "w") as f:
+        f.write(" ".join(defs))
+    objs = [os.path.join(obj_dir, s + ".o") for s in SOURCES]
+    if jobs or not os.path.exists(lib):
+        link = [cc, *ARCH, "-shared", "-o", lib, *objs, "-lcudart"]
         r = subprocess.run(link, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {r.stdout}\n{r.stderr}")
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

@@ -13,12 +13,20 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "../../include/dpkem.h"
 #include "common.cuh"
 
 using namespace dpkem;
+
+namespace dpkem {
+Tuning &tuning() {
+  static Tuning t;
+  return t;
+}
+}  // namespace dpkem
 
 struct dpkem_ctx {
   int device = 0;
@@ -556,6 +564,25 @@ int dpkem_probe_int_peaks(dpkem_ctx *c, double *int_ops_per_s, double *keccak_pe
   std::lock_guard<std::mutex> lock(c->mu);
   cudaSetDevice(c->device);
   return set_status(cuda_status(probe_int_peaks(c->stream, int_ops_per_s, keccak_per_s)));
+}
+
+int dpkem_set_tuning(const char *key, int value) {
+  if (!key || value <= 0) return set_status(DPKEM_EINVAL);
+  Tuning &t = tuning();
+  const std::string k(key);
+  if (k == "thread_block") {
+    if (value % 32 || value > 256) return set_status(DPKEM_EINVAL);
+    t.thread_block = value;
+  } else if (k == "mixed_frodo_task") {
+    t.mixed_frodo_task = std::min(value, 256);
+  } else if (k == "mixed_saber_task") {
+    t.mixed_saber_task = std::min(value, 128);
+  } else if (k == "mixed_thread_task") {
+    t.mixed_thread_task = std::min(value, 256);
+  } else {
+    return set_status(DPKEM_EINVAL);
+  }
+  return set_status(DPKEM_OK);
 }
 
 const char *dpkem_strerror(int s) {

@@ -37,6 +37,15 @@ __host__ __device__ constexpr Params params(int level) {
 
 enum Op : int { OP_KEYPAIR = 0, OP_ENC = 1, OP_DEC = 2 };
 
+// Runtime tuning knobs (set through dpkem_set_tuning; chosen by dpcrypto_b200/autotune.py).
+struct Tuning {
+  int thread_block = 64;        // block size of the thread-per-instance kernels
+  int mixed_frodo_task = 256;   // instances per Frodo thread-level task in a mixed batch
+  int mixed_saber_task = 128;   // instances per Saber prologue task (two threads each)
+  int mixed_thread_task = 256;  // instances per other thread-level task
+};
+Tuning &tuning();
+
 // Optional per-stage timing: when non-null, a launcher records ev[k] on its stream
 // before its k-th stage and ev[nstages] after the last one.
 struct StageTimer {

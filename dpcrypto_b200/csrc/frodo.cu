@@ -10,25 +10,25 @@ using namespace frodo;
 using fdev::inst_of;
 
 template <int OP>
-__global__ void __launch_bounds__(64) kp_prologue_kernel(FrodoBatch b) {
+__global__ void __launch_bounds__(256) kp_prologue_kernel(FrodoBatch b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < b.n) fdev::kp_prologue_inst(inst_of(b, i, OP));
 }
 
 template <int OP>
-__global__ void __launch_bounds__(64) pk_hash_kernel(FrodoBatch b) {
+__global__ void __launch_bounds__(256) pk_hash_kernel(FrodoBatch b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < b.n) fdev::pk_hash_inst(inst_of(b, i, OP));
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(64) prologue_kernel(FrodoBatch b) {
+__global__ void __launch_bounds__(256) prologue_kernel(FrodoBatch b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < b.n) fdev::prologue_inst<MODE>(inst_of(b, i, MODE));
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(64) ss_kernel(FrodoBatch b) {
+__global__ void __launch_bounds__(256) ss_kernel(FrodoBatch b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < b.n) fdev::ss_inst<MODE>(inst_of(b, i, MODE));
 }
@@ -122,8 +122,9 @@ inline void mark(const FrodoBatch &b, cudaStream_t st) {
 
 cudaError_t frodo_keypair(const FrodoBatch &b, int form, cudaStream_t st) {
   if (b.n <= 0) return cudaSuccess;
+  const int tb = tuning().thread_block;
   mark(b, st);
-  kp_prologue_kernel<OP_KEYPAIR><<<blocks_for(b.n, 64), 64, 0, st>>>(b);
+  kp_prologue_kernel<OP_KEYPAIR><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);
   if (form == FORM_TC) {
     cudaError_t e = set_smem(kp_as_tc_kernel, fdev::KptLayout::total);
@@ -133,35 +134,37 @@ cudaError_t frodo_keypair(const FrodoBatch &b, int form, cudaStream_t st) {
     kp_as_dp4a_kernel<<<b.n, 256, fdev::KP_AS_SMEM, st>>>(b);
   }
   mark(b, st);
-  pk_hash_kernel<OP_KEYPAIR><<<blocks_for(b.n, 64), 64, 0, st>>>(b);
+  pk_hash_kernel<OP_KEYPAIR><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);
   return cudaGetLastError();
 }
 
 cudaError_t frodo_enc(const FrodoBatch &b, int form, cudaStream_t st) {
   if (b.n <= 0) return cudaSuccess;
+  const int tb = tuning().thread_block;
   mark(b, st);
-  prologue_kernel<OP_ENC><<<blocks_for(b.n, 64), 64, 0, st>>>(b);
+  prologue_kernel<OP_ENC><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);
   cudaError_t e = launch_sa<OP_ENC>(b, form, st);
   if (e != cudaSuccess) return e;
   mark(b, st);
-  ss_kernel<OP_ENC><<<blocks_for(b.n, 64), 64, 0, st>>>(b);
+  ss_kernel<OP_ENC><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);
   return cudaGetLastError();
 }
 
 cudaError_t frodo_dec(const FrodoBatch &b, int form, cudaStream_t st) {
   if (b.n <= 0) return cudaSuccess;
+  const int tb = tuning().thread_block;
   mark(b, st);
   dec_w_kernel<<<b.n, 256, fdev::DEC_W_SMEM, st>>>(b);
   mark(b, st);
-  prologue_kernel<OP_DEC><<<blocks_for(b.n, 64), 64, 0, st>>>(b);
+  prologue_kernel<OP_DEC><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);
   cudaError_t e = launch_sa<OP_DEC>(b, form, st);
   if (e != cudaSuccess) return e;
   mark(b, st);
-  ss_kernel<OP_DEC><<<blocks_for(b.n, 64), 64, 0, st>>>(b);
+  ss_kernel<OP_DEC><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);
   return cudaGetLastError();
 }

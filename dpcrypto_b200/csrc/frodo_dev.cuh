@@ -569,7 +569,7 @@ __device__ __forceinline__ void wg_sync(int g) {
 // TMEM columns [tbase, tbase + 48) must be allocated by the caller.
 __device__ __forceinline__ bool kp_as_tc_cta(const Inst &v, uint8_t *smem, uint32_t tbase, uint32_t *err) {
   using L = KptLayout;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = warp >> 2, l = tid & 127;
+  const int tid = threadIdx.x, warp = tid >> 5, g = warp >> 2, l = tid & 127;
   uint8_t *stop = smem + L::st;
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bars) + g * (KPT_NST + 1);
   const uint16_t *rw = v.rw;

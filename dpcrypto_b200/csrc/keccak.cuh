@@ -102,8 +102,15 @@ __device__ __forceinline__ void keccak_round(uint2 (&a)[25], uint2 rcv) {
   a[0].y ^= rcv.y;
 }
 
+// Rounds per loop iteration (a tuning knob; dpcrypto_b200/tuning.json sets it at build time).
+#ifndef DPKEM_KECCAK_UNROLL
+#define DPKEM_KECCAK_UNROLL 2
+#endif
+
+constexpr int kKeccakUnroll = DPKEM_KECCAK_UNROLL;
+
 __device__ __forceinline__ void keccak_f1600(uint2 (&a)[25]) {
-#pragma unroll 2
+#pragma unroll kKeccakUnroll
   for (int r = 0; r < 24; r++) keccak_round(a, c_keccak_rc[r]);
 }
 

@@ -313,6 +313,14 @@ struct HostTask {
 
 }  // namespace
 
+// Instances per thread-level task (tuning knobs, clamped to what one CTA can hold).
+int task_size(int scheme, int kind) {
+  const Tuning &t = tuning();
+  int v = kind == K_THREAD2 ? t.mixed_saber_task : scheme == 0 ? t.mixed_frodo_task : t.mixed_thread_task;
+  const int cap = kind == K_THREAD2 ? 128 : 256;
+  return std::max(1, std::min(v, cap));
+}
+
 // Bytes of device memory a plan for these requests needs (tables + scratch records).
 size_t plan_bytes(const Req *reqs, size_t n, size_t *ntasks_out) {
   size_t scr = 0, ntasks = 0, nidx = 0;
@@ -327,7 +335,8 @@ size_t plan_bytes(const Req *reqs, size_t n, size_t *ntasks_out) {
       if (!c || s == 1) continue;
       for (int st = 0; st < nstages(s, op); st++) {
         const int kind = kind_of(s, op, st);
-        ntasks += kind == K_CTA ? c : (c + (kind == K_THREAD2 ? 127 : 255)) / (kind == K_THREAD2 ? 128 : 256);
+        const size_t per = kind == K_CTA ? 1 : (size_t)task_size(s, kind);
+        ntasks += (c + per - 1) / per;
         nidx += c;
       }
     }
@@ -374,7 +383,7 @@ cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *
     std::vector<int> owner_prev(R.size(), -1);  // task index of each instance's previous stage
     for (int stg = 0; stg < nstages(scheme, op); stg++) {
       const int kind = kind_of(scheme, op, stg);
-      const int per = kind == K_CTA ? 1 : kind == K_THREAD2 ? 128 : 256;
+      const int per = kind == K_CTA ? 1 : task_size(scheme, kind);
       const uint32_t base = (uint32_t)idx.size();
       idx.insert(idx.end(), R.begin(), R.end());
       std::vector<int> owner(R.size());

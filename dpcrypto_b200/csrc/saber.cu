@@ -18,7 +18,7 @@ __global__ void __launch_bounds__(64) prologue_kernel(SaberBatch b) {
 }
 
 template <int L, int OP>
-__global__ void __launch_bounds__(64) finish_kernel(SaberBatch b) {
+__global__ void __launch_bounds__(256) finish_kernel(SaberBatch b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < b.n) sdev::finish_inst<L, OP>(inst_of<L>(b, i, OP));
 }
@@ -82,7 +82,8 @@ inline void mark(const SaberBatch &b, cudaStream_t st) {
 
 template <int L>
 cudaError_t run(const SaberBatch &b, int op, int form, cudaStream_t st) {
-  const int pb = (b.n + 31) / 32, fb = (b.n + 63) / 64;
+  const int tb = tuning().thread_block;
+  const int pb = (b.n + 31) / 32, fb = (b.n + tb - 1) / tb;
   cudaError_t e;
   mark(b, st);
   switch (op) {
@@ -91,14 +92,14 @@ cudaError_t run(const SaberBatch &b, int op, int form, cudaStream_t st) {
       mark(b, st);
       if ((e = launch_product<L, sdev::PM_KEYPAIR>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
-      finish_kernel<L, OP_KEYPAIR><<<fb, 64, 0, st>>>(b);
+      finish_kernel<L, OP_KEYPAIR><<<fb, tb, 0, st>>>(b);
       break;
     case OP_ENC:
       prologue_kernel<L, OP_ENC><<<pb, 64, 0, st>>>(b);
       mark(b, st);
       if ((e = launch_product<L, sdev::PM_ENC>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
-      finish_kernel<L, OP_ENC><<<fb, 64, 0, st>>>(b);
+      finish_kernel<L, OP_ENC><<<fb, tb, 0, st>>>(b);
       break;
     default:
       if ((e = launch_product<L, sdev::PM_DEC_INNER>(b, form, st)) != cudaSuccess) return e;
@@ -107,7 +108,7 @@ cudaError_t run(const SaberBatch &b, int op, int form, cudaStream_t st) {
       mark(b, st);
       if ((e = launch_product<L, sdev::PM_DEC_CMP>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
-      finish_kernel<L, OP_DEC><<<fb, 64, 0, st>>>(b);
+      finish_kernel<L, OP_DEC><<<fb, tb, 0, st>>>(b);
       break;
   }
   mark(b, st);

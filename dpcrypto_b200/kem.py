@@ -19,7 +19,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libdpkem.so")
+# DPKEM_LIB selects another build of the library (the autotuner measures its variants this way).
+LIB_PATH = os.environ.get("DPKEM_LIB") or os.path.join(HERE, "libdpkem.so")
 
 FRODO976, LIGHTSABER, SABER, FIRESABER = 0, 2, 3, 4
 SCHEMES = (FRODO976, LIGHTSABER, SABER, FIRESABER)
@@ -64,6 +65,7 @@ EXPORTS = {
     "dpkem_saber_enc_batch_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_void_p]),
+    "dpkem_set_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     "dpkem_strerror": (ctypes.c_char_p, [ctypes.c_int]),
     "dpkem_last_status": (ctypes.c_int, []),
     "dpkem_set_compat_batch": (None, [ctypes.c_size_t]),
@@ -98,7 +100,34 @@ def load() -> ctypes.CDLL:
             fn.restype = res
             fn.argtypes = args
         _lib = lib
+        apply_tuning()
     return _lib
+
+
+TUNING_PATH = os.path.join(HERE, "tuning.json")
+RUNTIME_KNOBS = ("thread_block", "mixed_frodo_task", "mixed_saber_task", "mixed_thread_task")
+
+
+def apply_tuning(path: str = TUNING_PATH) -> dict:
+    """Apply the runtime knobs recorded by the autotuner (dpcrypto_b200/tuning.json), if any."""
+    import json
+
+    if not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        chosen = json.load(f).get("chosen", {})
+    for k in RUNTIME_KNOBS:
+        if k in chosen:
+            rc = _lib.dpkem_set_tuning(k.encode(), int(chosen[k]))
+            if rc != OK:
+                raise DpkemError(rc, f"tuning {k}={chosen[k]}")
+    return chosen
+
+
+def set_tuning(key: str, value: int) -> None:
+    rc = load().dpkem_set_tuning(key.encode(), int(value))
+    if rc != OK:
+        raise DpkemError(rc, f"set_tuning({key}, {value})")
 
 
 def sizes(scheme: int) -> dict:

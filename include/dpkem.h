@@ -135,6 +135,12 @@ int dpkem_probe_int_peaks(dpkem_ctx *ctx, double *int_ops_per_s, double *keccak_
 int dpkem_saber_enc_batch_static(int scheme, int form, size_t n, const uint8_t *coins, const uint8_t *pk,
                                  uint8_t *ct, uint8_t *ss, void *stream);
 
+/* Runtime tuning knobs (process-wide): "thread_block" (block size of the thread-per-instance
+ * kernels, multiple of 32, <= 256), "mixed_frodo_task" / "mixed_saber_task" /
+ * "mixed_thread_task" (instances per thread-level task in mixed batches).  Chosen by
+ * dpcrypto_b200/autotune.py and stored in dpcrypto_b200/tuning.json. */
+int dpkem_set_tuning(const char *key, int value);
+
 const char *dpkem_strerror(int status);
 /* Status of the last call made by this thread (the compatibility shims return void). */
 int dpkem_last_status(void);
