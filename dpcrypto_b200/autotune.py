@@ -4,7 +4,7 @@ Knobs:
   keccak_unroll      rounds per iteration of the Keccak-f[1600] round loop (compile time)
   thread_block       block size of the latency-bound thread-per-instance kernels
   mixed_frodo_task   instances per Frodo thread-level task in the persistent mixed kernel
-  mixed_saber_task   instances per Saber prologue task (two threads per instance)
+  mixed_pair_task    instances per two-role prologue task (two threads per instance)
   mixed_thread_task  instances per other thread-level task
 Not knobs, with the measured reason recorded in the output: the MMA tile shape (the int8
 MMAs are <1 % of the tensor pipe: M = 128 is the smallest tile that keeps one TMEM lane per
@@ -100,7 +100,7 @@ def _child(u: int) -> dict:
     msweep = {}
     for ft, stt, tt in ((256, 128, 256), (128, 128, 256), (64, 64, 128), (32, 32, 64)):
         kem.set_tuning("mixed_frodo_task", ft)
-        kem.set_tuning("mixed_saber_task", stt)
+        kem.set_tuning("mixed_pair_task", stt)
         kem.set_tuning("mixed_thread_task", tt)
         eng.mixed(mb.items, d.FORM_TC)
         torch.cuda.synchronize()
@@ -141,7 +141,7 @@ def measure() -> dict:
     out = {
         "device": torch.cuda.get_device_name(0),
         "chosen": {"keccak_unroll": best["keccak_unroll"], "thread_block": int(tb), "mixed_frodo_task": ft,
-                   "mixed_saber_task": stt, "mixed_thread_task": tt},
+                   "mixed_pair_task": stt, "mixed_thread_task": tt},
         "fixed": {"mma_tile": "M=128 (N=8 Frodo, N=8/16 Saber), K=32: int8 MMA <1% of the tensor pipe",
                   "keccak_lanes_per_thread": 1},
         "measurements": results,

@@ -73,7 +73,7 @@ bool scheme_sizes(int scheme, Sizes *z) {
 
 // Per-instance bytes of scratch and, in host mode, of device staging for each op.
 size_t scratch_per_instance(int scheme) {
-  if (scheme == DPKEM_FRODO976) return (size_t)frodo::RW * 2 + 24 + 24 + 4 + 64;
+  if (scheme == DPKEM_FRODO976) return (size_t)frodo::RW * 2 + 24 + 24 + 4 + 200 + 80;
   return saber_scratch_bytes(scheme) + 4 + 16;
 }
 
@@ -125,7 +125,7 @@ struct Carver {
 size_t arena_need(int scheme, int op, size_t chunk, bool host) {
   size_t s = 0;
   if (scheme == DPKEM_FRODO976) {
-    s += up(chunk * frodo::RW * 2) + up(chunk * 24) * 2 + up(chunk * 4);
+    s += up(chunk * frodo::RW * 2) + up(chunk * 24) * 2 + up(chunk * 4) + up(chunk * 200);
   } else {
     s += up(chunk * saber_scratch_bytes(scheme)) + up(chunk * 4);
   }
@@ -203,6 +203,7 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
       fb.kk = cv.take<uint8_t>(chunk * 24);
       fb.mu = cv.take<uint8_t>(chunk * 24);
       fb.fail = cv.take<uint32_t>(chunk * 4);
+      fb.hs = cv.take<uint2>(chunk * 200);
     } else {
       sb.scr = cv.take<uint8_t>(chunk * saber_scratch_bytes(scheme));
       sb.fail = cv.take<uint32_t>(chunk * 4);
@@ -575,8 +576,8 @@ int dpkem_set_tuning(const char *key, int value) {
     t.thread_block = value;
   } else if (k == "mixed_frodo_task") {
     t.mixed_frodo_task = std::min(value, 256);
-  } else if (k == "mixed_saber_task") {
-    t.mixed_saber_task = std::min(value, 128);
+  } else if (k == "mixed_pair_task") {
+    t.mixed_pair_task = std::min(value, 128);
   } else if (k == "mixed_thread_task") {
     t.mixed_thread_task = std::min(value, 256);
   } else {

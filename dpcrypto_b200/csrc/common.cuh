@@ -41,7 +41,7 @@ enum Op : int { OP_KEYPAIR = 0, OP_ENC = 1, OP_DEC = 2 };
 struct Tuning {
   int thread_block = 64;        // block size of the thread-per-instance kernels
   int mixed_frodo_task = 256;   // instances per Frodo thread-level task in a mixed batch
-  int mixed_saber_task = 128;   // instances per Saber prologue task (two threads each)
+  int mixed_pair_task = 128;    // instances per two-role prologue task (two threads each)
   int mixed_thread_task = 256;  // instances per other thread-level task
 };
 Tuning &tuning();
@@ -69,6 +69,7 @@ struct FrodoBatch {
   uint8_t *kk;           // scratch [n][24]: k (enc) or k' (dec)
   uint8_t *mu;           // scratch [n][24]: decoded mu' (dec)
   uint32_t *fail;        // scratch [n]: nonzero when the re-encryption differs (dec)
+  uint2 *hs;             // scratch [n][25]: SHAKE256 state after absorbing ct's full blocks (dec)
   uint32_t *err;         // device error word (DEV_ERR_*)
   StageTimer *timer;     // optional
 };

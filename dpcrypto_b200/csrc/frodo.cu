@@ -27,6 +27,15 @@ __global__ void __launch_bounds__(256) prologue_kernel(FrodoBatch b) {
   if (i < b.n) fdev::prologue_inst<MODE>(inst_of(b, i, MODE));
 }
 
+// Decaps prologue, 64 threads = 32 instances: warp 0 runs the sampling chain, warp 1 the
+// ciphertext pre-absorb of the final hash.
+__global__ void __launch_bounds__(64) dec_prologue_kernel(FrodoBatch b) {
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31);
+  if (i >= b.n) return;
+  if (threadIdx.x < 32) fdev::prologue_inst<OP_DEC>(inst_of(b, i, OP_DEC));
+  else fdev::ct_absorb_inst(inst_of(b, i, OP_DEC));
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256) ss_kernel(FrodoBatch b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -159,7 +168,7 @@ cudaError_t frodo_dec(const FrodoBatch &b, int form, cudaStream_t st) {
   mark(b, st);
   dec_w_kernel<<<b.n, 256, fdev::DEC_W_SMEM, st>>>(b);
   mark(b, st);
-  prologue_kernel<OP_DEC><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
+  dec_prologue_kernel<<<blocks_for(b.n, 32), 64, 0, st>>>(b);
   mark(b, st);
   cudaError_t e = launch_sa<OP_DEC>(b, form, st);
   if (e != cudaSuccess) return e;

@@ -30,6 +30,7 @@ struct Inst {
   uint16_t *rw;          // RW sampled words
   uint8_t *kk, *mu;      // 24 B each
   uint32_t *fail;
+  uint2 *hs;             // 25 lanes: SHAKE256 state after ct's full blocks (decaps)
 };
 
 __device__ __forceinline__ Inst inst_of(const FrodoBatch &b, int i, int op) {
@@ -43,6 +44,7 @@ __device__ __forceinline__ Inst inst_of(const FrodoBatch &b, int i, int op) {
   v.kk = b.kk + (size_t)i * LENSE;
   v.mu = b.mu + (size_t)i * LENMU;
   v.fail = b.fail + i;
+  v.hs = b.hs ? b.hs + (size_t)i * 25 : nullptr;
   return v;
 }
 
@@ -56,8 +58,37 @@ __device__ __forceinline__ uint32_t sample16(uint32_t v) {
   return (((0u - sign) ^ s) + sign) & 0xFFFFu;
 }
 
+// The same sampler with its ten comparisons on the FMA pipe, which Keccak leaves idle:
+// x = CDF[c] - t by mad.lo (t * (2^32 - 1) + CDF[c]) and s += x >> 31 by mad.hi (hi32(x * 2)).
+// The multipliers come from opaque registers so the compiler cannot turn them back into
+// integer-ALU adds and shifts.  Bit-identical to sample16 (checked exhaustively on the GPU).
+struct FmaConsts {
+  uint32_t neg1, two;
+};
+__device__ __forceinline__ FmaConsts fma_consts() {
+  FmaConsts k;
+  asm volatile("mov.u32 %0, 0xFFFFFFFF;" : "=r"(k.neg1));
+  asm volatile("mov.u32 %0, 2;" : "=r"(k.two));
+  return k;
+}
+
+__device__ __forceinline__ uint32_t sample16_fma(uint32_t v, FmaConsts k) {
+  constexpr uint32_t cdf[10] = {5638, 15915, 23689, 28571, 31116, 32217, 32613, 32731, 32760, 32766};
+  const uint32_t t = (v & 0xFFFFu) >> 1, sign = v & 1u;
+  uint32_t s = 0;
+#pragma unroll
+  for (int c = 0; c < 10; c++) {
+    uint32_t x;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(x) : "r"(t), "r"(k.neg1), "r"(cdf[c]));
+    asm("mad.hi.u32 %0, %1, %2, %0;" : "+r"(s) : "r"(x), "r"(k.two));
+  }
+  return (((0u - sign) ^ s) + sign) & 0xFFFFu;
+}
+
 __device__ __forceinline__ uint2 sample_lane(uint2 w) {
-  return make_uint2(sample16(w.x) | (sample16(w.x >> 16) << 16), sample16(w.y) | (sample16(w.y >> 16) << 16));
+  const FmaConsts k = fma_consts();
+  return make_uint2(sample16_fma(w.x, k) | (sample16_fma(w.x >> 16, k) << 16),
+                    sample16_fma(w.y, k) | (sample16_fma(w.y >> 16, k) << 16));
 }
 
 // Message lanes of 0x5F/0x96 || seed (24 bytes), i.e. the 25-byte sampling-stream input.
@@ -154,6 +185,19 @@ __device__ __forceinline__ void prologue_inst(const Inst &v) {
   sample_stream(a, v.rw, RW, nullptr, 0);
 }
 
+// Decaps: ss = SHAKE256(ct || k-hat) absorbs the input ciphertext's 115 full rate blocks
+// before k-hat is known, so that part runs beside the prologue (second role of its stage);
+// the state is parked in scratch and ss_inst<OP_DEC> finishes with one permutation.
+constexpr int CT_FULL = (CT / 136) * 136;  // 15,640
+
+__device__ __forceinline__ void ct_absorb_inst(const Inst &v) {
+  uint2 a[25];
+  keccak_zero(a);
+  absorb_aligned<136>(a, 0, v.ct, CT_FULL);
+#pragma unroll
+  for (int q = 0; q < 25; q++) v.hs[q] = a[q];
+}
+
 // ss = SHAKE256(ct || k); decaps selects k' or s in constant time (util.cu:193-226).
 template <int MODE>
 __device__ __forceinline__ void ss_inst(const Inst &v) {
@@ -170,8 +214,15 @@ __device__ __forceinline__ void ss_inst(const Inst &v) {
     }
   }
   uint2 a[25];
-  keccak_zero(a);
-  int pos = absorb_aligned<136>(a, 0, v.ct, CT);
+  int pos;
+  if (MODE == OP_DEC) {
+#pragma unroll
+    for (int q = 0; q < 25; q++) a[q] = v.hs[q];
+    pos = absorb_aligned<136>(a, 0, v.ct + CT_FULL, CT - CT_FULL);
+  } else {
+    keccak_zero(a);
+    pos = absorb_aligned<136>(a, 0, v.ct, CT);
+  }
 #pragma unroll
   for (int q = 0; q < 3; q++) pos = absorb_word<136>(a, pos, kh[q]);
   absorb_finish<136>(a, pos, 0x1Fu);

@@ -40,15 +40,16 @@ __host__ __device__ constexpr int op_of(int code) { return (code >> 4) & 3; }
 __host__ __device__ constexpr int stage_of(int code) { return (code >> 1) & 7; }
 __host__ __device__ constexpr bool tc_of(int code) { return code & 1; }
 
-// Stage kinds: 0 = thread (one instance per thread), 2 = thread with two roles
-// (Saber prologue: instance t on threads t and t + 128), 1 = CTA (one instance per task).
+// Stage kinds: 0 = thread (one instance per thread), 2 = thread with two roles (instance
+// t on threads t and t + 128: Saber's two prologue sponges, Frodo decaps' prologue and
+// ciphertext pre-absorb), 1 = CTA (one instance per task).
 enum Kind : int { K_THREAD = 0, K_CTA = 1, K_THREAD2 = 2 };
 
 __host__ __device__ constexpr int nstages(int scheme, int op) { return op == OP_DEC ? 4 : 3; }
 
 __host__ __device__ constexpr int kind_of(int scheme, int op, int stage) {
   if (scheme == 0) {
-    if (op == OP_DEC) return stage == 0 || stage == 2 ? K_CTA : K_THREAD;
+    if (op == OP_DEC) return stage == 0 || stage == 2 ? K_CTA : stage == 1 ? K_THREAD2 : K_THREAD;
     return stage == 1 ? K_CTA : K_THREAD;
   }
   if (op == OP_DEC) return stage == 1 ? K_THREAD2 : stage == 3 ? K_THREAD : K_CTA;
@@ -63,8 +64,9 @@ __host__ __device__ constexpr uint32_t threshold(int scheme, int op, int stage) 
 }
 
 // ---- per-request scratch records (256-byte multiples so no line is shared) ----
-constexpr size_t kFrodoRec = 31488;  // rw 31,360 | k 24 | mu 24 | fail 4
+constexpr size_t kFrodoRec = 31744;  // rw 31,360 | k 24 | mu 24 | fail 4 (+12) | sponge 200
 constexpr size_t kFrodoK = frodo::RW * 2, kFrodoMu = kFrodoK + 24, kFrodoFail = kFrodoMu + 24;
+constexpr size_t kFrodoHs = kFrodoFail + 16;
 
 __host__ __device__ inline size_t saber_rec_bytes(int level) {
   const size_t b = level == 2 ? sdev::Scr<2>::BYTES : level == 3 ? sdev::Scr<3>::BYTES : sdev::Scr<4>::BYTES;
@@ -106,6 +108,7 @@ __device__ __forceinline__ fdev::Inst frodo_view(const DevReq &r) {
   v.kk = r.scr + kFrodoK;
   v.mu = r.scr + kFrodoMu;
   v.fail = reinterpret_cast<uint32_t *>(r.scr + kFrodoFail);
+  v.hs = reinterpret_cast<uint2 *>(r.scr + kFrodoHs);
   return v;
 }
 
@@ -178,7 +181,8 @@ __device__ __forceinline__ void thread_stage(int code, const DevReq &r, int role
       if (stage == 0) fdev::prologue_inst<OP_ENC>(v);
       else fdev::ss_inst<OP_ENC>(v);
     } else {
-      if (stage == 1) fdev::prologue_inst<OP_DEC>(v);
+      if (stage == 1 && role == 0) fdev::prologue_inst<OP_DEC>(v);
+      else if (stage == 1) fdev::ct_absorb_inst(v);
       else fdev::ss_inst<OP_DEC>(v);
     }
   } else if (scheme == 2) {
@@ -316,7 +320,7 @@ struct HostTask {
 // Instances per thread-level task (tuning knobs, clamped to what one CTA can hold).
 int task_size(int scheme, int kind) {
   const Tuning &t = tuning();
-  int v = kind == K_THREAD2 ? t.mixed_saber_task : scheme == 0 ? t.mixed_frodo_task : t.mixed_thread_task;
+  int v = kind == K_THREAD2 ? t.mixed_pair_task : scheme == 0 ? t.mixed_frodo_task : t.mixed_thread_task;
   const int cap = kind == K_THREAD2 ? 128 : 256;
   return std::max(1, std::min(v, cap));
 }

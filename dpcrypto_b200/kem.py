@@ -105,7 +105,7 @@ def load() -> ctypes.CDLL:
 
 
 TUNING_PATH = os.path.join(HERE, "tuning.json")
-RUNTIME_KNOBS = ("thread_block", "mixed_frodo_task", "mixed_saber_task", "mixed_thread_task")
+RUNTIME_KNOBS = ("thread_block", "mixed_frodo_task", "mixed_pair_task", "mixed_thread_task")
 
 
 def apply_tuning(path: str = TUNING_PATH) -> dict:

@@ -136,7 +136,7 @@ int dpkem_saber_enc_batch_static(int scheme, int form, size_t n, const uint8_t *
                                  uint8_t *ct, uint8_t *ss, void *stream);
 
 /* Runtime tuning knobs (process-wide): "thread_block" (block size of the thread-per-instance
- * kernels, multiple of 32, <= 256), "mixed_frodo_task" / "mixed_saber_task" /
+ * kernels, multiple of 32, <= 256), "mixed_frodo_task" / "mixed_pair_task" /
  * "mixed_thread_task" (instances per thread-level task in mixed batches).  Chosen by
  * dpcrypto_b200/autotune.py and stored in dpcrypto_b200/tuning.json. */
 int dpkem_set_tuning(const char *key, int value);
