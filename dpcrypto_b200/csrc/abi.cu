@@ -33,6 +33,8 @@ struct dpkem_ctx {
   size_t budget = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t last = nullptr;
+  cudaStream_t pipe[2] = {nullptr, nullptr};  // host-mode copy/compute pipeline
+  cudaEvent_t pev[2] = {nullptr, nullptr};
   uint8_t *arena = nullptr;
   size_t arena_bytes = 0;
   uint32_t *d_err = nullptr;
@@ -52,6 +54,8 @@ int set_status(int s) {
 }
 
 constexpr size_t kAlign = 256;
+constexpr size_t kPipeChunkMin = 256;  // smallest chunk of a host-mode pipeline
+constexpr size_t kPipeChunks = 4;      // chunks per host-mode batch when pipelined
 constexpr size_t kDefaultBudget = 8ull << 30;
 
 size_t up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
@@ -179,11 +183,29 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
   std::lock_guard<std::mutex> lock(c->mu);
   if (cudaSetDevice(c->device) != cudaSuccess) return cuda_status(cudaErrorInvalidDevice);
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
-  const size_t chunk = std::min(n, chunk_for(c, scheme, op, !dev));
-  int rc = ensure_arena(c, arena_need(scheme, op, chunk, !dev));
+  // Host-mode batches of at least two chunks run as a two-stream pipeline: chunks alternate
+  // between the context's pipeline streams (each with its own half of the arena), so the
+  // copies of one chunk overlap the kernels of the other.
+  size_t chunk = std::min(n, chunk_for(c, scheme, op, !dev));
+  int npipe = 1;
+  if (!dev && !c->profile && n >= 2 * kPipeChunkMin) {
+    npipe = 2;
+    chunk = std::min(std::max(kPipeChunkMin, (n + kPipeChunks - 1) / kPipeChunks), chunk_for(c, scheme, op, true) / 2);
+    if (chunk == 0) chunk = 1;
+  }
+  const size_t per_pipe = (arena_need(scheme, op, chunk, !dev) + kAlign - 1) & ~(kAlign - 1);
+  int rc = ensure_arena(c, per_pipe * npipe);
   if (rc) return rc;
   cudaError_t e = cudaStreamWaitEvent(st, c->last, 0);
   if (e != cudaSuccess) return cuda_status(e);
+  cudaStream_t streams[2] = {st, st};
+  if (npipe == 2) {
+    if ((e = cudaEventRecord(c->pev[0], st)) != cudaSuccess) return cuda_status(e);
+    for (int j = 0; j < 2; j++) {
+      streams[j] = c->pipe[j];
+      if ((e = cudaStreamWaitEvent(streams[j], c->pev[0], 0)) != cudaSuccess) return cuda_status(e);
+    }
+  }
 
   size_t in0_sz, in1_sz = 0, out0_sz, out1_sz = 0;
   switch (op) {
@@ -191,9 +213,12 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
     case OP_ENC: in0_sz = z.encc; in1_sz = z.pk; out0_sz = z.ct; out1_sz = z.ss; break;
     default: in0_sz = z.ct; in1_sz = z.sk; out0_sz = z.ss; break;
   }
-  for (size_t first = 0; first < n; first += chunk) {
+  size_t k = 0;
+  for (size_t first = 0; first < n; first += chunk, k++) {
     const size_t m = std::min(chunk, n - first);
-    Carver cv{c->arena};
+    const int j = (int)(k % (size_t)npipe);
+    cudaStream_t sj = streams[j];
+    Carver cv{c->arena + (size_t)j * per_pipe};
     const uint8_t *d_in0, *d_in1 = nullptr;
     uint8_t *d_out0, *d_out1 = nullptr;
     FrodoBatch fb{};
@@ -218,9 +243,9 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
       uint8_t *b = in1_sz ? cv.take<uint8_t>(chunk * in1_sz) : nullptr;
       d_out0 = cv.take<uint8_t>(chunk * out0_sz);
       d_out1 = out1_sz ? cv.take<uint8_t>(chunk * out1_sz) : nullptr;
-      if ((e = cudaMemcpyAsync(a, in0 + first * in0_sz, m * in0_sz, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+      if ((e = cudaMemcpyAsync(a, in0 + first * in0_sz, m * in0_sz, cudaMemcpyHostToDevice, sj)) != cudaSuccess)
         return cuda_status(e);
-      if (b && (e = cudaMemcpyAsync(b, in1 + first * in1_sz, m * in1_sz, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+      if (b && (e = cudaMemcpyAsync(b, in1 + first * in1_sz, m * in1_sz, cudaMemcpyHostToDevice, sj)) != cudaSuccess)
         return cuda_status(e);
       d_in0 = a;
       d_in1 = b;
@@ -238,15 +263,15 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
       switch (op) {
         case OP_KEYPAIR:
           fb.coins = d_in0; fb.pk = d_out0; fb.sk = d_out1;
-          e = frodo_keypair(fb, form, st);
+          e = frodo_keypair(fb, form, sj);
           break;
         case OP_ENC:
           fb.coins = d_in0; fb.pk = const_cast<uint8_t *>(d_in1); fb.ct = d_out0; fb.ss = d_out1;
-          e = frodo_enc(fb, form, st);
+          e = frodo_enc(fb, form, sj);
           break;
         default:
           fb.ct = const_cast<uint8_t *>(d_in0); fb.sk = const_cast<uint8_t *>(d_in1); fb.ss = d_out0;
-          e = frodo_dec(fb, form, st);
+          e = frodo_dec(fb, form, sj);
           break;
       }
     } else {
@@ -256,28 +281,32 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
       switch (op) {
         case OP_KEYPAIR:
           sb.coins = d_in0; sb.pk = d_out0; sb.sk = d_out1;
-          e = saber_keypair(sb, form, st);
+          e = saber_keypair(sb, form, sj);
           break;
         case OP_ENC:
           sb.coins = d_in0; sb.pk = const_cast<uint8_t *>(d_in1); sb.ct = d_out0; sb.ss = d_out1;
-          e = saber_enc(sb, form, st);
+          e = saber_enc(sb, form, sj);
           break;
         default:
           sb.ct = const_cast<uint8_t *>(d_in0); sb.sk = const_cast<uint8_t *>(d_in1); sb.ss = d_out0;
-          e = saber_dec(sb, form, st);
+          e = saber_dec(sb, form, sj);
           break;
       }
     }
     if (e != cudaSuccess) return cuda_status(e);
     if (tm) c->timer_stages = tm->n - 1;
     if (!dev) {
-      if ((e = cudaMemcpyAsync(out0 + first * out0_sz, d_out0, m * out0_sz, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      if ((e = cudaMemcpyAsync(out0 + first * out0_sz, d_out0, m * out0_sz, cudaMemcpyDeviceToHost, sj)) != cudaSuccess)
         return cuda_status(e);
       if (d_out1 &&
-          (e = cudaMemcpyAsync(out1 + first * out1_sz, d_out1, m * out1_sz, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+          (e = cudaMemcpyAsync(out1 + first * out1_sz, d_out1, m * out1_sz, cudaMemcpyDeviceToHost, sj)) != cudaSuccess)
         return cuda_status(e);
-      // The next chunk reuses the staging buffers: finish this one first.
-      if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_status(e);
+    }
+  }
+  if (npipe == 2) {  // join the pipeline back into the caller's stream
+    for (int j = 0; j < 2; j++) {
+      if ((e = cudaEventRecord(c->pev[j], streams[j])) != cudaSuccess) return cuda_status(e);
+      if ((e = cudaStreamWaitEvent(st, c->pev[j], 0)) != cudaSuccess) return cuda_status(e);
     }
   }
   if ((e = cudaEventRecord(c->last, st)) != cudaSuccess) return cuda_status(e);
@@ -311,6 +340,10 @@ int dpkem_ctx_create(dpkem_ctx **out, int device, size_t hbm_budget_bytes) {
   c->device = device;
   c->budget = hbm_budget_bytes ? hbm_budget_bytes : kDefaultBudget;
   for (int k = 0; k <= StageTimer::kMax; k++) cudaEventCreate(&c->timer.ev[k]);
+  for (int j = 0; j < 2; j++) {
+    cudaStreamCreateWithFlags(&c->pipe[j], cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&c->pev[j], cudaEventDisableTiming);
+  }
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->last, cudaEventDisableTiming) != cudaSuccess ||
       cudaMalloc(&c->d_err, 4) != cudaSuccess || cudaMemset(c->d_err, 0, 4) != cudaSuccess) {
@@ -330,6 +363,13 @@ int dpkem_ctx_destroy(dpkem_ctx *c) {
   if (c->arena) cudaFree(c->arena);
   if (c->d_err) cudaFree(c->d_err);
   if (c->last) cudaEventDestroy(c->last);
+  for (int j = 0; j < 2; j++) {
+    if (c->pipe[j]) {
+      cudaStreamSynchronize(c->pipe[j]);
+      cudaStreamDestroy(c->pipe[j]);
+    }
+    if (c->pev[j]) cudaEventDestroy(c->pev[j]);
+  }
   for (int k = 0; k <= StageTimer::kMax; k++)
     if (c->timer.ev[k]) cudaEventDestroy(c->timer.ev[k]);
   if (c->stream) cudaStreamDestroy(c->stream);

@@ -92,3 +92,19 @@ def test_reference_named_shims(oracle):
     with pytest.raises(d.DpkemError):
         d.saber_enc(1, k_enc, spk, c)
     d.set_compat(batch=768)
+
+
+@pytest.mark.parametrize("scheme,n", [(d.SABER, 1100), (d.FRODO976, 600)])
+def test_host_pipeline_matches_device_mode(engine, oracle, scheme, n):
+    """Host-mode batches of several chunks run on a two-stream copy/compute pipeline."""
+    z = d.sizes(scheme)
+    kc, ec = oracle.coins(n, z["kp_coins"], "kp", first=77), oracle.coins(n, z["enc_coins"], "enc", first=77)
+    pk, sk = engine.keypair(scheme, kc, d.FORM_TC)
+    ct, ss = engine.enc(scheme, pk, ec, d.FORM_TC)
+    ss2 = engine.dec(scheme, ct, sk, d.FORM_TC)
+    dpk, dsk = engine.keypair(scheme, torch.from_numpy(kc).cuda(), d.FORM_TC)
+    dct, dss = engine.enc(scheme, dpk, torch.from_numpy(ec).cuda(), d.FORM_TC)
+    torch.cuda.synchronize()
+    assert (dpk.cpu().numpy() == pk).all() and (dsk.cpu().numpy() == sk).all()
+    assert (dct.cpu().numpy() == ct).all() and (dss.cpu().numpy() == ss).all()
+    assert (ss2 == ss).all()
