@@ -33,8 +33,8 @@ struct dpkem_ctx {
   size_t budget = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t last = nullptr;
-  cudaStream_t pipe[2] = {nullptr, nullptr};  // host-mode copy/compute pipeline
-  cudaEvent_t pev[2] = {nullptr, nullptr};
+  cudaStream_t pipe[4] = {};  // host-mode copy/compute pipeline, one stream per chunk
+  cudaEvent_t pev[4] = {};
   uint8_t *arena = nullptr;
   size_t arena_bytes = 0;
   uint32_t *d_err = nullptr;
@@ -55,7 +55,7 @@ int set_status(int s) {
 
 constexpr size_t kAlign = 256;
 constexpr size_t kPipeChunkMin = 256;  // smallest chunk of a host-mode pipeline
-constexpr size_t kPipeChunks = 4;      // chunks per host-mode batch when pipelined
+constexpr int kPipeChunks = 4;         // chunks (and streams) per pipelined host-mode batch
 constexpr size_t kDefaultBudget = 8ull << 30;
 
 size_t up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
@@ -183,25 +183,29 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
   std::lock_guard<std::mutex> lock(c->mu);
   if (cudaSetDevice(c->device) != cudaSuccess) return cuda_status(cudaErrorInvalidDevice);
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
-  // Host-mode batches of at least two chunks run as a two-stream pipeline: chunks alternate
-  // between the context's pipeline streams (each with its own half of the arena), so the
-  // copies of one chunk overlap the kernels of the other.
+  // Host-mode batches of at least two minimum chunks, when the budget holds the whole batch,
+  // run as a pipeline: up to four chunks, each on its own stream with its own arena region,
+  // all in flight at once.  The copies of later chunks and their latency-bound first stages
+  // then overlap the long kernels of earlier chunks.
   size_t chunk = std::min(n, chunk_for(c, scheme, op, !dev));
   int npipe = 1;
   if (!dev && !c->profile && n >= 2 * kPipeChunkMin) {
-    npipe = 2;
-    chunk = std::min(std::max(kPipeChunkMin, (n + kPipeChunks - 1) / kPipeChunks), chunk_for(c, scheme, op, true) / 2);
-    if (chunk == 0) chunk = 1;
+    const int want = (int)std::min<size_t>(kPipeChunks, n / kPipeChunkMin);
+    const size_t each = (n + want - 1) / want;
+    if (each * want <= chunk_for(c, scheme, op, true) && want > 1) {
+      npipe = want;
+      chunk = each;
+    }
   }
   const size_t per_pipe = (arena_need(scheme, op, chunk, !dev) + kAlign - 1) & ~(kAlign - 1);
   int rc = ensure_arena(c, per_pipe * npipe);
   if (rc) return rc;
   cudaError_t e = cudaStreamWaitEvent(st, c->last, 0);
   if (e != cudaSuccess) return cuda_status(e);
-  cudaStream_t streams[2] = {st, st};
-  if (npipe == 2) {
+  cudaStream_t streams[kPipeChunks] = {st, st, st, st};
+  if (npipe > 1) {
     if ((e = cudaEventRecord(c->pev[0], st)) != cudaSuccess) return cuda_status(e);
-    for (int j = 0; j < 2; j++) {
+    for (int j = 0; j < npipe; j++) {
       streams[j] = c->pipe[j];
       if ((e = cudaStreamWaitEvent(streams[j], c->pev[0], 0)) != cudaSuccess) return cuda_status(e);
     }
@@ -303,8 +307,8 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
         return cuda_status(e);
     }
   }
-  if (npipe == 2) {  // join the pipeline back into the caller's stream
-    for (int j = 0; j < 2; j++) {
+  if (npipe > 1) {  // join the pipeline back into the caller's stream
+    for (int j = 0; j < npipe; j++) {
       if ((e = cudaEventRecord(c->pev[j], streams[j])) != cudaSuccess) return cuda_status(e);
       if ((e = cudaStreamWaitEvent(st, c->pev[j], 0)) != cudaSuccess) return cuda_status(e);
     }
@@ -340,7 +344,7 @@ int dpkem_ctx_create(dpkem_ctx **out, int device, size_t hbm_budget_bytes) {
   c->device = device;
   c->budget = hbm_budget_bytes ? hbm_budget_bytes : kDefaultBudget;
   for (int k = 0; k <= StageTimer::kMax; k++) cudaEventCreate(&c->timer.ev[k]);
-  for (int j = 0; j < 2; j++) {
+  for (int j = 0; j < 4; j++) {
     cudaStreamCreateWithFlags(&c->pipe[j], cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&c->pev[j], cudaEventDisableTiming);
   }
@@ -363,7 +367,7 @@ int dpkem_ctx_destroy(dpkem_ctx *c) {
   if (c->arena) cudaFree(c->arena);
   if (c->d_err) cudaFree(c->d_err);
   if (c->last) cudaEventDestroy(c->last);
-  for (int j = 0; j < 2; j++) {
+  for (int j = 0; j < 4; j++) {
     if (c->pipe[j]) {
       cudaStreamSynchronize(c->pipe[j]);
       cudaStreamDestroy(c->pipe[j]);
