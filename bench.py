@@ -14,7 +14,6 @@ no data-path collective); value = instances of all ranks / max-over-ranks time.
 from __future__ import annotations
 
 import argparse
-import datetime
 import json
 import os
 import statistics
@@ -50,10 +49,9 @@ def parse():
 
 
 def dist_env():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from dpcrypto_b200.dist import env
+
+    return env()
 
 
 def config(args, world):
@@ -183,19 +181,16 @@ def main():
     import dpcrypto_b200 as d
 
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import torch.distributed as dist
+    from dpcrypto_b200 import dist as D
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
-        pg = dist
+    pg = D.init("nccl", timeout_s=120.0, device=torch.device("cuda", local)) if world > 1 else None
     eng = d.Engine(local)
     form = d.FORM_TC if args.form == "tc" else d.FORM_DP4A
     B = args.batch
     stream = torch.cuda.current_stream()
 
     # ---- inputs: keypairs and coins generated on the device, untimed ----
-    first = rank * B
+    first, _ = D.shard(B, rank)
     kc = torch.empty((B, 64), dtype=torch.uint8, device="cuda")
     ec = torch.empty((B, 24), dtype=torch.uint8, device="cuda")
     eng.coins(B, 64, "kp", first=first, out=kc)
@@ -231,11 +226,7 @@ def main():
         t1.record(stream)
         barrier()
         eng.profile(False)
-        ms = t0.elapsed_time(t1)
-        if pg is not None:
-            x = torch.tensor([ms], device="cuda")
-            pg.all_reduce(x, op=pg.ReduceOp.MAX)
-            ms = float(x.item())
+        ms = D.max_over_ranks(t0.elapsed_time(t1), device="cuda")
         return ms, stages
 
     for _ in range(args.warmup):
@@ -393,11 +384,7 @@ def main():
         for _ in range(args.steps):
             eng.enc(d.FRODO976, h_pk, h_ec, form, out=(h_ct, h_ss))
             eng.dec(d.FRODO976, h_ct, h_sk, form, out=h_ss2)
-        el = time.perf_counter() - t
-        if pg is not None:
-            x = torch.tensor([el], device="cuda", dtype=torch.float64)
-            pg.all_reduce(x, op=pg.ReduceOp.MAX)
-            el = float(x.item())
+        el = D.max_over_ranks(time.perf_counter() - t, device="cuda")
         line["e2e"] = {"value": world * B * args.steps / el, "unit": UNIT,
                        "h2d_bytes_per_step": B * (15632 + 24 + 15744 + 31296),
                        "d2h_bytes_per_step": B * (15744 + 24 + 24),
