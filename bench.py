@@ -304,6 +304,15 @@ def main():
             for _ in range(3):
                 eng.enc(d.SABER, spk, sec, f, out=(sct, sss))
                 eng.dec(d.SABER, sct, ssk, f, out=sss2)
+            # stage times (enc: prologue, product, finish; dec: inner product, prologue, product, finish)
+            eng.profile(True)
+            eng.enc(d.SABER, spk, sec, f, out=(sct, sss))
+            es = eng.stage_times()
+            eng.dec(d.SABER, sct, ssk, f, out=sss2)
+            ds = eng.stage_times()
+            eng.profile(False)
+            sres[name + "_stage_ms"] = {"enc": es, "dec": ds}
+            sres[name + "_product_ms"] = es[1] + ds[0] + ds[2]
             barrier()
             reps = 50
             t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -316,6 +325,7 @@ def main():
             sres[name] = SB * reps / (t0.elapsed_time(t1) * 1e-3)
             sres[name + "_roundtrip_ok"] = bool(torch.equal(sss, sss2))
         sres["tc_over_dp4a"] = sres["tc"] / sres["dp4a"]
+        sres["product_stage_tc_over_dp4a"] = sres["dp4a_product_ms"] / sres["tc_product_ms"]
         line["saber_l3_batch4096"] = dict(sres, unit=UNIT)
 
     # ---- mixed persistent batch: 16384 requests, 4 schemes x 3 ops, one CUDA-graph launch ----
