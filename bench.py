@@ -41,7 +41,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batch", type=int, default=8192)
-    p.add_argument("--form", default="tc", choices=["tc", "dp4a"])
+    p.add_argument("--form", default="tc", choices=["tc", "dp4a", "int32"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-secondary", action="store_true")
@@ -185,7 +185,7 @@ def main():
 
     pg = D.init("nccl", timeout_s=120.0, device=torch.device("cuda", local)) if world > 1 else None
     eng = d.Engine(local)
-    form = d.FORM_TC if args.form == "tc" else d.FORM_DP4A
+    form = {"tc": d.FORM_TC, "dp4a": d.FORM_DP4A, "int32": d.FORM_INT32}[args.form]
     B = args.batch
     stream = torch.cuda.current_stream()
 
@@ -258,12 +258,13 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u8xs8->s32 (tcgen05 kind::i8), u64 Keccak lanes" if form == d.FORM_TC else "s16xs8->s32 (dp2a)",
+        "dtype": {d.FORM_TC: "u8xs8->s32 (tcgen05 kind::i8), u64 Keccak lanes", d.FORM_DP4A: "s16xs8->s32 (dp2a)",
+                  d.FORM_INT32: "int32 multiply-add"}[form],
         "data": "synthetic (seeded SHAKE256 coins, keypairs generated on the GPU)", "config": config(args, world),
         "bit_exact_roundtrip": ok, "gpu_launches": 7 * args.steps,
         "roofline": {
             "kernel": "sa_tc_kernel (SHAKE128 A rows in registers -> int8 tcgen05 S'A)" if form == d.FORM_TC
-            else "sa_dp4a_kernel", "bound": "int", "unit": "Gop/s",
+            else "sa_dp4a_kernel" + ("<int32>" if form == d.FORM_INT32 else ""), "bound": "int", "unit": "Gop/s",
             "achieved": achieved, "peak": int_peak / 1e9, "frac": achieved * 1e9 / int_peak,
             "peak_source": "measured in-process: LOP3/SHF issue rate in Keccak's mix (dpkem_probe_int_peaks)",
             "algorithmic": f"{KECCAK_INT_OPS} int32 ops per Keccak-f x 12 per A row x 976 rows x batch",
@@ -275,20 +276,25 @@ def main():
         "clocks": clocks,
     }
 
-    # ---- comparison form (dp4a vs tc) on the same GPU ----
+    # ---- the other product forms (tc / dp4a / int32) on the same GPU ----
     if not args.no_secondary:
-        other = d.FORM_DP4A if form == d.FORM_TC else d.FORM_TC
-        for _ in range(2):
-            step(other)
-        oms, ostages = timed(other, max(3, args.steps // 2), profile=True)
-        ovalue = world * B * max(3, args.steps // 2) / (oms * 1e-3)
-        o_sa = statistics.mean([s[1] for s in ostages["enc"]] + [s[2] for s in ostages["dec"]])
-        line["forms"] = {
-            "tc": value if form == d.FORM_TC else ovalue, "dp4a": ovalue if form == d.FORM_TC else value,
-            "sa_kernel_ms": {"tc": sa_avg if form == d.FORM_TC else o_sa, "dp4a": o_sa if form == d.FORM_TC else sa_avg},
-        }
-        line["forms"]["tc_over_dp4a"] = line["forms"]["tc"] / line["forms"]["dp4a"]
-        line["forms"]["product_stage_tc_over_dp4a"] = line["forms"]["sa_kernel_ms"]["dp4a"] / line["forms"]["sa_kernel_ms"]["tc"]
+        fnames = {d.FORM_TC: "tc", d.FORM_DP4A: "dp4a", d.FORM_INT32: "int32"}
+        forms = {fnames[form]: value}
+        sa_k = {fnames[form]: sa_avg}
+        for other in (d.FORM_TC, d.FORM_DP4A, d.FORM_INT32):
+            if other == form:
+                continue
+            for _ in range(2):
+                step(other)
+            osteps = max(3, args.steps // 2)
+            oms, ostages = timed(other, osteps, profile=True)
+            forms[fnames[other]] = world * B * osteps / (oms * 1e-3)
+            sa_k[fnames[other]] = statistics.mean([s[1] for s in ostages["enc"]] + [s[2] for s in ostages["dec"]])
+        line["forms"] = dict(forms, sa_kernel_ms=sa_k)
+        line["forms"]["tc_over_dp4a"] = forms["tc"] / forms["dp4a"]
+        line["forms"]["tc_over_int32"] = forms["tc"] / forms["int32"]
+        line["forms"]["product_stage_tc_over_dp4a"] = sa_k["dp4a"] / sa_k["tc"]
+        line["forms"]["product_stage_tc_over_int32"] = sa_k["int32"] / sa_k["tc"]
         # Saber l=3, batch 4096 (configs' second workload)
         SB = 4096
         skc = torch.empty((SB, 96), dtype=torch.uint8, device="cuda")
@@ -300,7 +306,7 @@ def main():
         sss = torch.empty((SB, 32), dtype=torch.uint8, device="cuda")
         sss2 = torch.empty((SB, 32), dtype=torch.uint8, device="cuda")
         sres = {}
-        for name, f in (("tc", d.FORM_TC), ("dp4a", d.FORM_DP4A)):
+        for name, f in (("tc", d.FORM_TC), ("dp4a", d.FORM_DP4A), ("int32", d.FORM_INT32)):
             for _ in range(3):
                 eng.enc(d.SABER, spk, sec, f, out=(sct, sss))
                 eng.dec(d.SABER, sct, ssk, f, out=sss2)
@@ -326,6 +332,8 @@ def main():
             sres[name + "_roundtrip_ok"] = bool(torch.equal(sss, sss2))
         sres["tc_over_dp4a"] = sres["tc"] / sres["dp4a"]
         sres["product_stage_tc_over_dp4a"] = sres["dp4a_product_ms"] / sres["tc_product_ms"]
+        sres["tc_over_int32"] = sres["tc"] / sres["int32"]
+        sres["product_stage_tc_over_int32"] = sres["int32_product_ms"] / sres["tc_product_ms"]
         line["saber_l3_batch4096"] = dict(sres, unit=UNIT)
 
     # ---- mixed persistent batch: 16384 requests, 4 schemes x 3 ops, one CUDA-graph launch ----
@@ -334,7 +342,7 @@ def main():
 
         mb = MixedBatch(eng, 16384, seed=0, first=rank * 1000000)
         mres = {"requests": mb.n, "unit": "KEM ops/s", "counts": mb.counts}
-        for name, f in (("tc", d.FORM_TC), ("dp4a", d.FORM_DP4A)):
+        for name, f in (("tc", d.FORM_TC), ("dp4a", d.FORM_DP4A), ("int32", d.FORM_INT32)):
             g = eng.mixed_graph(mb.items, f)
             for _ in range(2):
                 g.launch()

@@ -174,7 +174,6 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
   Sizes z;
   if (!c || !scheme_sizes(scheme, &z)) return DPKEM_EINVAL;
   if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC && form != DPKEM_FORM_INT32) return DPKEM_EINVAL;
-  if (form == DPKEM_FORM_INT32) return DPKEM_EUNSUPPORTED;
   if (n == 0) return DPKEM_OK;
   if (n > (size_t)INT32_MAX) return DPKEM_EINVAL;
   if (!in0 || !out0 || (op != OP_KEYPAIR && !in1) || (op != OP_DEC && !out1)) return DPKEM_EINVAL;
@@ -432,8 +431,7 @@ static int check_requests(size_t n, const dpkem_request *reqs) {
 
 int dpkem_mixed_batch(dpkem_ctx *c, int form, size_t n, const dpkem_request *reqs, void *stream) {
   if (!c) return set_status(DPKEM_EINVAL);
-  if (form == DPKEM_FORM_INT32) return set_status(DPKEM_EUNSUPPORTED);
-  if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC) return set_status(DPKEM_EINVAL);
+  if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC && form != DPKEM_FORM_INT32) return set_status(DPKEM_EINVAL);
   if (n == 0) return set_status(DPKEM_OK);
   int rc = check_requests(n, reqs);
   if (rc) return set_status(rc);
@@ -477,8 +475,7 @@ int dpkem_mixed_graph_destroy(dpkem_graph *g) {
 int dpkem_mixed_graph_create(dpkem_ctx *c, int form, size_t n, const dpkem_request *reqs, dpkem_graph **out) {
   if (!c || !out) return set_status(DPKEM_EINVAL);
   *out = nullptr;
-  if (form == DPKEM_FORM_INT32) return set_status(DPKEM_EUNSUPPORTED);
-  if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC) return set_status(DPKEM_EINVAL);
+  if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC && form != DPKEM_FORM_INT32) return set_status(DPKEM_EINVAL);
   int rc = check_requests(n, reqs);
   if (rc) return set_status(rc);
   std::lock_guard<std::mutex> lock(c->mu);

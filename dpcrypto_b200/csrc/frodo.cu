@@ -47,10 +47,10 @@ __global__ void __launch_bounds__(256) dec_w_kernel(FrodoBatch b) {
   fdev::dec_w_cta(inst_of(b, blockIdx.x, OP_DEC), smem);
 }
 
-template <int MODE>
+template <int MODE, bool I32>
 __global__ void __launch_bounds__(256, 2) sa_dp4a_kernel(FrodoBatch b) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  fdev::sa_dp4a_cta<MODE>(inst_of(b, blockIdx.x, MODE), smem);
+  fdev::sa_dp4a_cta<MODE, I32>(inst_of(b, blockIdx.x, MODE), smem);
 }
 
 template <int MODE, int NST>
@@ -75,9 +75,10 @@ __global__ void __launch_bounds__(256, 2) sa_tc_kernel(FrodoBatch b) {
   }
 }
 
+template <bool I32>
 __global__ void __launch_bounds__(256, 2) kp_as_dp4a_kernel(FrodoBatch b) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  fdev::kp_as_dp4a_cta(inst_of(b, blockIdx.x, OP_KEYPAIR), smem);
+  fdev::kp_as_dp4a_cta<I32>(inst_of(b, blockIdx.x, OP_KEYPAIR), smem);
 }
 
 __global__ void __launch_bounds__(256, 2) kp_as_tc_kernel(FrodoBatch b) {
@@ -116,9 +117,12 @@ cudaError_t launch_sa(const FrodoBatch &b, int form, cudaStream_t st) {
     constexpr int bytes = fdev::TcLayout<kTcStages>::total;
     if ((e = set_smem(sa_tc_kernel<MODE, kTcStages>, bytes)) != cudaSuccess) return e;
     sa_tc_kernel<MODE, kTcStages><<<b.n, 256, bytes, st>>>(b);
+  } else if (form == FORM_INT32) {
+    if ((e = set_smem(sa_dp4a_kernel<MODE, true>, fdev::DP4A_SMEM)) != cudaSuccess) return e;
+    sa_dp4a_kernel<MODE, true><<<b.n, 256, fdev::DP4A_SMEM, st>>>(b);
   } else {
-    if ((e = set_smem(sa_dp4a_kernel<MODE>, fdev::DP4A_SMEM)) != cudaSuccess) return e;
-    sa_dp4a_kernel<MODE><<<b.n, 256, fdev::DP4A_SMEM, st>>>(b);
+    if ((e = set_smem(sa_dp4a_kernel<MODE, false>, fdev::DP4A_SMEM)) != cudaSuccess) return e;
+    sa_dp4a_kernel<MODE, false><<<b.n, 256, fdev::DP4A_SMEM, st>>>(b);
   }
   return cudaGetLastError();
 }
@@ -139,8 +143,10 @@ cudaError_t frodo_keypair(const FrodoBatch &b, int form, cudaStream_t st) {
     cudaError_t e = set_smem(kp_as_tc_kernel, fdev::KptLayout::total);
     if (e != cudaSuccess) return e;
     kp_as_tc_kernel<<<b.n, 256, fdev::KptLayout::total, st>>>(b);
+  } else if (form == FORM_INT32) {
+    kp_as_dp4a_kernel<true><<<b.n, 256, fdev::KP_AS_SMEM, st>>>(b);
   } else {
-    kp_as_dp4a_kernel<<<b.n, 256, fdev::KP_AS_SMEM, st>>>(b);
+    kp_as_dp4a_kernel<false><<<b.n, 256, fdev::KP_AS_SMEM, st>>>(b);
   }
   mark(b, st);
   pk_hash_kernel<OP_KEYPAIR><<<blocks_for(b.n, tb), tb, 0, st>>>(b);

@@ -318,7 +318,9 @@ __device__ __forceinline__ uint32_t finish_c(const Inst &v, SVal sval, uint32_t 
 // dp2a (16-bit A halves x 8-bit S'), flushing column partial sums with shared atomics.
 constexpr int DP4A_SMEM = 83200 + 4 * 64 * 4;
 
-template <int MODE>
+// I32 = true is the plain INT32 form (FrodoKEM976-GPU/src/matrix_kernel.cu:75-111, the
+// reference's non-DP path): the same tiles, 32-bit multiply-adds instead of dp2a.
+template <int MODE, bool I32 = false>
 __device__ __forceinline__ void sa_dp4a_cta(const Inst &v, uint8_t *smem) {
   uint32_t *acc = reinterpret_cast<uint32_t *>(smem);             // [8][976]
   uint32_t *sp8 = reinterpret_cast<uint32_t *>(smem + 31232);     // [248 quads][8 k]: S'[k][4q..4q+3]
@@ -365,10 +367,24 @@ __device__ __forceinline__ void sa_dp4a_cta(const Inst &v, uint8_t *smem) {
           const uint4 s0 = *reinterpret_cast<const uint4 *>(sp8 + (8 * c + rq) * 8);
           const uint4 s1 = *reinterpret_cast<const uint4 *>(sp8 + (8 * c + rq) * 8 + 4);
           const int sv[8] = {(int)s0.x, (int)s0.y, (int)s0.z, (int)s0.w, (int)s1.x, (int)s1.y, (int)s1.z, (int)s1.w};
+          if (I32) {
+            const uint32_t xr[4] = {x0, x1, x2, x3};
 #pragma unroll
-          for (int k = 0; k < 8; k++) {
-            alo[k] = dp2a_hi(p23l, sv[k], dp2a_lo(p01l, sv[k], alo[k]));
-            ahi[k] = dp2a_hi(p23h, sv[k], dp2a_lo(p01h, sv[k], ahi[k]));
+            for (int r = 0; r < 4; r++) {
+              const int lo = (int)(xr[r] & 0xFFFFu), hi = (int)(xr[r] >> 16);
+#pragma unroll
+              for (int k = 0; k < 8; k++) {
+                const int sk = (int)(int8_t)(sv[k] >> (8 * r));
+                alo[k] += lo * sk;
+                ahi[k] += hi * sk;
+              }
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+              alo[k] = dp2a_hi(p23l, sv[k], dp2a_lo(p01l, sv[k], alo[k]));
+              ahi[k] = dp2a_hi(p23h, sv[k], dp2a_lo(p01h, sv[k], ahi[k]));
+            }
           }
         }
         const int i0 = 84 * blk + 2 * w;
@@ -548,6 +564,7 @@ __device__ __forceinline__ bool sa_tc_cta(const Inst &v, uint8_t *smem, uint32_t
 // 8 rows of S^T (broadcast from shared memory), so B[j][k] accumulates in registers.
 constexpr int KP_AS_SMEM = 12 * 21 * 8 * 4;
 
+template <bool I32 = false>
 __device__ __forceinline__ void kp_as_dp4a_cta(const Inst &v, uint8_t *smem) {
   uint32_t *st8 = reinterpret_cast<uint32_t *>(smem);  // [blk][q][k]: S^T[k][84 blk + 4q .. +3]
   const int tid = threadIdx.x;
@@ -576,8 +593,17 @@ __device__ __forceinline__ void kp_as_dp4a_cta(const Inst &v, uint8_t *smem) {
         const uint4 s0 = *reinterpret_cast<const uint4 *>(st8 + (blk * 21 + q) * 8);
         const uint4 s1 = *reinterpret_cast<const uint4 *>(st8 + (blk * 21 + q) * 8 + 4);
         const int sv[8] = {(int)s0.x, (int)s0.y, (int)s0.z, (int)s0.w, (int)s1.x, (int)s1.y, (int)s1.z, (int)s1.w};
+        if (I32) {
+          const int c0 = (int)(a[q].x & 0xFFFFu), c1 = (int)(a[q].x >> 16), c2 = (int)(a[q].y & 0xFFFFu),
+                    c3 = (int)(a[q].y >> 16);
 #pragma unroll
-        for (int k = 0; k < 8; k++) acc[k] = dp2a_hi((int)a[q].y, sv[k], dp2a_lo((int)a[q].x, sv[k], acc[k]));
+          for (int k = 0; k < 8; k++)
+            acc[k] += c0 * (int)(int8_t)sv[k] + c1 * (int)(int8_t)(sv[k] >> 8) + c2 * (int)(int8_t)(sv[k] >> 16) +
+                      c3 * (sv[k] >> 24);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 8; k++) acc[k] = dp2a_hi((int)a[q].y, sv[k], dp2a_lo((int)a[q].x, sv[k], acc[k]));
+        }
       }
     }
     uint32_t x[8];

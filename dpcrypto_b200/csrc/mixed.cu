@@ -31,14 +31,14 @@ namespace dpkem {
 namespace mixed {
 namespace {
 
-// ---- stage codes: scheme * 64 + op * 16 + stage * 2 + form ----
+// ---- stage codes: scheme * 128 + op * 32 + stage * 4 + form ----
 __host__ __device__ constexpr int code_of(int scheme, int op, int stage, int form) {
-  return scheme * 64 + op * 16 + stage * 2 + (form == FORM_TC ? 1 : 0);
+  return scheme * 128 + op * 32 + stage * 4 + form;
 }
-__host__ __device__ constexpr int scheme_of(int code) { return code >> 6; }
-__host__ __device__ constexpr int op_of(int code) { return (code >> 4) & 3; }
-__host__ __device__ constexpr int stage_of(int code) { return (code >> 1) & 7; }
-__host__ __device__ constexpr bool tc_of(int code) { return code & 1; }
+__host__ __device__ constexpr int scheme_of(int code) { return code >> 7; }
+__host__ __device__ constexpr int op_of(int code) { return (code >> 5) & 3; }
+__host__ __device__ constexpr int stage_of(int code) { return (code >> 2) & 7; }
+__host__ __device__ constexpr int form_of(int code) { return code & 3; }
 
 // Stage kinds: 0 = thread (one instance per thread), 2 = thread with two roles (instance
 // t on threads t and t + 128: Saber's two prologue sponges, Frodo decaps' prologue and
@@ -195,14 +195,15 @@ __device__ __forceinline__ void thread_stage(int code, const DevReq &r, int role
 }
 
 template <int L, int MODE>
-__device__ __forceinline__ void saber_product(bool tc, const sdev::Inst &v, uint8_t *smem, uint32_t tbase,
+__device__ __forceinline__ void saber_product(int form, const sdev::Inst &v, uint8_t *smem, uint32_t tbase,
                                               uint32_t *err) {
-  if (tc) sdev::product_tc_cta<L, MODE>(v, smem, tbase, err);
-  else sdev::product_dp4a_cta<L, MODE>(v, smem);
+  if (form == FORM_TC) sdev::product_tc_cta<L, MODE>(v, smem, tbase, err);
+  else if (form == FORM_INT32) sdev::product_dp4a_cta<L, MODE, true>(v, smem);
+  else sdev::product_dp4a_cta<L, MODE, false>(v, smem);
 }
 
 template <int L>
-__device__ __forceinline__ void saber_cta(int op, int stage, bool tc, const DevReq &r, uint8_t *smem, uint32_t tbase,
+__device__ __forceinline__ void saber_cta(int op, int stage, int tc, const DevReq &r, uint8_t *smem, uint32_t tbase,
                                           uint32_t *err) {
   const sdev::Inst v = saber_view<L>(r);
   if (op == OP_KEYPAIR) saber_product<L, sdev::PM_KEYPAIR>(tc, v, smem, tbase, err);
@@ -215,20 +216,23 @@ constexpr int kTcStages = 2;
 
 __device__ __forceinline__ void cta_stage(int code, const DevReq &r, uint8_t *smem, uint32_t tbase, uint32_t *err) {
   const int scheme = scheme_of(code), op = op_of(code), stage = stage_of(code);
-  const bool tc = tc_of(code);
+  const int tc = form_of(code);  // product form (FORM_DP4A / FORM_INT32 / FORM_TC)
   if (scheme == 0) {
     const fdev::Inst v = frodo_view(r);
     if (op == OP_KEYPAIR) {
-      if (tc) fdev::kp_as_tc_cta(v, smem, tbase, err);
-      else fdev::kp_as_dp4a_cta(v, smem);
+      if (tc == FORM_TC) fdev::kp_as_tc_cta(v, smem, tbase, err);
+      else if (tc == FORM_INT32) fdev::kp_as_dp4a_cta<true>(v, smem);
+      else fdev::kp_as_dp4a_cta<false>(v, smem);
     } else if (op == OP_ENC) {
-      if (tc) fdev::sa_tc_cta<OP_ENC, kTcStages>(v, smem, tbase, err);
-      else fdev::sa_dp4a_cta<OP_ENC>(v, smem);
+      if (tc == FORM_TC) fdev::sa_tc_cta<OP_ENC, kTcStages>(v, smem, tbase, err);
+      else if (tc == FORM_INT32) fdev::sa_dp4a_cta<OP_ENC, true>(v, smem);
+      else fdev::sa_dp4a_cta<OP_ENC, false>(v, smem);
     } else if (stage == 0) {
       fdev::dec_w_cta(v, smem);
     } else {
-      if (tc) fdev::sa_tc_cta<OP_DEC, kTcStages>(v, smem, tbase, err);
-      else fdev::sa_dp4a_cta<OP_DEC>(v, smem);
+      if (tc == FORM_TC) fdev::sa_tc_cta<OP_DEC, kTcStages>(v, smem, tbase, err);
+      else if (tc == FORM_INT32) fdev::sa_dp4a_cta<OP_DEC, true>(v, smem);
+      else fdev::sa_dp4a_cta<OP_DEC, false>(v, smem);
     }
   } else if (scheme == 2) {
     saber_cta<2>(op, stage, tc, r, smem, tbase, err);

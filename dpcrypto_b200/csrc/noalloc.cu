@@ -43,7 +43,7 @@ bool aligned8(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 7u) == 0
 extern "C" int dpkem_saber_enc_batch_static(int scheme, int form, size_t n, const uint8_t *coins, const uint8_t *pk,
                                             uint8_t *ct, uint8_t *ss, void *stream) {
   if (scheme < DPKEM_LIGHTSABER || scheme > DPKEM_FIRESABER) return DPKEM_EINVAL;
-  if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC) return form == DPKEM_FORM_INT32 ? DPKEM_EUNSUPPORTED : DPKEM_EINVAL;
+  if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC && form != DPKEM_FORM_INT32) return DPKEM_EINVAL;
   if (n > kMaxInst) return DPKEM_EINVAL;  // larger batches: split them, or use dpkem_enc_batch
   if (n == 0) return DPKEM_OK;
   if (!coins || !pk || !ct || !ss || !aligned8(coins) || !aligned8(pk) || !aligned8(ct) || !aligned8(ss))

@@ -27,10 +27,10 @@ __host__ __device__ constexpr int op_of(int mode) {
   return mode == sdev::PM_KEYPAIR ? OP_KEYPAIR : mode == sdev::PM_ENC ? OP_ENC : OP_DEC;
 }
 
-template <int L, int MODE>
+template <int L, int MODE, bool I32>
 __global__ void __launch_bounds__(256) product_dp4a_kernel(SaberBatch b) {
   extern __shared__ __align__(1024) uint8_t sm[];
-  sdev::product_dp4a_cta<L, MODE>(inst_of<L>(b, blockIdx.x, op_of(MODE)), sm);
+  sdev::product_dp4a_cta<L, MODE, I32>(inst_of<L>(b, blockIdx.x, op_of(MODE)), sm);
 }
 
 template <int L, int MODE>
@@ -68,10 +68,14 @@ cudaError_t launch_product(const SaberBatch &b, int form, cudaStream_t st) {
     constexpr int bytes = Y::TC_TOTAL;
     if ((e = prep(product_tc_kernel<L, MODE>, bytes)) != cudaSuccess) return e;
     product_tc_kernel<L, MODE><<<b.n, 256, bytes, st>>>(b);
+  } else if (form == FORM_INT32) {
+    constexpr int bytes = Y::COMMON;
+    if ((e = prep(product_dp4a_kernel<L, MODE, true>, bytes)) != cudaSuccess) return e;
+    product_dp4a_kernel<L, MODE, true><<<b.n, 256, bytes, st>>>(b);
   } else {
     constexpr int bytes = Y::COMMON;
-    if ((e = prep(product_dp4a_kernel<L, MODE>, bytes)) != cudaSuccess) return e;
-    product_dp4a_kernel<L, MODE><<<b.n, 256, bytes, st>>>(b);
+    if ((e = prep(product_dp4a_kernel<L, MODE, false>, bytes)) != cudaSuccess) return e;
+    product_dp4a_kernel<L, MODE, false><<<b.n, 256, bytes, st>>>(b);
   }
   return cudaGetLastError();
 }

@@ -406,7 +406,9 @@ __device__ __forceinline__ void epilogue(const Inst &v, uint8_t *sm) {
 // Secret j's reversed sign-extended window R_j[t] = s_ext[255 - t], t in [0, 512), with
 // s_ext[d] = s[d] (d >= 0), -s[d + 256] (d < 0): coefficient i of s*P is
 // sum_m P[m] R_j[255 - i + m].
-template <int L, int MODE>
+// I32 = true is the INT32 schoolbook form (SABER-GPU/src/poly.cu:209-358, the reference's
+// mode 1): the same window, one 32-bit multiply-add per coefficient pair instead of dp2a.
+template <int L, int MODE, bool I32 = false>
 __device__ __forceinline__ void product_dp4a_cta(const Inst &v, uint8_t *sm) {
   using Y = PL<L>;
   constexpr int NO = n_out<L, MODE>();
@@ -437,10 +439,21 @@ __device__ __forceinline__ void product_dp4a_cta(const Inst &v, uint8_t *sm) {
       const uint32_t w1 = rw[wb + mq + 1];
       const int win = (int)__funnelshift_r(w0, w1, sh);
       w0 = w1;
+      if (I32) {
+        const int s0 = (int)(int8_t)win, s1 = (int)(int8_t)(win >> 8), s2 = (int)(int8_t)(win >> 16),
+                  s3 = win >> 24;
 #pragma unroll
-      for (int o = 0; o < NO; o++) {
-        const uint2 pw = pp[o][mq];
-        acc[o] = dp2a_hi((int)pw.y, win, dp2a_lo((int)pw.x, win, acc[o]));
+        for (int o = 0; o < NO; o++) {
+          const uint2 pw = pp[o][mq];
+          acc[o] += (int)(pw.x & 0xFFFFu) * s0 + (int)(pw.x >> 16) * s1 + (int)(pw.y & 0xFFFFu) * s2 +
+                    (int)(pw.y >> 16) * s3;
+        }
+      } else {
+#pragma unroll
+        for (int o = 0; o < NO; o++) {
+          const uint2 pw = pp[o][mq];
+          acc[o] = dp2a_hi((int)pw.y, win, dp2a_lo((int)pw.x, win, acc[o]));
+        }
       }
     }
   }

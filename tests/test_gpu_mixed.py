@@ -46,7 +46,7 @@ def _mixed_case(engine, per_kind, seed, form):
     return [items[k] for k in order], [expect[k] for k in order]
 
 
-@pytest.mark.parametrize("form", [d.FORM_TC, d.FORM_DP4A])
+@pytest.mark.parametrize("form", [d.FORM_TC, d.FORM_DP4A, d.FORM_INT32])
 def test_mixed_equals_batched(engine, form):
     items, expect = _mixed_case(engine, 5, 1, form)
     engine.mixed(items, form)

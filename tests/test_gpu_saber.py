@@ -6,7 +6,7 @@ import pytest
 import dpcrypto_b200 as d
 
 pytestmark = pytest.mark.gpu
-FORMS = [d.FORM_DP4A, d.FORM_TC]
+FORMS = [d.FORM_DP4A, d.FORM_INT32, d.FORM_TC]
 LEVELS = [2, 3, 4]
 
 
