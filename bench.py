@@ -108,6 +108,22 @@ def run_reference(args, world, rank):
 
 
 # ---------------------------------------------------------------- GPU helpers
+def pcie_gbs(h2d: bool, nbytes: int = 256 << 20) -> float:
+    """Pinned host<->device copy bandwidth (GB/s) of one 256 MiB buffer, CUDA-event timed."""
+    import torch
+
+    h = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    g = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for k in range(4):
+        if k == 1:
+            a.record()
+        (g.copy_(h, non_blocking=True) if h2d else h.copy_(g, non_blocking=True))
+    b.record()
+    b.synchronize()
+    return 3 * nbytes / (a.elapsed_time(b) * 1e-3) / 1e9
+
+
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -380,7 +396,8 @@ def main():
                     pool.clear()
                     r = srv.run(pool, poisson_arrivals(pool.n, rate=frac * peak, seed=int(frac * 100)))
                     levels.append({"load": frac, "offered_per_s": frac * peak, "ops_per_s": r["ops_per_s"],
-                                   "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "mean_batch": r["mean_batch"]})
+                                   "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "mean_batch": r["mean_batch"],
+                                   "host_max_gap_ms": r["host_max_gap_ms"]})
                 torch.cuda.synchronize()
                 serving[name] = {"peak_ops_per_s": peak, "levels": levels, "bit_exact": pool.check()}
             finally:
@@ -403,18 +420,22 @@ def main():
             eng.enc(d.FRODO976, h_pk, h_ec, form, out=(h_ct, h_ss))
             eng.dec(d.FRODO976, h_ct, h_sk, form, out=h_ss2)
         el = D.max_over_ranks(time.perf_counter() - t, device="cuda")
+        h2d_b, d2h_b = B * (15632 + 24 + 15744 + 31296), B * (15744 + 24 + 24)
+        h2d_gbs, d2h_gbs = pcie_gbs(True), pcie_gbs(False)
         line["e2e"] = {"value": world * B * args.steps / el, "unit": UNIT,
-                       "h2d_bytes_per_step": B * (15632 + 24 + 15744 + 31296),
-                       "d2h_bytes_per_step": B * (15744 + 24 + 24),
-                       "roundtrip_ok": bool((h_ss == h_ss2).all())}
+                       "h2d_bytes_per_step": h2d_b, "d2h_bytes_per_step": d2h_b,
+                       "roundtrip_ok": bool((h_ss == h_ss2).all()),
+                       "pipeline_chunks": d.kem.get_tuning().get("pipe_chunks"),
+                       "pcie_gbs": {"h2d": h2d_gbs, "d2h": d2h_gbs},
+                       "copy_ms_per_step_if_serial": 1e3 * (h2d_b / (h2d_gbs * 1e9) + d2h_b / (d2h_gbs * 1e9))}
 
     # ---- CPU baseline: the oracle on the host cores, rank 0 at N=1 ----
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        n_inst = 4 * threads
+        n_inst = 24 * threads
         cv, dt = cpu_sample(n_inst, threads)
         line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"{n_inst} FrodoKEM-976 encaps+decaps (4 per host thread), "
+                                "sample": f"{n_inst} FrodoKEM-976 encaps+decaps (24 per host thread), "
                                           f"oracle C restatement, {dt:.1f} s wall",
                                 "note": "reported baseline, not the target"}
 

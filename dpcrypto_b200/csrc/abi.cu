@@ -33,8 +33,8 @@ struct dpkem_ctx {
   size_t budget = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t last = nullptr;
-  cudaStream_t pipe[4] = {};  // host-mode copy/compute pipeline, one stream per chunk
-  cudaEvent_t pev[4] = {};
+  cudaStream_t pipe[8] = {};  // host-mode copy/compute pipeline, one stream per chunk
+  cudaEvent_t pev[8] = {};
   uint8_t *arena = nullptr;
   size_t arena_bytes = 0;
   uint32_t *d_err = nullptr;
@@ -55,7 +55,7 @@ int set_status(int s) {
 
 constexpr size_t kAlign = 256;
 constexpr size_t kPipeChunkMin = 256;  // smallest chunk of a host-mode pipeline
-constexpr int kPipeChunks = 4;         // chunks (and streams) per pipelined host-mode batch
+constexpr int kPipeChunks = 8;         // most chunks (and streams) of a pipelined host-mode batch
 constexpr size_t kDefaultBudget = 8ull << 30;
 
 size_t up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
@@ -101,7 +101,8 @@ int ensure_arena(dpkem_ctx *c, size_t bytes) {
   if (bytes <= c->arena_bytes) return DPKEM_OK;
   if (bytes > c->budget) return DPKEM_ENOMEM;
   if (c->arena) {
-    cudaStreamSynchronize(c->stream);
+    // c->last follows every launch that used the arena, on whichever stream it ran
+    cudaEventSynchronize(c->last);
     cudaFree(c->arena);
     c->arena = nullptr;
     c->arena_bytes = 0;
@@ -189,7 +190,7 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
   size_t chunk = std::min(n, chunk_for(c, scheme, op, !dev));
   int npipe = 1;
   if (!dev && !c->profile && n >= 2 * kPipeChunkMin) {
-    const int want = (int)std::min<size_t>(kPipeChunks, n / kPipeChunkMin);
+    const int want = (int)std::min<size_t>(std::min(tuning().pipe_chunks, kPipeChunks), n / kPipeChunkMin);
     const size_t each = (n + want - 1) / want;
     if (each * want <= chunk_for(c, scheme, op, true) && want > 1) {
       npipe = want;
@@ -201,7 +202,8 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
   if (rc) return rc;
   cudaError_t e = cudaStreamWaitEvent(st, c->last, 0);
   if (e != cudaSuccess) return cuda_status(e);
-  cudaStream_t streams[kPipeChunks] = {st, st, st, st};
+  cudaStream_t streams[kPipeChunks];
+  for (int j = 0; j < kPipeChunks; j++) streams[j] = st;
   if (npipe > 1) {
     if ((e = cudaEventRecord(c->pev[0], st)) != cudaSuccess) return cuda_status(e);
     for (int j = 0; j < npipe; j++) {
@@ -343,7 +345,7 @@ int dpkem_ctx_create(dpkem_ctx **out, int device, size_t hbm_budget_bytes) {
   c->device = device;
   c->budget = hbm_budget_bytes ? hbm_budget_bytes : kDefaultBudget;
   for (int k = 0; k <= StageTimer::kMax; k++) cudaEventCreate(&c->timer.ev[k]);
-  for (int j = 0; j < 4; j++) {
+  for (int j = 0; j < kPipeChunks; j++) {
     cudaStreamCreateWithFlags(&c->pipe[j], cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&c->pev[j], cudaEventDisableTiming);
   }
@@ -366,7 +368,7 @@ int dpkem_ctx_destroy(dpkem_ctx *c) {
   if (c->arena) cudaFree(c->arena);
   if (c->d_err) cudaFree(c->d_err);
   if (c->last) cudaEventDestroy(c->last);
-  for (int j = 0; j < 4; j++) {
+  for (int j = 0; j < kPipeChunks; j++) {
     if (c->pipe[j]) {
       cudaStreamSynchronize(c->pipe[j]);
       cudaStreamDestroy(c->pipe[j]);
@@ -621,6 +623,8 @@ int dpkem_set_tuning(const char *key, int value) {
     t.mixed_pair_task = std::min(value, 128);
   } else if (k == "mixed_thread_task") {
     t.mixed_thread_task = std::min(value, 256);
+  } else if (k == "pipe_chunks") {
+    t.pipe_chunks = std::min(value, kPipeChunks);
   } else {
     return set_status(DPKEM_EINVAL);
   }

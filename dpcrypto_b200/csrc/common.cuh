@@ -43,6 +43,7 @@ struct Tuning {
   int mixed_frodo_task = 256;   // instances per Frodo thread-level task in a mixed batch
   int mixed_pair_task = 128;    // instances per two-role prologue task (two threads each)
   int mixed_thread_task = 256;  // instances per other thread-level task
+  int pipe_chunks = 4;          // chunks (one stream each) of a pipelined host-mode batch, <= 8
 };
 Tuning &tuning();
 

@@ -105,7 +105,16 @@ def load() -> ctypes.CDLL:
 
 
 TUNING_PATH = os.path.join(HERE, "tuning.json")
-RUNTIME_KNOBS = ("thread_block", "mixed_frodo_task", "mixed_pair_task", "mixed_thread_task")
+RUNTIME_KNOBS = ("thread_block", "mixed_frodo_task", "mixed_pair_task", "mixed_thread_task", "pipe_chunks")
+
+
+_tuning: dict = {}
+
+
+def get_tuning() -> dict:
+    """Runtime knobs set through set_tuning / apply_tuning in this process."""
+    load()
+    return dict(_tuning)
 
 
 def apply_tuning(path: str = TUNING_PATH) -> dict:
@@ -121,6 +130,7 @@ def apply_tuning(path: str = TUNING_PATH) -> dict:
             rc = _lib.dpkem_set_tuning(k.encode(), int(chosen[k]))
             if rc != OK:
                 raise DpkemError(rc, f"tuning {k}={chosen[k]}")
+            _tuning[k] = int(chosen[k])
     return chosen
 
 
@@ -128,6 +138,7 @@ def set_tuning(key: str, value: int) -> None:
     rc = load().dpkem_set_tuning(key.encode(), int(value))
     if rc != OK:
         raise DpkemError(rc, f"set_tuning({key}, {value})")
+    _tuning[key] = int(value)
 
 
 def sizes(scheme: int) -> dict:

@@ -118,8 +118,10 @@ class Server:
         host0 = time.perf_counter()
         nxt = 0
         batches = []
+        prev, max_gap = 0.0, 0.0  # longest pause of this loop: a host stall, not device time
         while nxt < n or any(b is not None for b in busy):
             now = time.perf_counter() - host0
+            max_gap, prev = max(max_gap, now - prev), now
             for k, b in enumerate(busy):
                 if b is not None and b[0].query():
                     done_ms[b[1]:b[2]] = t_origin.elapsed_time(b[0])
@@ -145,7 +147,7 @@ class Server:
         span = (np.nanmax(done_ms) - arrivals[0] * 1e3) * 1e-3
         return {"requests": n, "ops_per_s": n / span, "p50_ms": float(np.nanpercentile(lat, 50)),
                 "p99_ms": float(np.nanpercentile(lat, 99)), "mean_batch": float(np.mean(batches)),
-                "batches": len(batches), "latency_ms": lat}
+                "batches": len(batches), "host_max_gap_ms": max_gap * 1e3, "latency_ms": lat}
 
 
 def poisson_arrivals(n: int, rate: float, seed: int = 0) -> np.ndarray:
