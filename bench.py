@@ -434,7 +434,9 @@ def main():
         threads = os.cpu_count() or 1
         n_inst = 24 * threads
         cv, dt = cpu_sample(n_inst, threads)
+        cv1, dt1 = cpu_sample(8, 1)
         line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
+                                "value_1core": cv1, "sample_1core": f"8 instances on 1 thread, {dt1:.2f} s wall",
                                 "sample": f"{n_inst} FrodoKEM-976 encaps+decaps (24 per host thread), "
                                           f"oracle C restatement, {dt:.1f} s wall",
                                 "note": "reported baseline, not the target"}
