@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdpkem.so")
-SOURCES = ["frodo.cu", "saber.cu", "coins.cu", "peak.cu", "abi.cu", "noalloc.cu", "mixed.cu"]
+SOURCES = ["frodo.cu", "saber.cu", "coins.cu", "peak.cu", "abi.cu", "noalloc.cu", "mixed.cu", "frames.cu"]
 # The persistent mixed-batch kernel reads data other CTAs wrote in the same launch: its
 # global loads bypass the (non-coherent) L1.
 EXTRA = {"mixed.cu": ["-Xptxas", "-dlcm=cg"]}
@@ -36,8 +36,9 @@ def nvcc() -> str:
 def _stale(src: str, obj: str) -> bool:
     if not os.path.exists(obj):
         return True
-    deps = [src] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".cuh")]
-    deps.append(os.path.join(HERE, "..", "include", "dpkem.h"))
+    deps = [src] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".cuh", ".h"))]
+    inc = os.path.join(HERE, "..", "include")
+    deps += [os.path.join(inc, h) for h in os.listdir(inc) if h.endswith(".h")]
     t = os.path.getmtime(obj)
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 

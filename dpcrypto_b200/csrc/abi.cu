@@ -18,6 +18,7 @@
 
 #include "../../include/dpkem.h"
 #include "common.cuh"
+#include "ctx.h"
 
 using namespace dpkem;
 
@@ -28,23 +29,8 @@ Tuning &tuning() {
 }
 }  // namespace dpkem
 
-struct dpkem_ctx {
-  int device = 0;
-  size_t budget = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t last = nullptr;
-  cudaStream_t pipe[8] = {};  // host-mode copy/compute pipeline, one stream per chunk
-  cudaEvent_t pev[8] = {};
-  uint8_t *arena = nullptr;
-  size_t arena_bytes = 0;
-  uint32_t *d_err = nullptr;
-  bool profile = false;
-  StageTimer timer;
-  int timer_stages = 0;
-  std::mutex mu;
-};
-
-namespace {
+namespace dpkem {
+namespace abi {
 
 thread_local int g_last_status = DPKEM_OK;
 
@@ -52,17 +38,6 @@ int set_status(int s) {
   g_last_status = s;
   return s;
 }
-
-constexpr size_t kAlign = 256;
-constexpr size_t kPipeChunkMin = 256;  // smallest chunk of a host-mode pipeline
-constexpr int kPipeChunks = 8;         // most chunks (and streams) of a pipelined host-mode batch
-constexpr size_t kDefaultBudget = 8ull << 30;
-
-size_t up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
-
-struct Sizes {
-  size_t pk, sk, ct, ss, kpc, encc;
-};
 
 bool scheme_sizes(int scheme, Sizes *z) {
   if (scheme == DPKEM_FRODO976) {
@@ -115,6 +90,22 @@ int ensure_arena(dpkem_ctx *c, size_t bytes) {
   return DPKEM_OK;
 }
 
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return DPKEM_OK;
+  cudaGetLastError();
+  return DPKEM_ECUDA;
+}
+
+}  // namespace abi
+}  // namespace dpkem
+
+using namespace dpkem::abi;
+
+namespace {
+
+constexpr size_t kPipeChunkMin = 256;  // smallest chunk of a host-mode pipeline
+constexpr size_t kDefaultBudget = 8ull << 30;
+
 struct Carver {
   uint8_t *base;
   size_t off = 0;
@@ -158,12 +149,6 @@ bool op_aligned(int op, const void *in0, const void *in1, const void *out0, cons
     case OP_ENC: return aligned8(in0) && aligned16(in1) && aligned16(out0) && aligned8(out1);  // coins, pk, ct, ss
     default: return aligned16(in0) && aligned8(in1) && aligned8(out0);                     // ct, sk, ss
   }
-}
-
-int cuda_status(cudaError_t e) {
-  if (e == cudaSuccess) return DPKEM_OK;
-  cudaGetLastError();
-  return DPKEM_ECUDA;
 }
 
 // Runs op on n instances.  in0/in1/out0/out1 follow the op's argument order:
@@ -639,6 +624,7 @@ const char *dpkem_strerror(int s) {
     case DPKEM_ECUDA: return "CUDA runtime error";
     case DPKEM_ETIMEOUT: return "bounded device wait expired";
     case DPKEM_EUNSUPPORTED: return "unsupported form";
+    case DPKEM_EAGAIN: return "nothing to take or no room yet";
     default: return "unknown status";
   }
 }

@@ -117,6 +117,9 @@ cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *
                        uint32_t *err, cudaStream_t st, void *plan_out);
 cudaError_t kernel_setup(int *grid);
 cudaError_t plan_launch(const void *plan, size_t n, int grid, cudaStream_t st);
+// Writes the wire-format response header before each request's first output (the request
+// header sits before its first input); resp_bytes[scheme * 3 + op] = response frame size.
+cudaError_t frame_headers_launch(const void *plan, size_t n, const uint32_t *resp_bytes, cudaStream_t st);
 int slots_for_device();
 }  // namespace mixed
 

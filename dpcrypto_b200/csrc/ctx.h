@@ -1,0 +1,46 @@
+// Host-side state of a dpkem context and the helpers shared by the C-ABI sources
+// (abi.cu: batched calls, mixed batches, graphs; frames.cu: the wire-format entry points).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+
+#include "common.cuh"
+
+struct dpkem_ctx {
+  int device = 0;
+  size_t budget = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t last = nullptr;  // recorded after every launch chain that used the arena
+  cudaStream_t pipe[8] = {};   // host-mode copy/compute pipeline, one stream per chunk
+  cudaEvent_t pev[8] = {};
+  uint8_t *arena = nullptr;
+  size_t arena_bytes = 0;
+  uint32_t *d_err = nullptr;
+  bool profile = false;
+  dpkem::StageTimer timer;
+  int timer_stages = 0;
+  std::mutex mu;
+};
+
+namespace dpkem {
+namespace abi {
+
+constexpr size_t kAlign = 256;
+constexpr int kPipeChunks = 8;  // most chunks (and streams) of a pipelined host-mode batch
+
+inline size_t up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
+
+struct Sizes {
+  size_t pk, sk, ct, ss, kpc, encc;
+};
+
+int set_status(int s);                      // records the calling thread's last status
+bool scheme_sizes(int scheme, Sizes *z);    // object sizes of a scheme; false if unknown
+int ensure_arena(dpkem_ctx *c, size_t bytes);  // grows the context's device arena
+int cuda_status(cudaError_t e);             // DPKEM_OK or DPKEM_ECUDA (clears the error)
+
+}  // namespace abi
+}  // namespace dpkem

@@ -1,0 +1,53 @@
+"""Frame server: answers request frames that another process writes into a shared ring.
+
+    python -m dpcrypto_b200.frame_server --ring /dev/shm/dpkem.ring [--create CAPACITY]
+        [--form tc|dp4a|int32] [--device 0] [--max-frames 4096] [--budget-gib 8]
+
+The ring (include/dpkem_wire.h) is page-locked once with dpkem_host_register, so each
+batch is copied between the ring and the GPU by DMA straight from and into the shared
+pages.  The loop itself is the library's dpkem_ring_serve (acquire contiguous request
+frames and response room, dpkem_frames_run, publish), called without holding the GIL.
+It returns, and the process exits 0, when a client sets the ring's stop word.
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+
+from . import frames as F
+from . import kem as K
+
+FORMS = {"tc": K.FORM_TC, "dp4a": K.FORM_DP4A, "int32": K.FORM_INT32}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--ring", required=True)
+    ap.add_argument("--create", type=int, default=None, help="create the ring with this capacity (bytes)")
+    ap.add_argument("--form", default="tc", choices=sorted(FORMS))
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--max-frames", type=int, default=4096)
+    ap.add_argument("--budget-gib", type=float, default=8.0)
+    ap.add_argument("--idle-us", type=int, default=50)
+    a = ap.parse_args(argv)
+
+    ring = F.Ring(a.ring, a.create)
+    eng = K.Engine(a.device, hbm_budget=int(a.budget_gib * (1 << 30)))
+    lib = K.load()
+    rc = lib.dpkem_host_register(ring.base, ring.size)
+    if rc != K.OK:
+        print(f"frame_server: host_register failed: {lib.dpkem_strerror(rc).decode()}", file=sys.stderr)
+        return 1
+    try:
+        rc = lib.dpkem_ring_serve(eng._h, FORMS[a.form], ring.base, a.max_frames, a.idle_us)
+    finally:
+        lib.dpkem_host_unregister(ring.base)
+        eng.close()
+    if rc != K.OK:
+        print(f"frame_server: {lib.dpkem_strerror(rc).decode()}", file=sys.stderr)
+        return 1
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -26,7 +26,7 @@ FRODO976, LIGHTSABER, SABER, FIRESABER = 0, 2, 3, 4
 SCHEMES = (FRODO976, LIGHTSABER, SABER, FIRESABER)
 FORM_DP4A, FORM_INT32, FORM_TC = 0, 1, 2
 FLAG_DEVICE_PTRS = 1
-OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, EUNSUPPORTED = 0, -1, -2, -3, -4, -5
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, EUNSUPPORTED, EAGAIN = 0, -1, -2, -3, -4, -5, -6
 
 class Request(ctypes.Structure):
     """dpkem_request: one operation of a mixed batch (device buffers, batched-call order)."""
@@ -76,6 +76,25 @@ EXPORTS = {
     "frodoKEMDecap": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "saber_enc": (None, [ctypes.c_uint8, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "saber_dec": (None, [ctypes.c_uint8, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    # wire format and shared-memory ring (include/dpkem_wire.h)
+    "dpkem_frame_bytes": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t),
+                                         ctypes.POINTER(ctypes.c_size_t)]),
+    "dpkem_frames_scan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t]
+                          + [ctypes.POINTER(ctypes.c_size_t)] * 3),
+    "dpkem_frames_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+                                        ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "dpkem_host_register": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t]),
+    "dpkem_host_unregister": (ctypes.c_int, [ctypes.c_void_p]),
+    "dpkem_ring_bytes": (ctypes.c_size_t, [ctypes.c_size_t]),
+    "dpkem_ring_init": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t]),
+    "dpkem_ring_push": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                       ctypes.POINTER(ctypes.c_size_t)]),
+    "dpkem_ring_pop": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                      ctypes.POINTER(ctypes.c_size_t)]),
+    "dpkem_ring_acquire": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t] + [ctypes.POINTER(ctypes.c_size_t)] * 7),
+    "dpkem_ring_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t]),
+    "dpkem_ring_serve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+                                        ctypes.c_int]),
 }
 
 _lib = None

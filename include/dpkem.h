@@ -7,8 +7,8 @@
  *     FrodoKEM976-GPU/include/cuda_kernel.cuh:7-9 (batch = compile-time BLOCK there,
  *     dpkem_set_compat_batch() here);
  *   - saber_enc / saber_dec replace SABER-GPU/include/cuda_kernel.cuh:6-7
- *     (mode 0 = DP / dp4a form, 1 = INT32 in the reference; here 1 is unsupported and
- *     2 selects the int8 tensor-core form).
+ *     (mode 0 = DP / dp4a form, 1 = INT32 schoolbook, as in the reference; 2 selects the
+ *     int8 tensor-core form).
  *   - dpkem_{keypair,enc,dec}_batch are the batched form of the PQClean-style API the
  *     reference's headers declare (FrodoKEM976-GPU/include/api.h:14-18), with explicit
  *     coins so every call is reproducible.
@@ -39,7 +39,8 @@ enum {
   DPKEM_ENOMEM = -2,       /* allocation failed or the request exceeds the HBM budget */
   DPKEM_ECUDA = -3,        /* a CUDA runtime call failed */
   DPKEM_ETIMEOUT = -4,     /* a bounded device wait expired (the kernel unwound) */
-  DPKEM_EUNSUPPORTED = -5  /* valid request this build does not implement */
+  DPKEM_EUNSUPPORTED = -5, /* valid request this build does not implement */
+  DPKEM_EAGAIN = -6        /* non-blocking ring call: nothing to take / no room yet (dpkem_wire.h) */
 };
 
 /* Schemes: the value of a Saber scheme is its module rank l. */

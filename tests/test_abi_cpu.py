@@ -10,7 +10,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _declared():
-    text = open(os.path.join(ROOT, "include", "dpkem.h")).read()
+    inc = os.path.join(ROOT, "include")
+    text = "".join(open(os.path.join(inc, f)).read() for f in sorted(os.listdir(inc)) if f.endswith(".h"))
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     names = set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*([A-Za-z_][A-Za-z_0-9]*)\s*\(", text, flags=re.M))
     return {n for n in names if n not in ("if", "defined")}
