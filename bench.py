@@ -108,6 +108,66 @@ def run_reference(args, world, rank):
 
 
 # ---------------------------------------------------------------- GPU helpers
+def bench_frames(eng, form, n: int = 16384, reps: int = 3) -> dict:
+    """dpkem_frames_run on n mixed request frames (pinned host block in, pinned block out,
+    copies inside the timing), and the same block served through the ring by the frame
+    server process (client push -> last response popped)."""
+    import tempfile
+
+    import numpy as np
+    import torch
+
+    import dpcrypto_b200 as d
+    from dpcrypto_b200 import frames as F
+    from dpcrypto_b200.workloads import mixed_frames
+
+    blk = mixed_frames(eng, n, seed=0)
+    _, _, rb = F.scan(blk)
+    req = torch.from_numpy(blk).pin_memory().numpy()
+    resp = torch.empty(rb, dtype=torch.uint8).pin_memory().numpy()
+    F.run(eng, req, form, out=resp)
+    t = time.perf_counter()
+    for _ in range(reps):
+        F.run(eng, req, form, out=resp)
+    dt = (time.perf_counter() - t) / reps
+    out = {"requests": n, "unit": "KEM ops/s", "mix": "4 schemes x 3 ops, uniform, shuffled",
+           "frames_run": {"ops_per_s": n / dt, "ms_per_block": dt * 1e3, "request_bytes": int(blk.nbytes),
+                          "response_bytes": int(rb)}}
+    # through the ring, served by another process
+    shm = "/dev/shm" if os.path.isdir("/dev/shm") else tempfile.gettempdir()
+    path = os.path.join(shm, f"dpkem-bench-{os.getpid()}.ring")
+    cap = 128 << 20
+    ring = F.Ring(path, capacity=cap)
+    fname = {d.FORM_TC: "tc", d.FORM_DP4A: "dp4a", d.FORM_INT32: "int32"}[form]
+    proc = subprocess.Popen([sys.executable, "-m", "dpcrypto_b200.frame_server", "--ring", path, "--form", fname,
+                             "--max-frames", "4096", "--idle-us", "20", "--inflight", "2"], cwd=os.path.dirname(os.path.abspath(__file__)))
+    try:
+        popbuf = np.empty(rb, np.uint8)
+        for rep in range(2):  # the first pass warms the server up
+            n_got, n_bytes, pending = 0, 0, req
+            t = time.perf_counter()
+            deadline = t + 300
+            while n_got < n:
+                if time.perf_counter() > deadline or proc.poll() is not None:
+                    raise RuntimeError("frame server stalled or exited")
+                if len(pending):
+                    pending = pending[ring.push(pending):]
+                r, count = ring.pop(out=popbuf[n_bytes:])
+                n_bytes += len(r)
+                n_got += count
+            dt = time.perf_counter() - t
+        same = bool(n_bytes == rb and np.array_equal(popbuf, resp))
+        out["ring_external_process"] = {"ops_per_s": n / dt, "ms_per_block": dt * 1e3, "ring_capacity": cap,
+                                        "max_frames_per_batch": 4096, "batches_in_flight": 2,
+                                        "bit_exact_vs_frames_run": same}
+    finally:
+        ring.stop()
+        proc.wait(timeout=60)
+        ring.close()
+        os.unlink(path)
+    return out
+
+
 def pcie_gbs(h2d: bool, nbytes: int = 256 << 20) -> float:
     """Pinned host<->device copy bandwidth (GB/s) of one 256 MiB buffer, CUDA-event timed."""
     import torch
@@ -403,6 +463,11 @@ def main():
             finally:
                 srv.close()
         line["serving"] = serving
+
+    # ---- wire format: 16384 mixed request frames from pinned host memory, then the same
+    #      frames through the shared-memory ring with the frame server in its own process ----
+    if not args.no_secondary and world == 1:
+        line["frames_16384"] = bench_frames(eng, form)
 
     # ---- end to end through the public API with pinned host buffers ----
     if not args.no_e2e:

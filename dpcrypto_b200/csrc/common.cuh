@@ -118,8 +118,10 @@ cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *
 cudaError_t kernel_setup(int *grid);
 cudaError_t plan_launch(const void *plan, size_t n, int grid, cudaStream_t st);
 // Writes the wire-format response header before each request's first output (the request
-// header sits before its first input); resp_bytes[scheme * 3 + op] = response frame size.
-cudaError_t frame_headers_launch(const void *plan, size_t n, const uint32_t *resp_bytes, cudaStream_t st);
+// header sits before its first input) and zeroes the frame's tail padding;
+// resp_bytes / payload_end [scheme * 3 + op] = response frame size / end of its payload.
+cudaError_t frame_headers_launch(const void *plan, size_t n, const uint32_t *resp_bytes, const uint32_t *payload_end,
+                                 cudaStream_t st);
 int slots_for_device();
 }  // namespace mixed
 

@@ -11,6 +11,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <deque>
+#include <utility>
 #include <vector>
 
 #include "../../include/dpkem.h"
@@ -33,6 +35,7 @@ size_t pad32(size_t x) { return (x + 31) & ~(size_t)31; }
 struct Layout {
   size_t req, resp;
   size_t in0, in1, out0, out1;
+  size_t resp_end;  // end of the last response section (zero padding follows)
 };
 
 bool layout_of(int scheme, int op, Layout *L) {
@@ -40,14 +43,14 @@ bool layout_of(int scheme, int op, Layout *L) {
   if (!scheme_sizes(scheme, &z)) return false;
   switch (op) {
     case DPKEM_OP_KEYPAIR:
-      *L = {pad32(kHdr + pad16(z.kpc)), pad32(kHdr + z.pk + z.sk), kHdr, 0, kHdr, kHdr + z.pk};
+      *L = {pad32(kHdr + pad16(z.kpc)), pad32(kHdr + z.pk + z.sk), kHdr, 0, kHdr, kHdr + z.pk, kHdr + z.pk + z.sk};
       return true;
     case DPKEM_OP_ENC:
       *L = {pad32(kHdr + pad16(z.encc) + z.pk), pad32(kHdr + z.ct + pad16(z.ss)), kHdr, kHdr + pad16(z.encc), kHdr,
-            kHdr + z.ct};
+            kHdr + z.ct, kHdr + z.ct + z.ss};
       return true;
     case DPKEM_OP_DEC:
-      *L = {pad32(kHdr + z.ct + z.sk), pad32(kHdr + pad16(z.ss)), kHdr, kHdr + z.ct, kHdr, 0};
+      *L = {pad32(kHdr + z.ct + z.sk), pad32(kHdr + pad16(z.ss)), kHdr, kHdr + z.ct, kHdr, 0, kHdr + z.ss};
       return true;
     default:
       return false;
@@ -89,12 +92,14 @@ int scan(const uint8_t *req, size_t bytes, size_t max_frames, std::vector<Frame>
   return DPKEM_OK;
 }
 
-// Response frame sizes indexed by scheme * 3 + op (0 for unknown schemes).
-void resp_table(uint32_t out[15]) {
+// Response frame sizes and payload ends indexed by scheme * 3 + op (0 for unknown schemes).
+void resp_table(uint32_t bytes[15], uint32_t end[15]) {
   for (int s = 0; s < 5; s++)
     for (int op = 0; op < 3; op++) {
       Layout L;
-      out[s * 3 + op] = layout_of(s, op, &L) ? (uint32_t)L.resp : 0u;
+      const bool ok = layout_of(s, op, &L);
+      bytes[s * 3 + op] = ok ? (uint32_t)L.resp : 0u;
+      end[s * 3 + op] = ok ? (uint32_t)L.resp_end : 0u;
     }
 }
 
@@ -153,6 +158,175 @@ void write_pad(uint8_t *at, size_t bytes) {
   std::memcpy(at, &h, sizeof(h));
 }
 
+// Enqueues a frame block on the context's streams (see dpkem_frames_run); frames_finish
+// waits for it.  *resp_bytes is set on success.
+int frames_submit(dpkem_ctx *c, int form, const uint8_t *req, size_t req_bytes, uint8_t *resp, size_t resp_cap,
+                  size_t *resp_bytes) {
+  if (!c || !resp_bytes || (!req && req_bytes)) return DPKEM_EINVAL;
+  if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC && form != DPKEM_FORM_INT32) return DPKEM_EINVAL;
+  *resp_bytes = 0;
+  std::vector<Frame> fr;
+  ScanResult sr;
+  int rc = scan(req, req_bytes, 0, &fr, &sr);
+  if (rc) return rc;
+  if (sr.resp_bytes > resp_cap || (!resp && sr.resp_bytes)) return DPKEM_EINVAL;
+  if (fr.empty()) return DPKEM_OK;
+
+  std::lock_guard<std::mutex> lock(c->mu);
+  if (cudaSetDevice(c->device) != cudaSuccess) return cuda_status(cudaErrorInvalidDevice);
+  // Chunks: up to pipe_chunks of at least kGroupMin frames, all in flight on their own
+  // streams; halved until the chunks in flight fit the context's budget.
+  const size_t n = fr.size();
+  int npipe = (int)std::min<size_t>(std::min(std::max(tuning().pipe_chunks, 1), kPipeChunks),
+                                    std::max<size_t>(1, n / kGroupMin));
+  size_t per = (n + npipe - 1) / npipe;
+  std::vector<Group> gs;
+  size_t region = 0;
+  while (true) {
+    gs = make_groups(fr, per);
+    region = 0;
+    for (const Group &g : gs) region = std::max(region, g.need);
+    npipe = (int)std::min<size_t>(npipe, gs.size());
+    if (region * npipe <= c->budget) break;
+    if (npipe > 1) {
+      npipe--;
+      continue;
+    }
+    if (per == 1) return DPKEM_ENOMEM;
+    per = (per + 1) / 2;
+  }
+  if ((rc = ensure_arena(c, region * npipe)) != DPKEM_OK) return rc;
+
+  cudaStream_t st = c->stream;
+  cudaError_t e = cudaStreamWaitEvent(st, c->last, 0);
+  if (e == cudaSuccess) e = cudaEventRecord(c->pev[0], st);
+  for (int j = 0; j < npipe && e == cudaSuccess; j++) e = cudaStreamWaitEvent(c->pipe[j], c->pev[0], 0);
+  int grid = 0;
+  if (e == cudaSuccess) e = mixed::kernel_setup(&grid);
+  uint32_t rtab[15], rend[15];
+  resp_table(rtab, rend);
+  std::vector<std::vector<uint8_t>> plans(gs.size(), std::vector<uint8_t>(mixed::plan_struct_bytes()));
+  for (size_t k = 0; k < gs.size() && e == cudaSuccess; k++) {
+    const Group &g = gs[k];
+    cudaStream_t sj = c->pipe[k % npipe];
+    uint8_t *d_req = c->arena + (k % npipe) * region;
+    uint8_t *d_resp = d_req + up(g.req_len);
+    uint8_t *d_plan = d_resp + up(g.resp_len);
+    const std::vector<mixed::Req> rq = group_reqs(fr, g, d_req, d_resp);
+    e = cudaMemcpyAsync(d_req, req + g.req_start, g.req_len, cudaMemcpyHostToDevice, sj);
+    if (e == cudaSuccess)
+      e = mixed::plan_build(rq.data(), rq.size(), form, grid, d_plan, region - (size_t)(d_plan - d_req), c->d_err, sj,
+                            plans[k].data());
+    if (e == cudaSuccess) e = mixed::plan_launch(plans[k].data(), rq.size(), grid, sj);
+    if (e == cudaSuccess) e = mixed::frame_headers_launch(plans[k].data(), rq.size(), rtab, rend, sj);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(resp + g.resp_start, d_resp, g.resp_len, cudaMemcpyDeviceToHost, sj);
+  }
+  for (int j = 0; j < npipe && e == cudaSuccess; j++) {
+    e = cudaEventRecord(c->pev[j], c->pipe[j]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, c->pev[j], 0);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(c->last, st);
+  if (e != cudaSuccess) return cuda_status(e);
+  *resp_bytes = sr.resp_bytes;
+  return DPKEM_OK;
+}
+
+// Waits for the context's last submitted block; reports (and clears) a device timeout.
+int frames_finish(dpkem_ctx *c) {
+  std::lock_guard<std::mutex> lock(c->mu);
+  cudaSetDevice(c->device);
+  uint32_t err = 0;
+  cudaError_t e = cudaEventSynchronize(c->last);
+  if (e == cudaSuccess) e = cudaMemcpy(&err, c->d_err, 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (err) {
+    cudaMemset(c->d_err, 0, 4);
+    return DPKEM_ETIMEOUT;
+  }
+  return DPKEM_OK;
+}
+
+bool frames_done(dpkem_ctx *c) { return cudaEventQuery(c->last) != cudaErrorNotReady; }
+
+// Server-side position in a ring: where the next batch starts, plus PAD bytes passed over
+// that no published batch has accounted for yet.
+struct Cursor {
+  uint64_t req, resp;
+  uint64_t req_pending, resp_pending;
+};
+
+struct RingBatch {
+  size_t req_off, req_bytes, req_advance, resp_off, resp_bytes, resp_advance, n;
+};
+
+void publish(dpkem_ring_control *c, uint64_t req_advance, uint64_t resp_advance, uint64_t n) {
+  st_rel(&c->resp_tail, c->resp_tail + resp_advance);  // responses first, then free the requests
+  st_rel(&c->req_head, c->req_head + req_advance);
+  if (n) st_rel(&c->served, c->served + n);
+}
+
+// Takes up to max_frames contiguous request frames at cur->req and reserves response room
+// at cur->resp; advances the cursor.  EAGAIN with nothing taken may still have moved the
+// cursor over PAD frames (recorded in the pending counts).
+int acquire_at(void *base, size_t max_frames, Cursor *cur, RingBatch *out) {
+  dpkem_ring_control *c = ring_ctl(base);
+  const uint64_t cap = c->capacity, tail = ld_acq(&c->req_tail);
+  const uint8_t *ring = ring_req(base);
+  while (cur->req < tail) {  // skip PAD frames
+    dpkem_frame_header h;
+    std::memcpy(&h, ring + cur->req % cap, sizeof(h));
+    if (h.magic != DPKEM_FRAME_PAD) break;
+    if (h.frame_bytes < kHdr || h.frame_bytes % DPKEM_FRAME_ALIGN) return DPKEM_EINVAL;
+    cur->req += h.frame_bytes;
+    cur->req_pending += h.frame_bytes;
+  }
+  if (cur->req == tail) return DPKEM_EAGAIN;
+  const uint64_t pos = cur->req % cap, avail = std::min<uint64_t>(tail - cur->req, cap - pos);
+  // response room: contiguous at the cursor, or from 0 after a PAD to the end
+  const uint64_t rfree = cap - (cur->resp - ld_acq(&c->resp_head)), rpos = cur->resp % cap;
+  size_t k = 0, used = 0, rneed = 0;
+  bool wrap = false;
+  while (used < avail && (max_frames == 0 || k < max_frames)) {
+    dpkem_frame_header h;
+    std::memcpy(&h, ring + pos + used, sizeof(h));
+    if (h.magic == DPKEM_FRAME_PAD) break;  // a PAD ends the contiguous run
+    Layout L;
+    if (h.magic != DPKEM_FRAME_MAGIC || h.version != DPKEM_FRAME_VERSION || !layout_of(h.scheme, h.op, &L) ||
+        h.frame_bytes != L.req || L.req > avail - used)
+      return DPKEM_EINVAL;
+    if (L.resp > cap) return DPKEM_EINVAL;  // a response that can never fit
+    const uint64_t r = rneed + L.resp;
+    const bool fits_here = rpos + r <= cap && r <= rfree;
+    const bool fits_wrapped = rpos != 0 && (cap - rpos) + r <= rfree;
+    if (!fits_here && !fits_wrapped) break;
+    wrap = !fits_here;
+    rneed = r;
+    used += L.req;
+    k++;
+  }
+  if (k == 0) {
+    // The first response fits neither before the end nor after a PAD: close the end with
+    // a PAD now (if it fits), so the response starts at 0 once the client has caught up.
+    if (rpos != 0 && cap - rpos <= rfree) {
+      write_pad(ring_resp(base, cap) + rpos, cap - rpos);
+      cur->resp += cap - rpos;
+      cur->resp_pending += cap - rpos;
+    }
+    return DPKEM_EAGAIN;
+  }
+  uint64_t rpad = 0;
+  if (wrap) {
+    write_pad(ring_resp(base, cap) + rpos, cap - rpos);
+    rpad = cap - rpos;
+  }
+  *out = RingBatch{pos, used, (size_t)(cur->req_pending + used), wrap ? 0 : rpos, rneed,
+                   (size_t)(cur->resp_pending + rpad + rneed), k};
+  cur->req += used;
+  cur->resp += rpad + rneed;
+  cur->req_pending = cur->resp_pending = 0;
+  return DPKEM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -179,81 +353,11 @@ int dpkem_frames_scan(const uint8_t *req, size_t req_bytes, size_t max_frames, s
 
 int dpkem_frames_run(dpkem_ctx *c, int form, const uint8_t *req, size_t req_bytes, uint8_t *resp, size_t resp_cap,
                      size_t *resp_bytes) {
-  if (!c || !resp_bytes || (!req && req_bytes)) return set_status(DPKEM_EINVAL);
-  if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC && form != DPKEM_FORM_INT32) return set_status(DPKEM_EINVAL);
-  *resp_bytes = 0;
-  std::vector<Frame> fr;
-  ScanResult sr;
-  int rc = scan(req, req_bytes, 0, &fr, &sr);
+  int rc = frames_submit(c, form, req, req_bytes, resp, resp_cap, resp_bytes);
   if (rc) return set_status(rc);
-  if (sr.resp_bytes > resp_cap || (!resp && sr.resp_bytes)) return set_status(DPKEM_EINVAL);
-  if (fr.empty()) return set_status(DPKEM_OK);
-
-  std::lock_guard<std::mutex> lock(c->mu);
-  if (cudaSetDevice(c->device) != cudaSuccess) return set_status(cuda_status(cudaErrorInvalidDevice));
-  // Chunks: up to pipe_chunks of at least kGroupMin frames, all in flight on their own
-  // streams; halved until the chunks in flight fit the context's budget.
-  const size_t n = fr.size();
-  int npipe = (int)std::min<size_t>(std::min(std::max(tuning().pipe_chunks, 1), kPipeChunks),
-                                    std::max<size_t>(1, n / kGroupMin));
-  size_t per = (n + npipe - 1) / npipe;
-  std::vector<Group> gs;
-  size_t region = 0;
-  while (true) {
-    gs = make_groups(fr, per);
-    region = 0;
-    for (const Group &g : gs) region = std::max(region, g.need);
-    npipe = (int)std::min<size_t>(npipe, gs.size());
-    if (region * npipe <= c->budget) break;
-    if (npipe > 1) {
-      npipe--;
-      continue;
-    }
-    if (per == 1) return set_status(DPKEM_ENOMEM);
-    per = (per + 1) / 2;
-  }
-  if ((rc = ensure_arena(c, region * npipe)) != DPKEM_OK) return set_status(rc);
-
-  cudaStream_t st = c->stream;
-  cudaError_t e = cudaStreamWaitEvent(st, c->last, 0);
-  if (e == cudaSuccess) e = cudaEventRecord(c->pev[0], st);
-  for (int j = 0; j < npipe && e == cudaSuccess; j++) e = cudaStreamWaitEvent(c->pipe[j], c->pev[0], 0);
-  int grid = 0;
-  if (e == cudaSuccess) e = mixed::kernel_setup(&grid);
-  uint32_t rtab[15];
-  resp_table(rtab);
-  std::vector<std::vector<uint8_t>> plans(gs.size(), std::vector<uint8_t>(mixed::plan_struct_bytes()));
-  for (size_t k = 0; k < gs.size() && e == cudaSuccess; k++) {
-    const Group &g = gs[k];
-    cudaStream_t sj = c->pipe[k % npipe];
-    uint8_t *d_req = c->arena + (k % npipe) * region;
-    uint8_t *d_resp = d_req + up(g.req_len);
-    uint8_t *d_plan = d_resp + up(g.resp_len);
-    const std::vector<mixed::Req> rq = group_reqs(fr, g, d_req, d_resp);
-    e = cudaMemcpyAsync(d_req, req + g.req_start, g.req_len, cudaMemcpyHostToDevice, sj);
-    if (e == cudaSuccess)
-      e = mixed::plan_build(rq.data(), rq.size(), form, grid, d_plan, region - (size_t)(d_plan - d_req), c->d_err, sj,
-                            plans[k].data());
-    if (e == cudaSuccess) e = mixed::plan_launch(plans[k].data(), rq.size(), grid, sj);
-    if (e == cudaSuccess) e = mixed::frame_headers_launch(plans[k].data(), rq.size(), rtab, sj);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(resp + g.resp_start, d_resp, g.resp_len, cudaMemcpyDeviceToHost, sj);
-  }
-  for (int j = 0; j < npipe && e == cudaSuccess; j++) {
-    e = cudaEventRecord(c->pev[j], c->pipe[j]);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, c->pev[j], 0);
-  }
-  if (e == cudaSuccess) e = cudaEventRecord(c->last, st);
-  uint32_t err = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&err, c->d_err, 4, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return set_status(cuda_status(e));
-  if (err) {
-    cudaMemsetAsync(c->d_err, 0, 4, st);
-    cudaStreamSynchronize(st);
-    return set_status(DPKEM_ETIMEOUT);
-  }
-  *resp_bytes = sr.resp_bytes;
-  return set_status(DPKEM_OK);
+  rc = frames_finish(c);
+  if (rc) *resp_bytes = 0;
+  return set_status(rc);
 }
 
 int dpkem_host_register(void *ptr, size_t bytes) {
@@ -315,14 +419,15 @@ int dpkem_ring_push(void *base, const uint8_t *frames, size_t bytes, size_t *pus
   return set_status(taken ? DPKEM_OK : DPKEM_EAGAIN);
 }
 
-int dpkem_ring_pop(void *base, uint8_t *out, size_t cap_out, size_t *got) {
+int dpkem_ring_pop(void *base, uint8_t *out, size_t cap_out, size_t *got, size_t *n_frames) {
   dpkem_ring_control *c = ring_ctl(base);
   if (!c || !got || (!out && cap_out)) return set_status(DPKEM_EINVAL);
   *got = 0;
+  if (n_frames) *n_frames = 0;
   const uint64_t cap = c->capacity, tail = ld_acq(&c->resp_tail);
   uint64_t head = c->resp_head;
   const uint8_t *ring = ring_resp(base, cap);
-  size_t copied = 0;
+  size_t copied = 0, count = 0;
   while (head < tail) {
     dpkem_frame_header h;
     std::memcpy(&h, ring + head % cap, sizeof(h));
@@ -333,11 +438,13 @@ int dpkem_ring_pop(void *base, uint8_t *out, size_t cap_out, size_t *got) {
       if (copied + h.frame_bytes > cap_out) break;
       std::memcpy(out + copied, ring + head % cap, h.frame_bytes);
       copied += h.frame_bytes;
+      count++;
     }
     head += h.frame_bytes;
   }
   st_rel(&c->resp_head, head);
   *got = copied;
+  if (n_frames) *n_frames = count;
   return set_status(DPKEM_OK);
 }
 
@@ -346,93 +453,72 @@ int dpkem_ring_acquire(void *base, size_t max_frames, size_t *req_off, size_t *r
   dpkem_ring_control *c = ring_ctl(base);
   if (!c || !req_off || !req_bytes || !req_advance || !resp_off || !resp_bytes || !resp_advance || !n_frames)
     return set_status(DPKEM_EINVAL);
-  const uint64_t cap = c->capacity, tail = ld_acq(&c->req_tail);
-  uint64_t head = c->req_head, pads = 0;
-  const uint8_t *ring = ring_req(base);
-  // skip PAD frames at the head
-  while (head < tail) {
-    dpkem_frame_header h;
-    std::memcpy(&h, ring + head % cap, sizeof(h));
-    if (h.magic != DPKEM_FRAME_PAD) break;
-    if (h.frame_bytes < kHdr || h.frame_bytes % DPKEM_FRAME_ALIGN) return set_status(DPKEM_EINVAL);
-    head += h.frame_bytes;
-    pads += h.frame_bytes;
-  }
-  if (head == tail) {
-    if (pads) st_rel(&c->req_head, head);
-    return set_status(DPKEM_EAGAIN);
-  }
-  const uint64_t pos = head % cap, avail = std::min<uint64_t>(tail - head, cap - pos);
-  // response room: contiguous from the response tail, or from 0 after a PAD to the end
-  const uint64_t rtail = c->resp_tail, rfree = cap - (rtail - ld_acq(&c->resp_head)), rpos = rtail % cap;
-  size_t k = 0, used = 0, rneed = 0;
-  bool wrap = false;
-  while (used < avail && (max_frames == 0 || k < max_frames)) {
-    dpkem_frame_header h;
-    std::memcpy(&h, ring + pos + used, sizeof(h));
-    if (h.magic == DPKEM_FRAME_PAD) break;  // a PAD ends the contiguous run
-    Layout L;
-    if (h.magic != DPKEM_FRAME_MAGIC || h.version != DPKEM_FRAME_VERSION || !layout_of(h.scheme, h.op, &L) ||
-        h.frame_bytes != L.req || L.req > avail - used)
-      return set_status(DPKEM_EINVAL);
-    if (L.resp > cap) return set_status(DPKEM_EINVAL);  // a response that can never fit
-    const uint64_t r = rneed + L.resp;
-    const bool fits_here = rpos + r <= cap && r <= rfree;
-    const bool fits_wrapped = (cap - rpos) + r <= rfree && r <= cap;
-    if (!fits_here && !fits_wrapped) break;
-    wrap = !fits_here;
-    rneed = r;
-    used += L.req;
-    k++;
-  }
-  if (k == 0) {
-    if (pads) st_rel(&c->req_head, head);
-    // The first response fits neither before the end nor after a PAD: close the end with
-    // a PAD now (if it fits), so the response starts at 0 once the client has skipped it.
-    if (rpos != 0 && cap - rpos <= rfree) {
-      write_pad(ring_resp(base, cap) + rpos, cap - rpos);
-      st_rel(&c->resp_tail, rtail + (cap - rpos));
-    }
-    return set_status(DPKEM_EAGAIN);
-  }
-  if (wrap) write_pad(ring_resp(base, cap) + rpos, cap - rpos);
-  *req_off = pos;
-  *req_bytes = used;
-  *req_advance = pads + used;
-  *resp_off = wrap ? 0 : rpos;
-  *resp_bytes = rneed;
-  *resp_advance = (wrap ? cap - rpos : 0) + rneed;
-  *n_frames = k;
+  Cursor cur{c->req_head, c->resp_tail, 0, 0};
+  RingBatch b;
+  const int rc = acquire_at(base, max_frames, &cur, &b);
+  if (rc == DPKEM_EAGAIN && (cur.req_pending || cur.resp_pending)) publish(c, cur.req_pending, cur.resp_pending, 0);
+  if (rc) return set_status(rc);
+  *req_off = b.req_off;
+  *req_bytes = b.req_bytes;
+  *req_advance = b.req_advance;
+  *resp_off = b.resp_off;
+  *resp_bytes = b.resp_bytes;
+  *resp_advance = b.resp_advance;
+  *n_frames = b.n;
   return set_status(DPKEM_OK);
 }
 
 int dpkem_ring_release(void *base, size_t req_advance, size_t resp_advance, size_t n_frames) {
   dpkem_ring_control *c = ring_ctl(base);
   if (!c) return set_status(DPKEM_EINVAL);
-  st_rel(&c->resp_tail, c->resp_tail + resp_advance);  // responses first, then free the requests
-  st_rel(&c->req_head, c->req_head + req_advance);
-  st_rel(&c->served, c->served + n_frames);
+  publish(c, req_advance, resp_advance, n_frames);
   return set_status(DPKEM_OK);
 }
 
-int dpkem_ring_serve(dpkem_ctx *ctx, int form, void *base, size_t max_frames, int idle_us) {
+int dpkem_ring_serve(dpkem_ctx *const *ctxs, int nctx, int form, void *base, size_t max_frames, int idle_us) {
   dpkem_ring_control *c = ring_ctl(base);
-  if (!ctx || !c) return set_status(DPKEM_EINVAL);
+  if (!ctxs || nctx < 1 || nctx > 16 || !c) return set_status(DPKEM_EINVAL);
+  for (int k = 0; k < nctx; k++)
+    if (!ctxs[k]) return set_status(DPKEM_EINVAL);
   const size_t cap = c->capacity;
-  while (!ld_acq(&c->stop)) {
-    size_t ro, rb, ra, so, sb, sa, n;
-    int rc = dpkem_ring_acquire(base, max_frames, &ro, &rb, &ra, &so, &sb, &sa, &n);
-    if (rc == DPKEM_EAGAIN) {
-      if (idle_us > 0) usleep((useconds_t)idle_us);
+  // Batches are acquired at the server's own cursors (ahead of the published counters),
+  // run on the contexts in turn, and published strictly in acquisition order.
+  Cursor cur{c->req_head, c->resp_tail, 0, 0};
+  std::deque<std::pair<RingBatch, int>> inflight;
+  int next = 0, rc = DPKEM_OK;
+  while (true) {
+    const bool stop = ld_acq(&c->stop) != 0;
+    if (stop && inflight.empty()) break;
+    if (!stop && (int)inflight.size() < nctx) {
+      RingBatch b;
+      rc = acquire_at(base, max_frames, &cur, &b);
+      if (rc == DPKEM_OK) {
+        size_t wrote = 0;
+        rc = frames_submit(ctxs[next], form, ring_req(base) + b.req_off, b.req_bytes, ring_resp(base, cap) + b.resp_off,
+                           b.resp_bytes, &wrote);
+        if (rc) break;
+        inflight.emplace_back(b, next);
+        next = (next + 1) % nctx;
+        continue;
+      }
+      if (rc != DPKEM_EAGAIN) break;
+      rc = DPKEM_OK;
+    }
+    if (!inflight.empty()) {  // nothing new to start: retire the oldest batch
+      const auto [b, k] = inflight.front();
+      inflight.pop_front();
+      if ((rc = frames_finish(ctxs[k])) != DPKEM_OK) break;
+      publish(c, b.req_advance, b.resp_advance, b.n);
       continue;
     }
-    if (rc) return set_status(rc);
-    size_t wrote = 0;
-    rc = dpkem_frames_run(ctx, form, ring_req(base) + ro, rb, ring_resp(base, cap) + so, sb, &wrote);
-    if (rc) return set_status(rc);
-    dpkem_ring_release(base, ra, sa, n);
+    if (cur.req_pending || cur.resp_pending) {  // PADs passed while idle
+      publish(c, cur.req_pending, cur.resp_pending, 0);
+      cur.req_pending = cur.resp_pending = 0;
+    }
+    if (idle_us > 0) usleep((useconds_t)idle_us);
   }
-  return set_status(DPKEM_OK);
+  for (auto &f : inflight) frames_finish(ctxs[f.second]);  // error path: let the copies land
+  return set_status(rc);
 }
 
 }  // extern "C"

@@ -502,10 +502,12 @@ cudaError_t plan_launch(const void *plan, size_t n, int grid, cudaStream_t st) {
 
 // Response headers of a frame batch (the wire format of dpkem_wire.h): every request's
 // header sits 32 bytes before its first input, its response header 32 bytes before its
-// first output.  One thread per request copies version, scheme, op and id, and writes the
-// magic, status OK and the response frame size from resp_bytes[scheme * 3 + op].
+// first output.  One thread per request copies version, scheme, op and id, writes the
+// magic, status OK and the response frame size from resp_bytes[scheme * 3 + op], and
+// zeroes the frame's tail padding from payload_end[scheme * 3 + op] on.
 struct FrameSizes {
   uint32_t resp_bytes[15];
+  uint32_t payload_end[15];
 };
 
 __global__ void __launch_bounds__(256) frame_headers_kernel(const DevReq *req, uint32_t n, FrameSizes fs) {
@@ -516,14 +518,21 @@ __global__ void __launch_bounds__(256) frame_headers_kernel(const DevReq *req, u
   const uint2 w0 = rq[0], w1 = rq[1];
   uint4 *rs = reinterpret_cast<uint4 *>(r.out0 - 32);
   // bytes 0-3 magic, 4 version, 5 scheme, 6 op, 7 status (0), 8-15 id, 16-19 frame_bytes
+  const int k = r.scheme * 3 + r.op;
   rs[0] = make_uint4(0x464B5044u, w0.y & 0x00FFFFFFu, w1.x, w1.y);
-  rs[1] = make_uint4(fs.resp_bytes[r.scheme * 3 + r.op], 0u, 0u, 0u);
+  rs[1] = make_uint4(fs.resp_bytes[k], 0u, 0u, 0u);
+  uint8_t *frame = r.out0 - 32;
+  for (uint32_t b = fs.payload_end[k]; b < fs.resp_bytes[k]; b++) frame[b] = 0;
 }
 
-cudaError_t frame_headers_launch(const void *plan, size_t n, const uint32_t *resp_bytes, cudaStream_t st) {
+cudaError_t frame_headers_launch(const void *plan, size_t n, const uint32_t *resp_bytes, const uint32_t *payload_end,
+                                 cudaStream_t st) {
   const Plan &p = *static_cast<const Plan *>(plan);
   FrameSizes fs{};
-  for (int k = 0; k < 15; k++) fs.resp_bytes[k] = resp_bytes[k];
+  for (int k = 0; k < 15; k++) {
+    fs.resp_bytes[k] = resp_bytes[k];
+    fs.payload_end[k] = payload_end[k];
+  }
   frame_headers_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p.req, (uint32_t)n, fs);
   return cudaGetLastError();
 }

@@ -5,13 +5,16 @@
 
 The ring (include/dpkem_wire.h) is page-locked once with dpkem_host_register, so each
 batch is copied between the ring and the GPU by DMA straight from and into the shared
-pages.  The loop itself is the library's dpkem_ring_serve (acquire contiguous request
-frames and response room, dpkem_frames_run, publish), called without holding the GIL.
+pages.  The loop itself is the library's dpkem_ring_serve, called without holding the
+GIL: it takes contiguous request frames and response room at its own cursors, runs up to
+--inflight batches at once (one dpkem context each, so one batch's copies overlap
+another's kernels) and publishes the responses in request order.
 It returns, and the process exits 0, when a client sets the ring's stop word.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import sys
 
 from . import frames as F
@@ -29,20 +32,23 @@ def main(argv=None) -> int:
     ap.add_argument("--max-frames", type=int, default=4096)
     ap.add_argument("--budget-gib", type=float, default=8.0)
     ap.add_argument("--idle-us", type=int, default=50)
+    ap.add_argument("--inflight", type=int, default=2, help="batches in flight (one context each)")
     a = ap.parse_args(argv)
 
     ring = F.Ring(a.ring, a.create)
-    eng = K.Engine(a.device, hbm_budget=int(a.budget_gib * (1 << 30)))
+    engines = [K.Engine(a.device, hbm_budget=int(a.budget_gib * (1 << 30) / a.inflight)) for _ in range(a.inflight)]
+    handles = (ctypes.c_void_p * len(engines))(*[e._h for e in engines])
     lib = K.load()
     rc = lib.dpkem_host_register(ring.base, ring.size)
     if rc != K.OK:
         print(f"frame_server: host_register failed: {lib.dpkem_strerror(rc).decode()}", file=sys.stderr)
         return 1
     try:
-        rc = lib.dpkem_ring_serve(eng._h, FORMS[a.form], ring.base, a.max_frames, a.idle_us)
+        rc = lib.dpkem_ring_serve(handles, len(engines), FORMS[a.form], ring.base, a.max_frames, a.idle_us)
     finally:
         lib.dpkem_host_unregister(ring.base)
-        eng.close()
+        for e in engines:
+            e.close()
     if rc != K.OK:
         print(f"frame_server: {lib.dpkem_strerror(rc).decode()}", file=sys.stderr)
         return 1

@@ -178,14 +178,15 @@ class Ring:
             raise K.DpkemError(rc, "ring_push")
         return got.value
 
-    def pop(self, cap: int = 64 << 20) -> np.ndarray:
-        """Take the response frames available now (possibly none)."""
-        out = np.empty(cap, np.uint8)
-        got = ctypes.c_size_t()
-        rc = K.load().dpkem_ring_pop(self.base, out.ctypes.data, cap, ctypes.byref(got))
+    def pop(self, cap: int = 64 << 20, out: np.ndarray | None = None) -> tuple:
+        """Take the response frames available now: (bytes as a view of `out`, frame count)."""
+        if out is None:
+            out = np.empty(cap, np.uint8)
+        got, n = ctypes.c_size_t(), ctypes.c_size_t()
+        rc = K.load().dpkem_ring_pop(self.base, out.ctypes.data, out.nbytes, ctypes.byref(got), ctypes.byref(n))
         if rc != K.OK:
             raise K.DpkemError(rc, "ring_pop")
-        return out[:got.value]
+        return out[:got.value], n.value
 
     def acquire(self, max_frames: int = 0):
         """Server side by hand: None, or dict of the offsets dpkem_ring_acquire returns."""

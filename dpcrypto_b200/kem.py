@@ -90,11 +90,11 @@ EXPORTS = {
     "dpkem_ring_push": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                                        ctypes.POINTER(ctypes.c_size_t)]),
     "dpkem_ring_pop": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
-                                      ctypes.POINTER(ctypes.c_size_t)]),
+                                      ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
     "dpkem_ring_acquire": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t] + [ctypes.POINTER(ctypes.c_size_t)] * 7),
     "dpkem_ring_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t]),
-    "dpkem_ring_serve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
-                                        ctypes.c_int]),
+    "dpkem_ring_serve": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]),
 }
 
 _lib = None

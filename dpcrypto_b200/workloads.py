@@ -61,3 +61,30 @@ class MixedBatch:
 
     def check(self) -> bool:
         return all(torch.equal(got, ref) for got, ref in self.expected)
+
+
+def mixed_frames(eng: K.Engine, n: int, seed: int = 0, first: int = 0) -> np.ndarray:
+    """n request frames (include/dpkem_wire.h), kinds uniform over the 4 schemes x 3 ops
+    and shuffled; id = position.  Keys and ciphertexts come from the batched calls."""
+    from . import frames as F
+
+    rng = np.random.default_rng(seed)
+    kinds = rng.integers(0, 12, size=n)
+    rows = [None] * n
+    for si, scheme in enumerate(MIX_SCHEMES):
+        z = K.sizes(scheme)
+        idx = [np.nonzero(kinds == si * 3 + op)[0] for op in range(3)]
+        m = max(1, len(idx[1]), len(idx[2]))
+        kc = eng.coins(len(idx[0]) + m, z["kp_coins"], "frm-kp", first=first + 100000 * si)
+        ec = eng.coins(m, z["enc_coins"], "frm-enc", first=first + 100000 * si)
+        pk, sk = eng.keypair(scheme, kc[len(idx[0]):], K.FORM_TC)
+        ct, _ = eng.enc(scheme, pk, ec, K.FORM_TC)
+        blocks = [F.encode(scheme, 0, idx[0], coins=kc[:len(idx[0])]),
+                  F.encode(scheme, 1, idx[1], coins=ec[:len(idx[1])], pk=pk[:len(idx[1])]),
+                  F.encode(scheme, 2, idx[2], ct=ct[:len(idx[2])], sk=sk[:len(idx[2])])]
+        for op in range(3):
+            size = F.frame_bytes(scheme, op)[0]
+            b = blocks[op].reshape(-1, size)
+            for j, r in enumerate(idx[op]):
+                rows[r] = b[j]
+    return np.concatenate(rows)

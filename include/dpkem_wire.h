@@ -121,19 +121,23 @@ int dpkem_ring_init(void *base, size_t capacity);
  * *pushed = bytes of `frames` taken.  DPKEM_EAGAIN if not even one frame fits yet;
  * DPKEM_EINVAL for a frame larger than the ring. */
 int dpkem_ring_push(void *base, const uint8_t *frames, size_t bytes, size_t *pushed);
-/* Client: move whole response frames (PAD skipped) into out; *got = bytes copied (0 if none). */
-int dpkem_ring_pop(void *base, uint8_t *out, size_t cap, size_t *got);
-/* Server: take up to max_frames contiguous request frames and reserve room for their
- * responses.  Offsets are relative to each ring's start; *req_advance / *resp_advance
+/* Client: move whole response frames (PAD skipped) into out; *got = bytes copied (0 if
+ * none), *n_frames (if non-null) = frames copied. */
+int dpkem_ring_pop(void *base, uint8_t *out, size_t cap, size_t *got, size_t *n_frames);
+/* Server, one batch at a time: take up to max_frames contiguous request frames and
+ * reserve room for their responses (call dpkem_ring_release before the next acquire).  Offsets are relative to each ring's start; *req_advance / *resp_advance
  * include PAD bytes and are what dpkem_ring_release publishes.  DPKEM_EAGAIN: nothing
  * to take, or no room for even one response; DPKEM_EINVAL: a bad frame, or a response
  * larger than the ring. */
 int dpkem_ring_acquire(void *base, size_t max_frames, size_t *req_off, size_t *req_bytes, size_t *req_advance,
                        size_t *resp_off, size_t *resp_bytes, size_t *resp_advance, size_t *n_frames);
 int dpkem_ring_release(void *base, size_t req_advance, size_t resp_advance, size_t n_frames);
-/* Server loop: acquire / run / release until control->stop is set.  Sleeps idle_us
- * microseconds when idle.  The mapping should be host-registered first. */
-int dpkem_ring_serve(dpkem_ctx *ctx, int form, void *base, size_t max_frames, int idle_us);
+/* Server loop until control->stop is set: batches of up to max_frames request frames are
+ * taken at the server's own cursors and run on ctxs[0..nctx) in turn, so up to nctx
+ * batches are in flight (copies of one overlapping the kernels of another); responses
+ * are published strictly in request order.  Sleeps idle_us microseconds when idle.
+ * Register the mapping with dpkem_host_register first. */
+int dpkem_ring_serve(dpkem_ctx *const *ctxs, int nctx, int form, void *base, size_t max_frames, int idle_us);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -121,10 +121,10 @@ def test_frame_server_process(engine, oracle):
             assert time.time() < deadline and proc.poll() is None
             if len(pending):
                 pending = pending[ring.push(pending):]
-            r = ring.pop()
-            if len(r):
-                got.append(r)
-                n_got += len(F.headers(r))
+            r, count = ring.pop()
+            if count:
+                got.append(r.copy())
+                n_got += count
         resp = np.concatenate(got)
         assert _check(resp, expected, kinds) == req_ids
         assert proc.poll() is None  # still serving

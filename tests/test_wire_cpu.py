@@ -123,8 +123,9 @@ def _client_loop(ring, batches, serve):
             if a is not None:
                 _fake_answer(ring, a)
                 ring.release(a)
-        blk = ring.pop()
+        blk, count = ring.pop()
         pos = 0
+        assert count == (len(F.headers(blk)) if len(blk) else 0)
         for h in (F.headers(blk) if len(blk) else []):
             size = int(h["frame_bytes"])
             assert h["magic"] == F.MAGIC
