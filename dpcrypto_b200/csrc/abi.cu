@@ -403,24 +403,41 @@ int dpkem_dec_batch(dpkem_ctx *c, int scheme, int form, size_t n, const uint8_t 
 
 static_assert(sizeof(dpkem_request) == sizeof(mixed::Req), "request layout");
 
-static int check_requests(size_t n, const dpkem_request *reqs) {
+// device_coins: keypair / encaps requests may leave in0 (coins) null.
+static int check_requests(size_t n, const dpkem_request *reqs, bool device_coins = false) {
   if (!reqs || n == 0 || n > (size_t)INT32_MAX) return DPKEM_EINVAL;
+  alignas(16) static const uint8_t kAligned[16] = {};
   for (size_t i = 0; i < n; i++) {
     const dpkem_request &r = reqs[i];
     Sizes z;
     if (!scheme_sizes(r.scheme, &z) || r.op < 0 || r.op > 2) return DPKEM_EINVAL;
     const bool two_out = r.op != OP_DEC;
-    if (!r.in0 || !r.out0 || (r.op != OP_KEYPAIR && !r.in1) || (two_out && !r.out1)) return DPKEM_EINVAL;
-    if (!op_aligned(r.op, r.in0, r.in1, r.out0, r.out1)) return DPKEM_EINVAL;
+    const bool coins_ok = r.in0 || (device_coins && r.op != OP_DEC);
+    if (!coins_ok || !r.out0 || (r.op != OP_KEYPAIR && !r.in1) || (two_out && !r.out1)) return DPKEM_EINVAL;
+    if (!op_aligned(r.op, r.in0 ? r.in0 : kAligned, r.in1, r.out0, r.out1)) return DPKEM_EINVAL;
   }
   return DPKEM_OK;
 }
 
+static int mixed_batch(dpkem_ctx *c, int form, size_t n, const dpkem_request *reqs, const uint8_t *key,
+                       uint64_t first, void *stream);
+
 int dpkem_mixed_batch(dpkem_ctx *c, int form, size_t n, const dpkem_request *reqs, void *stream) {
+  return mixed_batch(c, form, n, reqs, nullptr, 0, stream);
+}
+
+int dpkem_mixed_batch_keyed(dpkem_ctx *c, int form, size_t n, const dpkem_request *reqs, const uint8_t *key,
+                            uint64_t first, void *stream) {
+  if (!key) return set_status(DPKEM_EINVAL);
+  return mixed_batch(c, form, n, reqs, key, first, stream);
+}
+
+static int mixed_batch(dpkem_ctx *c, int form, size_t n, const dpkem_request *reqs, const uint8_t *key,
+                       uint64_t first, void *stream) {
   if (!c) return set_status(DPKEM_EINVAL);
   if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC && form != DPKEM_FORM_INT32) return set_status(DPKEM_EINVAL);
   if (n == 0) return set_status(DPKEM_OK);
-  int rc = check_requests(n, reqs);
+  int rc = check_requests(n, reqs, key != nullptr);
   if (rc) return set_status(rc);
   std::lock_guard<std::mutex> lock(c->mu);
   cudaSetDevice(c->device);
@@ -433,7 +450,7 @@ int dpkem_mixed_batch(dpkem_ctx *c, int form, size_t n, const dpkem_request *req
   if (e == cudaSuccess) e = mixed::kernel_setup(&grid);
   std::vector<uint8_t> plan(mixed::plan_struct_bytes());
   if (e == cudaSuccess)
-    e = mixed::plan_build(mr, n, form, grid, c->arena, c->arena_bytes, c->d_err, st, plan.data());
+    e = mixed::plan_build(mr, n, form, grid, c->arena, c->arena_bytes, c->d_err, st, plan.data(), key, first);
   if (e == cudaSuccess) e = mixed::plan_launch(plan.data(), n, grid, st);
   if (e == cudaSuccess) e = cudaEventRecord(c->last, st);
   return set_status(cuda_status(e));

@@ -21,9 +21,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <queue>
 #include <vector>
 
+#include "coins_dev.cuh"
 #include "frodo_dev.cuh"
 #include "saber_dev.cuh"
 
@@ -67,10 +69,16 @@ __host__ __device__ constexpr uint32_t threshold(int scheme, int op, int stage) 
 constexpr size_t kFrodoRec = 31744;  // rw 31,360 | k 24 | mu 24 | fail 4 (+12) | sponge 200
 constexpr size_t kFrodoK = frodo::RW * 2, kFrodoMu = kFrodoK + 24, kFrodoFail = kFrodoMu + 24;
 constexpr size_t kFrodoHs = kFrodoFail + 16;
+constexpr size_t kFrodoCoins = kFrodoHs + 200;  // 64 B of device-drawn coins
+static_assert(kFrodoCoins + 64 <= kFrodoRec, "Frodo record too small");
 
+// Saber record: scratch | fail word | two 96-byte coin slots (one per prologue role).
+__host__ __device__ inline size_t saber_scr_bytes(int level) {
+  return level == 2 ? sdev::Scr<2>::BYTES : level == 3 ? sdev::Scr<3>::BYTES : sdev::Scr<4>::BYTES;
+}
+__host__ __device__ inline size_t saber_coins_off(int level) { return (saber_scr_bytes(level) + 4 + 7) & ~(size_t)7; }
 __host__ __device__ inline size_t saber_rec_bytes(int level) {
-  const size_t b = level == 2 ? sdev::Scr<2>::BYTES : level == 3 ? sdev::Scr<3>::BYTES : sdev::Scr<4>::BYTES;
-  return (b + 4 + 255) & ~(size_t)255;
+  return (saber_coins_off(level) + 192 + 255) & ~(size_t)255;
 }
 
 struct DevReq {
@@ -78,6 +86,8 @@ struct DevReq {
   const uint8_t *in0, *in1;
   uint8_t *out0, *out1;
   uint8_t *scr;
+  uint64_t coin_index;  // with gen: coins = SHAKE256(key || LE64(coin_index) || tag), drawn into in0
+  uint32_t gen, pad;
 };
 
 struct Task {
@@ -94,7 +104,17 @@ struct Plan {
   uint32_t *head;
   uint32_t *done;
   uint32_t *err;
+  CoinKey key;  // coin stream key of requests with gen set
 };
+
+// Draws a request's coins into `dst` (the first stage of a keypair / encaps whose request
+// carried none): tag "kp" / "enc", length of the scheme's coins.
+__device__ __forceinline__ void draw_coins(const Plan &p, const DevReq &r, uint8_t *dst) {
+  const uint8_t kp[2] = {'k', 'p'}, enc[3] = {'e', 'n', 'c'};
+  const bool is_kp = r.op == OP_KEYPAIR;
+  const int len = r.scheme == 0 ? (is_kp ? frodo::KP_COINS : frodo::ENC_COINS) : (is_kp ? 96 : 32);
+  coin_generate(p.key, r.coin_index, is_kp ? kp : enc, is_kp ? 2 : 3, len, dst);
+}
 
 __device__ __forceinline__ fdev::Inst frodo_view(const DevReq &r) {
   fdev::Inst v{};
@@ -156,8 +176,15 @@ __device__ __forceinline__ void mark_done(const Plan &p, uint32_t r) {
 }
 
 template <int L>
-__device__ __forceinline__ void saber_thread(int op, int stage, const DevReq &r, int role) {
-  const sdev::Inst v = saber_view<L>(r);
+__device__ __forceinline__ void saber_thread(const Plan &p, int op, int stage, const DevReq &r, int role) {
+  sdev::Inst v = saber_view<L>(r);
+  if (r.gen && stage == 0 && op != OP_DEC) {
+    // each prologue role draws its own copy (role 1 into the second slot), so neither
+    // waits for the other; later stages read the first slot through in0
+    uint8_t *slot = const_cast<uint8_t *>(r.in0) + (role ? 96 : 0);
+    if (role == 0 || op == OP_KEYPAIR) draw_coins(p, r, slot);
+    v.coins = slot;
+  }
   if (op == OP_KEYPAIR) {
     if (stage == 0) sdev::prologue_inst<L, OP_KEYPAIR>(v, role);
     else sdev::finish_inst<L, OP_KEYPAIR>(v);
@@ -170,9 +197,10 @@ __device__ __forceinline__ void saber_thread(int op, int stage, const DevReq &r,
   }
 }
 
-__device__ __forceinline__ void thread_stage(int code, const DevReq &r, int role) {
+__device__ __forceinline__ void thread_stage(const Plan &p, int code, const DevReq &r, int role) {
   const int scheme = scheme_of(code), op = op_of(code), stage = stage_of(code);
   if (scheme == 0) {
+    if (r.gen && stage == 0 && op != OP_DEC) draw_coins(p, r, const_cast<uint8_t *>(r.in0));
     const fdev::Inst v = frodo_view(r);
     if (op == OP_KEYPAIR) {
       if (stage == 0) fdev::kp_prologue_inst(v);
@@ -186,11 +214,11 @@ __device__ __forceinline__ void thread_stage(int code, const DevReq &r, int role
       else fdev::ss_inst<OP_DEC>(v);
     }
   } else if (scheme == 2) {
-    saber_thread<2>(op, stage, r, role);
+    saber_thread<2>(p, op, stage, r, role);
   } else if (scheme == 3) {
-    saber_thread<3>(op, stage, r, role);
+    saber_thread<3>(p, op, stage, r, role);
   } else {
-    saber_thread<4>(op, stage, r, role);
+    saber_thread<4>(p, op, stage, r, role);
   }
 }
 
@@ -282,7 +310,7 @@ __global__ void __launch_bounds__(256, 2) mixed_kernel(Plan p) {
       if (slot < tk.count) {
         const uint32_t r = p.idx[tk.first + slot];
         wait_done(p, r, need);
-        thread_stage(code, p.req[r], role);
+        thread_stage(p, code, p.req[r], role);
         mark_done(p, r);
       }
     }
@@ -355,7 +383,7 @@ size_t plan_bytes(const Req *reqs, size_t n, size_t *ntasks_out) {
 
 // Builds the plan in host memory, uploads it into `arena` and returns the launch descriptor.
 cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *arena, size_t arena_bytes,
-                       uint32_t *err, cudaStream_t st, void *plan_out) {
+                       uint32_t *err, cudaStream_t st, void *plan_out, const uint8_t *coin_key, uint64_t coin_first) {
   size_t ntasks = 0;
   const size_t need = plan_bytes(reqs, n, &ntasks);
   if (need > arena_bytes) return cudaErrorMemoryAllocation;
@@ -377,7 +405,12 @@ cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *
   size_t off = 0;
   for (size_t i = 0; i < n; i++) {
     const Req &r = reqs[i];
-    hreq[i] = DevReq{r.scheme, r.op, r.in0, r.in1, r.out0, r.out1, d_scr + off};
+    uint8_t *rec = d_scr + off;
+    hreq[i] = DevReq{r.scheme, r.op, r.in0, r.in1, r.out0, r.out1, rec, coin_first + i, 0u, 0u};
+    if (coin_key && !r.in0 && r.op != OP_DEC) {  // coins drawn on the device into the record
+      hreq[i].in0 = rec + (r.scheme == 0 ? kFrodoCoins : saber_coins_off(r.scheme));
+      hreq[i].gen = 1;
+    }
     off += r.scheme == 0 ? kFrodoRec : saber_rec_bytes(r.scheme);
   }
   // Tasks per group and stage, with dependencies on the previous stage's tasks.
@@ -470,7 +503,14 @@ cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *
   Plan *p = static_cast<Plan *>(plan_out);
   *p = Plan{reinterpret_cast<const DevReq *>(d_req), reinterpret_cast<const Task *>(d_tasks),
             reinterpret_cast<const uint32_t *>(d_idx), (uint32_t)ntasks, reinterpret_cast<uint32_t *>(d_head),
-            reinterpret_cast<uint32_t *>(d_done), err};
+            reinterpret_cast<uint32_t *>(d_done), err, default_coin_key()};
+  if (coin_key)
+    for (int q = 0; q < 4; q++) {
+      uint32_t lo, hi;
+      std::memcpy(&lo, coin_key + 8 * q, 4);
+      std::memcpy(&hi, coin_key + 8 * q + 4, 4);
+      p->key.w[q] = make_uint2(lo, hi);
+    }
   return cudaSuccess;
 }
 

@@ -54,6 +54,8 @@ EXPORTS = {
     "dpkem_sync": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "dpkem_mixed_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
                                          ctypes.c_void_p]),
+    "dpkem_mixed_batch_keyed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
+                                               ctypes.c_char_p, ctypes.c_uint64, ctypes.c_void_p]),
     "dpkem_mixed_graph_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
                                                 ctypes.POINTER(ctypes.c_void_p)]),
     "dpkem_mixed_graph_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
@@ -309,14 +311,24 @@ class Engine:
             arr[k] = Request(scheme, op, ptr(a), ptr(b), ptr(c), ptr(e))
         return arr
 
-    def mixed(self, items, form: int = FORM_TC):
-        """Run a mixed-scheme, mixed-operation batch as one persistent launch (device buffers)."""
+    def mixed(self, items, form: int = FORM_TC, coin_key: bytes | None = None, coin_first: int = 0):
+        """Run a mixed-scheme, mixed-operation batch as one persistent launch (device buffers).
+        items: (scheme, op, in0, in1, out0, out1) tuples, or a table from Engine.requests.
+        With coin_key (32 bytes), keypair / encaps items whose coins are None draw them on the
+        device: SHAKE256(coin_key || LE64(coin_first + position) || "kp" / "enc")."""
         import torch
 
-        arr = self.requests(items)
+        arr = items if isinstance(items, ctypes.Array) else self.requests(items)  # prebuilt table as is
         st = torch.cuda.current_stream().cuda_stream or 1
-        self._check(self._lib.dpkem_mixed_batch(self._h, form, len(arr), ctypes.cast(arr, ctypes.c_void_p),
-                                                ctypes.c_void_p(st)), "mixed_batch")
+        if coin_key is None:
+            rc = self._lib.dpkem_mixed_batch(self._h, form, len(arr), ctypes.cast(arr, ctypes.c_void_p),
+                                             ctypes.c_void_p(st))
+        else:
+            if len(coin_key) != 32:
+                raise ValueError("coin_key must be 32 bytes")
+            rc = self._lib.dpkem_mixed_batch_keyed(self._h, form, len(arr), ctypes.cast(arr, ctypes.c_void_p),
+                                                   bytes(coin_key), coin_first, ctypes.c_void_p(st))
+        self._check(rc, "mixed_batch")
 
     def mixed_graph(self, items, form: int = FORM_TC) -> "MixedGraph":
         return MixedGraph(self, items, form)

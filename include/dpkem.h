@@ -95,6 +95,14 @@ typedef struct {
 /* Enqueue on `stream` (NULL = context stream); dpkem_sync() reports device-side errors. */
 int dpkem_mixed_batch(dpkem_ctx *ctx, int form, size_t n, const dpkem_request *reqs, void *stream);
 
+/* The same, with device-drawn randomness: a keypair or encaps request whose in0 (coins) is
+ * NULL gets coins = SHAKE256(key[0..32) || LE64(first + i) || "kp" / "enc"), i = its
+ * position in reqs, truncated to the scheme's coin length, computed inside the persistent
+ * kernel by the request's first stage (no host-to-device randomness).  With key = 00 01 ..
+ * 1F these are the dpkem_coins streams. */
+int dpkem_mixed_batch_keyed(dpkem_ctx *ctx, int form, size_t n, const dpkem_request *reqs, const uint8_t *key,
+                            uint64_t first, void *stream);
+
 /* The same batch captured once as a CUDA graph (its own device memory) and replayed. */
 typedef struct dpkem_graph dpkem_graph;
 int dpkem_mixed_graph_create(dpkem_ctx *ctx, int form, size_t n, const dpkem_request *reqs, dpkem_graph **out);

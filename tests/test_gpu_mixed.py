@@ -71,3 +71,59 @@ def test_mixed_graph_replay(engine):
             for got, ref in pairs:
                 assert torch.equal(got, ref)
     g.close()
+
+
+def _host_coins(key, index, tag, length):
+    import hashlib
+    import struct
+
+    return np.frombuffer(hashlib.shake_256(key + struct.pack("<Q", index) + tag).digest(length), np.uint8)
+
+
+@pytest.mark.parametrize("form", [d.FORM_TC, d.FORM_DP4A])
+def test_mixed_device_coins(engine, form):
+    """Keypair / encaps requests without coins draw them inside the persistent kernel; the
+    coins are recomputed independently (hashlib) and checked through the batched calls."""
+    rng = np.random.default_rng(11)
+    key, first = bytes(rng.integers(0, 256, 32, dtype=np.uint8)), 5000
+    items = []
+    for scheme in SCHEMES:
+        z = d.sizes(scheme)
+        pk_base, _ = engine.keypair(scheme, engine.coins(3, z["kp_coins"], "base", first=scheme), d.FORM_TC)
+        for k in range(3):
+            items.append((scheme, 0, None, None, torch.empty(z["pk"], dtype=torch.uint8, device="cuda"),
+                          torch.empty(z["sk"], dtype=torch.uint8, device="cuda")))
+            items.append((scheme, 1, None, torch.from_numpy(pk_base[k].copy()).cuda(),
+                          torch.empty(z["ct"], dtype=torch.uint8, device="cuda"),
+                          torch.empty(z["ss"], dtype=torch.uint8, device="cuda")))
+    items = [items[j] for j in rng.permutation(len(items))]
+    expect = []  # the coin index is the position in the submitted list
+    for pos, (scheme, op, _, in1, o0, o1) in enumerate(items):
+        z = d.sizes(scheme)
+        tag, length = (b"kp", z["kp_coins"]) if op == 0 else (b"enc", z["enc_coins"])
+        c = _host_coins(key, first + pos, tag, length)[None].copy()
+        if op == 0:
+            r0, r1 = engine.keypair(scheme, c, d.FORM_TC)
+        else:
+            r0, r1 = engine.enc(scheme, in1.cpu().numpy()[None], c, d.FORM_TC)
+        expect.append(((o0, r0[0]), (o1, r1[0])))
+    engine.mixed(items, form, coin_key=key, coin_first=first)
+    engine.sync()
+    torch.cuda.synchronize()
+    for pairs in expect:
+        for got, ref in pairs:
+            assert (got.cpu().numpy() == ref).all()
+
+
+def test_mixed_null_inputs_rejected(engine):
+    z = d.sizes(d.SABER)
+    opk = torch.empty(z["pk"], dtype=torch.uint8, device="cuda")
+    osk = torch.empty(z["sk"], dtype=torch.uint8, device="cuda")
+    oss = torch.empty(z["ss"], dtype=torch.uint8, device="cuda")
+    sk = torch.zeros(z["sk"], dtype=torch.uint8, device="cuda")
+    with pytest.raises(d.DpkemError) as e:  # no coins and no key
+        engine.mixed([(d.SABER, 0, None, None, opk, osk)], d.FORM_TC)
+    assert e.value.status == d.kem.EINVAL
+    with pytest.raises(d.DpkemError) as e:  # decaps needs its ciphertext even with a key
+        engine.mixed([(d.SABER, 2, None, sk, oss, None)], d.FORM_TC, coin_key=bytes(32))
+    assert e.value.status == d.kem.EINVAL
