@@ -22,12 +22,12 @@ typedef struct {
 
 static int sizes(int scheme, int op, size_t *o0, size_t *o1, size_t *i0, size_t *i1) {
   size_t pk, sk, ct, ss;
-  if (scheme == 0) {
+  if (scheme == 0 || scheme == 1) {
     pk = ORACLE_FRODO_PK; sk = ORACLE_FRODO_SK; ct = ORACLE_FRODO_CT; ss = ORACLE_FRODO_SS;
   } else if (oracle_saber_sizes(scheme, &pk, &sk, &ct, &ss)) {
     return -1;
   }
-  size_t kpc = scheme == 0 ? ORACLE_FRODO_KP_COINS : 96, encc = scheme == 0 ? ORACLE_FRODO_ENC_COINS : 32;
+  size_t kpc = scheme <= 1 ? ORACLE_FRODO_KP_COINS : 96, encc = scheme <= 1 ? ORACLE_FRODO_ENC_COINS : 32;
   switch (op) {
     case 0: *o0 = pk; *o1 = sk; *i0 = kpc; *i1 = 0; return 0;
     case 1: *o0 = ct; *o1 = ss; *i0 = pk; *i1 = encc; return 0;
@@ -42,9 +42,11 @@ static void *run(void *arg) {
     uint8_t *o0 = w->out0 + i * w->s_out0, *o1 = w->out1 ? w->out1 + i * w->s_out1 : NULL;
     const uint8_t *a = w->in0 + i * w->s_in0, *b = w->in1 ? w->in1 + i * w->s_in1 : NULL;
     int rc;
-    if (w->scheme == 0) {
-      rc = w->op == 0 ? oracle_frodo_keypair(o0, o1, a) : w->op == 1 ? oracle_frodo_enc(o0, o1, a, b)
-                                                                       : oracle_frodo_dec(o0, a, b);
+    if (w->scheme <= 1) { /* 0 FrodoKEM-976-SHAKE, 1 FrodoKEM-976-AES */
+      const int aes = w->scheme;
+      rc = w->op == 0   ? oracle_frodo_keypair_v(o0, o1, a, aes)
+           : w->op == 1 ? oracle_frodo_enc_v(o0, o1, a, b, aes)
+                        : oracle_frodo_dec_v(o0, a, b, aes);
     } else {
       rc = w->op == 0 ? oracle_saber_keypair(w->scheme, o0, o1, a)
            : w->op == 1 ? oracle_saber_enc(w->scheme, o0, o1, a, b)

@@ -1,5 +1,6 @@
 /*
- * CPU oracle: FrodoKEM-976-SHAKE keypair / encaps / decaps (round-3 form).
+ * CPU oracle: FrodoKEM-976-SHAKE and FrodoKEM-976-AES keypair / encaps / decaps
+ * (round-3 form; the two variants differ only in how A is generated).
  *
  * TEST INFRASTRUCTURE ONLY (parity checker and CPU baseline; never linked by the
  * product).  Parity unpinned: the reference ships no Frodo fixture
@@ -20,7 +21,9 @@
  *  - pack: 16-bit words stored MSB first (big-endian), sample_pack.cu:55-198
  *  - Encode/Decode with B = 3 extracted bits, encode_decode.cu:13-53
  *  - A row i = SHAKE128(LE16(i) || seedA, 2n bytes) read as LE uint16 (the spec form;
- *    the reference's shake128_ser truncates the index, SURVEY defect D1/D3).
+ *    the reference's shake128_ser truncates the index); AES variant: A[i][j..j+7] =
+ *    AES128(seedA, LE16(i) || LE16(j) || 0^12) as LE uint16 (the reference declares it,
+ *    FrodoKEM976-GPU/include/aes.h and gen_a_mat_mul.cuh:6-7, but never implements it).
  */
 #include <stdlib.h>
 #include <string.h>
@@ -53,6 +56,32 @@ void oracle_frodo_gen_row(uint16_t *row, const uint8_t *seed_a, int i) {
   memcpy(in + 2, seed_a, SEEDA);
   oracle_shake128(out, sizeof out, in, sizeof in);
   for (int j = 0; j < N; j++) row[j] = (uint16_t)(out[2 * j] | (out[2 * j + 1] << 8));
+}
+
+/* FrodoKEM-976-AES: A[i][j + k] (k < 8) is the k-th LE16 word of
+ * AES128(seedA, LE16(i) || LE16(j) || 0^12), j a multiple of 8 (rk = expanded seedA). */
+static void gen_row_aes(uint16_t *row, const uint8_t rk[176], int i) {
+  uint8_t in[16] = {0}, out[16];
+  in[0] = (uint8_t)i;
+  in[1] = (uint8_t)(i >> 8);
+  for (int j = 0; j < N; j += 8) {
+    in[2] = (uint8_t)j;
+    in[3] = (uint8_t)(j >> 8);
+    oracle_aes128_encrypt(out, in, rk);
+    for (int k = 0; k < 8; k++) row[j + k] = (uint16_t)(out[2 * k] | (out[2 * k + 1] << 8));
+  }
+}
+
+void oracle_frodo_gen_row_aes(uint16_t *row, const uint8_t *seed_a, int i) {
+  uint8_t rk[176];
+  oracle_aes128_expand(rk, seed_a);
+  gen_row_aes(row, rk, i);
+}
+
+/* Row i of A for the variant: rk == NULL selects SHAKE128, else AES-128 with rk. */
+static void gen_row(uint16_t *row, const uint8_t *seed_a, const uint8_t *rk, int i) {
+  if (rk) gen_row_aes(row, rk, i);
+  else oracle_frodo_gen_row(row, seed_a, i);
 }
 
 static void pack_be16(uint8_t *out, const uint16_t *in, size_t n) {
@@ -94,7 +123,7 @@ static void shake256_words(uint16_t *w, size_t count, const uint8_t *in, size_t 
   free(b);
 }
 
-int oracle_frodo_keypair(uint8_t *pk, uint8_t *sk, const uint8_t *coins) {
+int oracle_frodo_keypair_v(uint8_t *pk, uint8_t *sk, const uint8_t *coins, int aes) {
   const uint8_t *s = coins, *seed_se = coins + LENS, *z = coins + LENS + LENSE;
   uint16_t *st = (uint16_t *)malloc(sizeof(uint16_t) * 2 * N * NBAR); /* S^T then E */
   uint16_t *b = (uint16_t *)malloc(sizeof(uint16_t) * N * NBAR);
@@ -107,8 +136,10 @@ int oracle_frodo_keypair(uint8_t *pk, uint8_t *sk, const uint8_t *coins) {
   shake256_words(st, 2 * N * NBAR, in, sizeof in);
   oracle_frodo_sample(st, 2 * N * NBAR);
   const uint16_t *e = st + N * NBAR;
+  uint8_t rk[176];
+  if (aes) oracle_aes128_expand(rk, pk);
   for (int i = 0; i < N; i++) {
-    oracle_frodo_gen_row(row, pk, i);
+    gen_row(row, pk, aes ? rk : NULL, i);
     for (int k = 0; k < NBAR; k++) {
       uint16_t acc = e[i * NBAR + k];
       for (int j = 0; j < N; j++) acc = (uint16_t)(acc + (uint32_t)row[j] * st[k * N + j]);
@@ -129,7 +160,8 @@ int oracle_frodo_keypair(uint8_t *pk, uint8_t *sk, const uint8_t *coins) {
 }
 
 /* Shared by encaps and the decaps re-encryption: B' = S'A + E', C = S'B + E'' + Encode(mu). */
-static void frodo_encrypt(uint16_t *bp, uint16_t *c, const uint8_t *pk, const uint8_t *mu, const uint8_t *seed_se) {
+static void frodo_encrypt(uint16_t *bp, uint16_t *c, const uint8_t *pk, const uint8_t *mu, const uint8_t *seed_se,
+                          int aes) {
   uint16_t *r = (uint16_t *)malloc(sizeof(uint16_t) * (2 * N + NBAR) * NBAR);
   uint16_t *b = (uint16_t *)malloc(sizeof(uint16_t) * N * NBAR);
   uint16_t row[N];
@@ -140,8 +172,10 @@ static void frodo_encrypt(uint16_t *bp, uint16_t *c, const uint8_t *pk, const ui
   oracle_frodo_sample(r, (2 * N + NBAR) * NBAR);
   const uint16_t *sp = r, *ep = r + N * NBAR, *epp = r + 2 * N * NBAR;
   for (int i = 0; i < NBAR * N; i++) bp[i] = ep[i];
+  uint8_t rk[176];
+  if (aes) oracle_aes128_expand(rk, pk);
   for (int j = 0; j < N; j++) {
-    oracle_frodo_gen_row(row, pk, j);
+    gen_row(row, pk, aes ? rk : NULL, j);
     for (int k = 0; k < NBAR; k++) {
       uint16_t s = sp[k * N + j];
       uint16_t *o = bp + k * N;
@@ -161,14 +195,14 @@ static void frodo_encrypt(uint16_t *bp, uint16_t *c, const uint8_t *pk, const ui
   free(b);
 }
 
-int oracle_frodo_enc(uint8_t *ct, uint8_t *ss, const uint8_t *pk, const uint8_t *coins) {
+int oracle_frodo_enc_v(uint8_t *ct, uint8_t *ss, const uint8_t *pk, const uint8_t *coins, int aes) {
   uint8_t g2in[LENPKH + LENMU], g2out[2 * LENSE];
   uint16_t *bp = (uint16_t *)malloc(sizeof(uint16_t) * N * NBAR);
   uint16_t c[NBAR * NBAR];
   oracle_shake256(g2in, LENPKH, pk, ORACLE_FRODO_PK);
   memcpy(g2in + LENPKH, coins, LENMU);
   oracle_shake256(g2out, sizeof g2out, g2in, sizeof g2in);
-  frodo_encrypt(bp, c, pk, coins, g2out);
+  frodo_encrypt(bp, c, pk, coins, g2out, aes);
   pack_be16(ct, bp, N * NBAR);
   pack_be16(ct + PKB, c, NBAR * NBAR);
   uint8_t *fin = (uint8_t *)malloc(ORACLE_FRODO_CT + LENSE);
@@ -180,7 +214,7 @@ int oracle_frodo_enc(uint8_t *ct, uint8_t *ss, const uint8_t *pk, const uint8_t 
   return 0;
 }
 
-int oracle_frodo_dec(uint8_t *ss, const uint8_t *ct, const uint8_t *sk) {
+int oracle_frodo_dec_v(uint8_t *ss, const uint8_t *ct, const uint8_t *sk, int aes) {
   const uint8_t *s = sk, *pk = sk + LENS, *skS = sk + LENS + ORACLE_FRODO_PK;
   const uint8_t *pkh = skS + PKB;
   uint16_t *bp = (uint16_t *)malloc(sizeof(uint16_t) * N * NBAR);
@@ -202,7 +236,7 @@ int oracle_frodo_dec(uint8_t *ss, const uint8_t *ct, const uint8_t *sk) {
   memcpy(g2in, pkh, LENPKH);
   decode_mu(g2in + LENPKH, w);
   oracle_shake256(g2out, sizeof g2out, g2in, sizeof g2in);
-  frodo_encrypt(bpp, cc, pk, g2in + LENPKH, g2out);
+  frodo_encrypt(bpp, cc, pk, g2in + LENPKH, g2out, aes);
   uint16_t diff = 0;
   for (int i = 0; i < N * NBAR; i++) diff |= bp[i] ^ bpp[i];
   for (int i = 0; i < NBAR * NBAR; i++) diff |= c[i] ^ cc[i];
@@ -217,3 +251,9 @@ int oracle_frodo_dec(uint8_t *ss, const uint8_t *ct, const uint8_t *sk) {
   free(bpp);
   return 0;
 }
+
+int oracle_frodo_keypair(uint8_t *pk, uint8_t *sk, const uint8_t *coins) { return oracle_frodo_keypair_v(pk, sk, coins, 0); }
+int oracle_frodo_enc(uint8_t *ct, uint8_t *ss, const uint8_t *pk, const uint8_t *coins) {
+  return oracle_frodo_enc_v(ct, ss, pk, coins, 0);
+}
+int oracle_frodo_dec(uint8_t *ss, const uint8_t *ct, const uint8_t *sk) { return oracle_frodo_dec_v(ss, ct, sk, 0); }

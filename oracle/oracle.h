@@ -6,7 +6,7 @@
  *
  * The reference (DPCrypto) has no CPU implementation and does not vendor the
  * PQClean sources its headers name, so this is a restatement of the published
- * FrodoKEM (round 3, SHAKE variant) and Saber (round 3) algorithms, following the
+ * FrodoKEM (round 3, SHAKE and AES variants) and Saber (round 3) algorithms, following the
  * reference's data flow and byte layouts (file:line citations in each .c file).
  * Saber l=3 is pinned by SABER-GPU/include/tv.h; Keccak by Python hashlib;
  * FrodoKEM-976 and LightSaber/FireSaber have no fixture in the reference
@@ -52,8 +52,18 @@ void oracle_coins_batch(uint8_t *out, size_t len, uint64_t first, size_t count, 
 int oracle_frodo_keypair(uint8_t *pk, uint8_t *sk, const uint8_t *coins);
 int oracle_frodo_enc(uint8_t *ct, uint8_t *ss, const uint8_t *pk, const uint8_t *coins);
 int oracle_frodo_dec(uint8_t *ss, const uint8_t *ct, const uint8_t *sk);
-/* Row i of A as 976 uint16 values. */
+/* Row i of A as 976 uint16 values (SHAKE128 / AES-128 variant). */
 void oracle_frodo_gen_row(uint16_t *row, const uint8_t *seed_a, int i);
+void oracle_frodo_gen_row_aes(uint16_t *row, const uint8_t *seed_a, int i);
+/* aes = 0: FrodoKEM-976-SHAKE, 1: FrodoKEM-976-AES (same sizes and layouts). */
+int oracle_frodo_keypair_v(uint8_t *pk, uint8_t *sk, const uint8_t *coins, int aes);
+int oracle_frodo_enc_v(uint8_t *ct, uint8_t *ss, const uint8_t *pk, const uint8_t *coins, int aes);
+int oracle_frodo_dec_v(uint8_t *ss, const uint8_t *ct, const uint8_t *sk, int aes);
+
+/* ---- AES-128 (FIPS 197) ---- */
+void oracle_aes128_expand(uint8_t rk[176], const uint8_t key[16]);
+void oracle_aes128_encrypt(uint8_t out[16], const uint8_t in[16], const uint8_t rk[176]);
+void oracle_aes128_ecb(uint8_t *out, const uint8_t *in, size_t blocks, const uint8_t key[16]);
 void oracle_frodo_sample(uint16_t *s, size_t n);
 
 /* ---- Saber (level = 2 LightSaber, 3 Saber, 4 FireSaber) ---- */

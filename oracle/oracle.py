@@ -17,6 +17,7 @@ _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 _lib = None
 
 FRODO = 0
+FRODO_AES = 1
 SABER_LEVELS = (2, 3, 4)
 FRODO_SIZES = dict(pk=15632, sk=31296, ct=15744, ss=24, kp_coins=64, enc_coins=24)
 
@@ -44,6 +45,8 @@ def lib():
             "oracle_frodo_enc": [u8p, u8p, u8p, u8p],
             "oracle_frodo_dec": [u8p, u8p, u8p],
             "oracle_frodo_gen_row": [u8p, u8p, ctypes.c_int],
+            "oracle_frodo_gen_row_aes": [u8p, u8p, ctypes.c_int],
+            "oracle_aes128_ecb": [u8p, u8p, ctypes.c_size_t, u8p],
             "oracle_frodo_sample": [u8p, ctypes.c_size_t],
             "oracle_saber_sizes": [ctypes.c_int] + [ctypes.POINTER(ctypes.c_size_t)] * 4,
             "oracle_saber_keypair": [ctypes.c_int, u8p, u8p, u8p],
@@ -59,6 +62,7 @@ def lib():
             fn.restype = ctypes.c_int if name not in ("oracle_shake128", "oracle_shake256", "oracle_sha3_256",
                                                      "oracle_sha3_512", "oracle_coins_batch",
                                                      "oracle_frodo_gen_row", "oracle_frodo_sample",
+                                                     "oracle_frodo_gen_row_aes", "oracle_aes128_ecb",
                                                      "oracle_saber_genmatrix", "oracle_saber_gensecret",
                                                      "oracle_saber_matvec") else None
         _lib = L
@@ -112,7 +116,7 @@ def coins(count: int, length: int, tag: str, first: int = 0) -> np.ndarray:
 
 
 def sizes(scheme: int) -> dict:
-    if scheme == FRODO:
+    if scheme in (FRODO, FRODO_AES):
         return dict(FRODO_SIZES)
     pk, sk, ct, ss = (ctypes.c_size_t() for _ in range(4))
     if lib().oracle_saber_sizes(scheme, ctypes.byref(pk), ctypes.byref(sk), ctypes.byref(ct), ctypes.byref(ss)):
@@ -159,6 +163,22 @@ def frodo_gen_row(seed_a: bytes, i: int) -> np.ndarray:
     s = _u8(seed_a)
     lib().oracle_frodo_gen_row(_p(row), _p(s), i)
     return row
+
+
+def frodo_gen_row_aes(seed_a: bytes, i: int) -> np.ndarray:
+    row = np.zeros(976, np.uint16)
+    s = _u8(seed_a)
+    lib().oracle_frodo_gen_row_aes(_p(row), _p(s), i)
+    return row
+
+
+def aes128_ecb(key: bytes, data: bytes) -> bytes:
+    """AES-128 ECB encryption of whole 16-byte blocks (oracle restatement of FIPS 197)."""
+    if len(key) != 16 or len(data) % 16:
+        raise ValueError("AES-128 ECB needs a 16-byte key and whole blocks")
+    src, out, k = _u8(data), np.zeros(len(data), np.uint8), _u8(key)
+    lib().oracle_aes128_ecb(_p(out), _p(src), len(data) // 16, _p(k))
+    return out.tobytes()
 
 
 def frodo_sample(words: np.ndarray) -> np.ndarray:
