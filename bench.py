@@ -371,6 +371,36 @@ def main():
         line["forms"]["tc_over_int32"] = forms["tc"] / forms["int32"]
         line["forms"]["product_stage_tc_over_dp4a"] = sa_k["dp4a"] / sa_k["tc"]
         line["forms"]["product_stage_tc_over_int32"] = sa_k["int32"] / sa_k["tc"]
+        # FrodoKEM-976-AES at the same batch: only A's generator differs (AES-128 T-tables in
+        # shared memory instead of the SHAKE128 sponge)
+        pk_a, sk_a = eng.keypair(d.FRODO976AES, kc, d.FORM_TC)
+        ares = {}
+        for name, f in (("tc", d.FORM_TC), ("dp4a", d.FORM_DP4A)):
+            for _ in range(2):
+                eng.enc(d.FRODO976AES, pk_a, ec, f, out=(ct, ss))
+                eng.dec(d.FRODO976AES, ct, sk_a, f, out=ss2)
+            eng.profile(True)
+            eng.enc(d.FRODO976AES, pk_a, ec, f, out=(ct, ss))
+            es = eng.stage_times()
+            eng.dec(d.FRODO976AES, ct, sk_a, f, out=ss2)
+            ds = eng.stage_times()
+            eng.profile(False)
+            barrier()
+            reps = max(3, args.steps // 2)
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for _ in range(reps):
+                eng.enc(d.FRODO976AES, pk_a, ec, f, out=(ct, ss))
+                eng.dec(d.FRODO976AES, ct, sk_a, f, out=ss2)
+            t1.record(stream)
+            barrier()
+            ares[name] = world * B * reps / (t0.elapsed_time(t1) * 1e-3)
+            ares[name + "_sa_kernel_ms"] = (es[1] + ds[2]) / 2
+            ares[name + "_aes_blocks_per_s"] = B * 976 * 126 / ((es[1] + ds[2]) / 2 * 1e-3)
+            ares[name + "_roundtrip_ok"] = bool(torch.equal(ss, ss2))
+        ares["tc_over_shake_tc"] = ares["tc"] / value
+        line["frodo976aes_batch8192"] = dict(ares, unit=UNIT, note="AES blocks = 976 rows x 126 (12 x 10.5 per row)")
+
         # Saber l=3, batch 4096 (configs' second workload)
         SB = 4096
         skc = torch.empty((SB, 96), dtype=torch.uint8, device="cuda")

@@ -40,7 +40,7 @@ int set_status(int s) {
 }
 
 bool scheme_sizes(int scheme, Sizes *z) {
-  if (scheme == DPKEM_FRODO976) {
+  if (scheme == DPKEM_FRODO976 || scheme == DPKEM_FRODO976AES) {  // the variants share every size
     *z = {frodo::PK, frodo::SK, frodo::CT, frodo::SS, frodo::KP_COINS, frodo::ENC_COINS};
     return true;
   }
@@ -52,7 +52,7 @@ bool scheme_sizes(int scheme, Sizes *z) {
 
 // Per-instance bytes of scratch and, in host mode, of device staging for each op.
 size_t scratch_per_instance(int scheme) {
-  if (scheme == DPKEM_FRODO976) return (size_t)frodo::RW * 2 + 24 + 24 + 4 + 200 + 80;
+  if (scheme <= DPKEM_FRODO976AES) return (size_t)frodo::RW * 2 + 24 + 24 + 4 + 200 + 80;
   return saber_scratch_bytes(scheme) + 4 + 16;
 }
 
@@ -120,7 +120,7 @@ struct Carver {
 // Layout of one chunk's arena: scratch first, then (host mode) staging.
 size_t arena_need(int scheme, int op, size_t chunk, bool host) {
   size_t s = 0;
-  if (scheme == DPKEM_FRODO976) {
+  if (scheme <= DPKEM_FRODO976AES) {
     s += up(chunk * frodo::RW * 2) + up(chunk * 24) * 2 + up(chunk * 4) + up(chunk * 200);
   } else {
     s += up(chunk * saber_scratch_bytes(scheme)) + up(chunk * 4);
@@ -213,7 +213,7 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
     uint8_t *d_out0, *d_out1 = nullptr;
     FrodoBatch fb{};
     SaberBatch sb{};
-    if (scheme == DPKEM_FRODO976) {
+    if (scheme <= DPKEM_FRODO976AES) {
       fb.rw = cv.take<uint16_t>(chunk * frodo::RW * 2);
       fb.kk = cv.take<uint8_t>(chunk * 24);
       fb.mu = cv.take<uint8_t>(chunk * 24);
@@ -247,8 +247,9 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
     }
     fb.timer = tm;
     sb.timer = tm;
-    if (scheme == DPKEM_FRODO976) {
+    if (scheme <= DPKEM_FRODO976AES) {
       fb.n = (int)m;
+      fb.aes = scheme == DPKEM_FRODO976AES;
       fb.err = c->d_err;
       switch (op) {
         case OP_KEYPAIR:

@@ -61,6 +61,7 @@ enum Form : int { FORM_DP4A = 0, FORM_INT32 = 1, FORM_TC = 2 };
 
 struct FrodoBatch {
   int n;
+  int aes;               // 0: FrodoKEM-976-SHAKE, 1: FrodoKEM-976-AES (A rows from AES-128)
   const uint8_t *coins;  // keypair [n][64] = s||seedSE||z; enc [n][24] = mu
   uint8_t *pk;           // [n][15632]
   uint8_t *sk;           // [n][31296]

@@ -1,5 +1,5 @@
-// FrodoKEM-976-SHAKE batched keypair / encaps / decaps: one launch per stage over n
-// instances.  The stage bodies live in frodo_dev.cuh (shared with the persistent
+// FrodoKEM-976 (SHAKE and AES variants) batched keypair / encaps / decaps: one launch per
+// stage over n instances.  The stage bodies live in frodo_dev.cuh (shared with the persistent
 // mixed-batch kernel); these wrappers only map blockIdx/threadIdx to instances.
 #include "frodo_dev.cuh"
 
@@ -47,13 +47,13 @@ __global__ void __launch_bounds__(256) dec_w_kernel(FrodoBatch b) {
   fdev::dec_w_cta(inst_of(b, blockIdx.x, OP_DEC), smem);
 }
 
-template <int MODE, bool I32>
+template <int MODE, bool I32, class G>
 __global__ void __launch_bounds__(256, 2) sa_dp4a_kernel(FrodoBatch b) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  fdev::sa_dp4a_cta<MODE, I32>(inst_of(b, blockIdx.x, MODE), smem);
+  fdev::sa_dp4a_cta<MODE, I32, G>(inst_of(b, blockIdx.x, MODE), smem);
 }
 
-template <int MODE, int NST>
+template <int MODE, int NST, class G>
 __global__ void __launch_bounds__(256, 2) sa_tc_kernel(FrodoBatch b) {
   using L = fdev::TcLayout<NST>;
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(256, 2) sa_tc_kernel(FrodoBatch b) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = *tslot;
-  fdev::sa_tc_cta<MODE, NST>(inst_of(b, blockIdx.x, MODE), smem, tbase, b.err);
+  fdev::sa_tc_cta<MODE, NST, G>(inst_of(b, blockIdx.x, MODE), smem, tbase, b.err);
   tc_fence_before();
   __syncthreads();
   if (threadIdx.x < 32) {
@@ -75,12 +75,13 @@ __global__ void __launch_bounds__(256, 2) sa_tc_kernel(FrodoBatch b) {
   }
 }
 
-template <bool I32>
+template <bool I32, class G>
 __global__ void __launch_bounds__(256, 2) kp_as_dp4a_kernel(FrodoBatch b) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  fdev::kp_as_dp4a_cta<I32>(inst_of(b, blockIdx.x, OP_KEYPAIR), smem);
+  fdev::kp_as_dp4a_cta<I32, G>(inst_of(b, blockIdx.x, OP_KEYPAIR), smem);
 }
 
+template <int NST, class G>
 __global__ void __launch_bounds__(256, 2) kp_as_tc_kernel(FrodoBatch b) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint32_t tslot;
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(256, 2) kp_as_tc_kernel(FrodoBatch b) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = tslot;
-  fdev::kp_as_tc_cta(inst_of(b, blockIdx.x, OP_KEYPAIR), smem, tbase, b.err);
+  fdev::kp_as_tc_cta<NST, G>(inst_of(b, blockIdx.x, OP_KEYPAIR), smem, tbase, b.err);
   tc_fence_before();
   __syncthreads();
   if (threadIdx.x < 32) {
@@ -110,19 +111,51 @@ cudaError_t set_smem(K kernel, int bytes) {
 
 constexpr int kTcStages = 2;
 
-template <int MODE>
-cudaError_t launch_sa(const FrodoBatch &b, int form, cudaStream_t st) {
+// GT feeds the tcgen05 stage (with NST tile stages per warp), GD the dp4a / INT32 stage.
+// FrodoKEM-976-AES runs its tensor stages with one tile stage: a warp spends thousands of
+// cycles producing a tile, long after the previous tile's MMAs have finished, and the
+// shared memory goes to the AES table copies instead.
+template <int MODE, class GT, class GD, int NST>
+cudaError_t launch_sa_g(const FrodoBatch &b, int form, cudaStream_t st) {
   cudaError_t e;
   if (form == FORM_TC) {
-    constexpr int bytes = fdev::TcLayout<kTcStages>::total;
-    if ((e = set_smem(sa_tc_kernel<MODE, kTcStages>, bytes)) != cudaSuccess) return e;
-    sa_tc_kernel<MODE, kTcStages><<<b.n, 256, bytes, st>>>(b);
+    constexpr int bytes = fdev::TcLayout<NST>::total + GT::SMEM;
+    if ((e = set_smem(sa_tc_kernel<MODE, NST, GT>, bytes)) != cudaSuccess) return e;
+    sa_tc_kernel<MODE, NST, GT><<<b.n, 256, bytes, st>>>(b);
   } else if (form == FORM_INT32) {
-    if ((e = set_smem(sa_dp4a_kernel<MODE, true>, fdev::DP4A_SMEM)) != cudaSuccess) return e;
-    sa_dp4a_kernel<MODE, true><<<b.n, 256, fdev::DP4A_SMEM, st>>>(b);
+    constexpr int bytes = fdev::DP4A_SMEM + GD::SMEM;
+    if ((e = set_smem(sa_dp4a_kernel<MODE, true, GD>, bytes)) != cudaSuccess) return e;
+    sa_dp4a_kernel<MODE, true, GD><<<b.n, 256, bytes, st>>>(b);
   } else {
-    if ((e = set_smem(sa_dp4a_kernel<MODE, false>, fdev::DP4A_SMEM)) != cudaSuccess) return e;
-    sa_dp4a_kernel<MODE, false><<<b.n, 256, fdev::DP4A_SMEM, st>>>(b);
+    constexpr int bytes = fdev::DP4A_SMEM + GD::SMEM;
+    if ((e = set_smem(sa_dp4a_kernel<MODE, false, GD>, bytes)) != cudaSuccess) return e;
+    sa_dp4a_kernel<MODE, false, GD><<<b.n, 256, bytes, st>>>(b);
+  }
+  return cudaGetLastError();
+}
+
+template <int MODE>
+cudaError_t launch_sa(const FrodoBatch &b, int form, cudaStream_t st) {
+  if (b.aes) return launch_sa_g<MODE, fdev::AesRowsFull, fdev::AesRowsHalf, 1>(b, form, st);
+  return launch_sa_g<MODE, fdev::ShakeRows, fdev::ShakeRows, kTcStages>(b, form, st);
+}
+
+template <class G, int NST>
+cudaError_t launch_kp_as(const FrodoBatch &b, int form, cudaStream_t st) {
+  cudaError_t e;
+  if (form == FORM_TC) {
+    constexpr int bytes = fdev::KptLayoutT<NST>::total + G::SMEM;
+    if ((e = set_smem(kp_as_tc_kernel<NST, G>, bytes)) != cudaSuccess) return e;
+    kp_as_tc_kernel<NST, G><<<b.n, 256, bytes, st>>>(b);
+  } else {
+    constexpr int bytes = fdev::KP_AS_SMEM + G::SMEM;
+    if (form == FORM_INT32) {
+      if ((e = set_smem(kp_as_dp4a_kernel<true, G>, bytes)) != cudaSuccess) return e;
+      kp_as_dp4a_kernel<true, G><<<b.n, 256, bytes, st>>>(b);
+    } else {
+      if ((e = set_smem(kp_as_dp4a_kernel<false, G>, bytes)) != cudaSuccess) return e;
+      kp_as_dp4a_kernel<false, G><<<b.n, 256, bytes, st>>>(b);
+    }
   }
   return cudaGetLastError();
 }
@@ -139,15 +172,9 @@ cudaError_t frodo_keypair(const FrodoBatch &b, int form, cudaStream_t st) {
   mark(b, st);
   kp_prologue_kernel<OP_KEYPAIR><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);
-  if (form == FORM_TC) {
-    cudaError_t e = set_smem(kp_as_tc_kernel, fdev::KptLayout::total);
-    if (e != cudaSuccess) return e;
-    kp_as_tc_kernel<<<b.n, 256, fdev::KptLayout::total, st>>>(b);
-  } else if (form == FORM_INT32) {
-    kp_as_dp4a_kernel<true><<<b.n, 256, fdev::KP_AS_SMEM, st>>>(b);
-  } else {
-    kp_as_dp4a_kernel<false><<<b.n, 256, fdev::KP_AS_SMEM, st>>>(b);
-  }
+  const cudaError_t e = b.aes ? launch_kp_as<fdev::AesRowsFull, 1>(b, form, st)
+                             : launch_kp_as<fdev::ShakeRows, fdev::KPT_NST>(b, form, st);
+  if (e != cudaSuccess) return e;
   mark(b, st);
   pk_hash_kernel<OP_KEYPAIR><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);

@@ -280,6 +280,185 @@ __device__ __forceinline__ void row_init(uint2 (&a)[25], uint32_t j, uint2 sa0, 
 
 __device__ __forceinline__ uint32_t bswap16x2(uint32_t v0, uint32_t v1) { return prmt(v0, v1, 0x4501); }
 
+// ---------------------------------------------------------------- A-row generators
+// The stages that consume A take its rows from a generator: start(a, j) begins row j and
+// every next(a) leaves the row's next 84 entries in a[0..20] (4 x u16 per lane, LE), the
+// block one SHAKE128 squeeze yields.  setup() runs on all threads of the CTA before the
+// CTA's first __syncthreads; `mem` is the generator's SMEM bytes of shared memory.
+//   ShakeRows  FrodoKEM-976-SHAKE: row j = SHAKE128(LE16(j) || seedA), one Keccak-f per block.
+//   AesRows    FrodoKEM-976-AES: A[j][8c .. 8c+7] = AES128(seedA, LE16(j) || LE16(8c) || 0^12)
+//              as LE u16; a block is 10.5 AES blocks, the odd half carried to the next call.
+struct ShakeRows {
+  static constexpr int SMEM = 0;
+  uint2 sa0, sa1;
+  __device__ __forceinline__ void setup(const uint8_t *seed, uint8_t *) {
+    sa0 = ld_lane(seed);
+    sa1 = ld_lane(seed + 8);
+  }
+  __device__ __forceinline__ void start(uint2 (&a)[25], uint32_t j) { row_init(a, j, sa0, sa1); }
+  __device__ __forceinline__ void next(uint2 (&a)[25]) { keccak_f1600(a); }
+};
+
+// AES-128 (FIPS 197) tables, evaluated at compile time from the definitions: the S-box is
+// the inverse in GF(2^8) mod x^8 + x^4 + x^3 + x + 1 followed by the affine map (constant
+// 0x63); te[x] holds MixColumns' first column times S(x) as bytes (2S, S, S, 3S), so a
+// round column is te[.] ^ rotl8(te[.]) ^ rotl16(te[.]) ^ rotl24(te[.]) ^ key, and S(x) is
+// byte 1 of te[x].
+namespace aes {
+__host__ __device__ constexpr uint32_t xt(uint32_t a) { return ((a << 1) ^ ((a & 0x80u) ? 0x1Bu : 0u)) & 0xFFu; }
+constexpr uint32_t gmul(uint32_t a, uint32_t b) {
+  uint32_t r = 0;
+  for (int i = 0; i < 8; i++) {
+    if (b & 1u) r ^= a;
+    a = xt(a);
+    b >>= 1;
+  }
+  return r;
+}
+constexpr uint32_t ginv(uint32_t a) {  // a^254
+  uint32_t r = 1, p = a;
+  for (int e = 254; e; e >>= 1) {
+    if (e & 1) r = gmul(r, p);
+    p = gmul(p, p);
+  }
+  return a ? r : 0u;
+}
+constexpr uint32_t rotb(uint32_t b, int k) { return ((b << k) | (b >> (8 - k))) & 0xFFu; }
+constexpr uint32_t sbox(uint32_t x) {
+  const uint32_t b = ginv(x);
+  return b ^ rotb(b, 1) ^ rotb(b, 2) ^ rotb(b, 3) ^ rotb(b, 4) ^ 0x63u;
+}
+struct Table {
+  uint32_t te[256];
+};
+constexpr Table make_table() {
+  Table t{};
+  for (uint32_t x = 0; x < 256; x++) {
+    const uint32_t s = sbox(x), s2 = xt(s);
+    t.te[x] = s2 | (s << 8) | (s << 16) | ((s2 ^ s) << 24);
+  }
+  return t;
+}
+}  // namespace aes
+
+static __constant__ aes::Table kAesTable = aes::make_table();
+
+// C copies of the table, copy c of entry x at word x * C + c (bank c mod 32): with
+// C = 32 every lane reads its own bank, with C = 16 lanes l and l + 16 may meet.
+template <int C>
+struct AesRows {
+  static constexpr int SMEM = 256 * C * 4 + 48 * 4;
+  const uint32_t *T;   // this lane's copy: entry x at T[x * C]
+  const uint32_t *rk;  // 44 round-key words (LE columns), then 4 round-1 constants
+  uint32_t row, cb, odd, r0, r3;
+  uint2 carry;
+
+  __device__ __forceinline__ static uint32_t rot8(uint32_t x) { return __funnelshift_l(x, x, 8); }
+  __device__ __forceinline__ static uint32_t rot16(uint32_t x) { return __funnelshift_l(x, x, 16); }
+  __device__ __forceinline__ static uint32_t rot24(uint32_t x) { return __funnelshift_l(x, x, 24); }
+  __device__ __forceinline__ uint32_t te(uint32_t x) const { return T[x * C]; }
+  __device__ __forceinline__ static uint32_t cte(uint32_t x) { return kAesTable.te[x]; }
+
+  // Key schedule (one thread), then the round-1 terms that depend on the key alone: the
+  // input block's words 1..3 are zero, so three of the four table terms of every round-1
+  // column are constants of the instance.
+  __device__ static void expand(const uint8_t *seed, uint32_t *k) {
+    for (int i = 0; i < 4; i++)
+      k[i] = seed[4 * i] | (seed[4 * i + 1] << 8) | (seed[4 * i + 2] << 16) | ((uint32_t)seed[4 * i + 3] << 24);
+    uint32_t rc = 1;
+    for (int i = 4; i < 44; i++) {
+      uint32_t t = k[i - 1];
+      if ((i & 3) == 0) {
+        t = (t >> 8) | (t << 24);  // RotWord: bytes (a0 a1 a2 a3) -> (a1 a2 a3 a0)
+        t = ((cte(t & 0xFFu) >> 8) & 0xFFu) | (cte((t >> 8) & 0xFFu) & 0xFF00u) |
+            ((cte((t >> 16) & 0xFFu) << 8) & 0xFF0000u) | ((cte(t >> 24) << 16) & 0xFF000000u);  // SubWord
+        t ^= rc;
+        rc = aes::xt(rc);
+      }
+      k[i] = k[i - 4] ^ t;
+    }
+    const uint32_t s1 = k[1], s2 = k[2], s3 = k[3];
+    k[44] = rot8(cte((s1 >> 8) & 0xFFu)) ^ rot16(cte((s2 >> 16) & 0xFFu)) ^ rot24(cte(s3 >> 24)) ^ k[4];
+    k[45] = cte(s1 & 0xFFu) ^ rot8(cte((s2 >> 8) & 0xFFu)) ^ rot16(cte((s3 >> 16) & 0xFFu)) ^ k[5];
+    k[46] = cte(s2 & 0xFFu) ^ rot8(cte((s3 >> 8) & 0xFFu)) ^ rot24(cte(s1 >> 24)) ^ k[6];
+    k[47] = cte(s3 & 0xFFu) ^ rot16(cte((s1 >> 16) & 0xFFu)) ^ rot24(cte(s2 >> 24)) ^ k[7];
+  }
+
+  __device__ __forceinline__ void setup(const uint8_t *seed, uint8_t *mem) {
+    uint32_t *tab = reinterpret_cast<uint32_t *>(mem);
+    uint32_t *k = tab + 256 * C;
+    for (int i = threadIdx.x; i < 256 * C; i += blockDim.x) tab[i] = kAesTable.te[i / C];
+    if (threadIdx.x == 0) expand(seed, k);
+    T = tab + (threadIdx.x & 31) % C;
+    rk = k;
+  }
+
+  __device__ __forceinline__ void start(uint2 (&)[25], uint32_t j) {
+    row = j;
+    cb = 0;
+    odd = 0;
+    const uint32_t s0 = j ^ rk[0];  // bytes 0 and 1 of the first state word depend on the row only
+    r0 = rk[44] ^ te(s0 & 0xFFu);
+    r3 = rk[47] ^ rot8(te((s0 >> 8) & 0xFFu));
+  }
+
+  // Bytes S(b0(a)), S(b1(b)), S(b2(c)), S(b3(d)) of the last round.
+  __device__ __forceinline__ uint32_t last(uint32_t a, uint32_t b, uint32_t c, uint32_t d) const {
+    const uint32_t lo = prmt(te(a & 0xFFu), te((b >> 8) & 0xFFu), 0x0051);
+    const uint32_t hi = prmt(te((c >> 16) & 0xFFu), te(d >> 24), 0x5100);
+    return prmt(lo, hi, 0x7610);
+  }
+
+  // AES-128 of LE16(row) || LE16(8 c) || 0^12.
+  __device__ __forceinline__ uint4 block(uint32_t c) const {
+    const uint32_t s0 = (row | ((8u * c) << 16)) ^ rk[0];
+    uint32_t t0 = r0, t1 = rk[45] ^ rot24(te(s0 >> 24)), t2 = rk[46] ^ rot16(te((s0 >> 16) & 0xFFu)), t3 = r3;
+#pragma unroll
+    for (int r = 2; r < 10; r++) {
+      const uint4 k = *reinterpret_cast<const uint4 *>(rk + 4 * r);
+      const uint32_t u0 = te(t0 & 0xFFu) ^ rot8(te((t1 >> 8) & 0xFFu)) ^ rot16(te((t2 >> 16) & 0xFFu)) ^
+                          rot24(te(t3 >> 24)) ^ k.x;
+      const uint32_t u1 = te(t1 & 0xFFu) ^ rot8(te((t2 >> 8) & 0xFFu)) ^ rot16(te((t3 >> 16) & 0xFFu)) ^
+                          rot24(te(t0 >> 24)) ^ k.y;
+      const uint32_t u2 = te(t2 & 0xFFu) ^ rot8(te((t3 >> 8) & 0xFFu)) ^ rot16(te((t0 >> 16) & 0xFFu)) ^
+                          rot24(te(t1 >> 24)) ^ k.z;
+      const uint32_t u3 = te(t3 & 0xFFu) ^ rot8(te((t0 >> 8) & 0xFFu)) ^ rot16(te((t1 >> 16) & 0xFFu)) ^
+                          rot24(te(t2 >> 24)) ^ k.w;
+      t0 = u0;
+      t1 = u1;
+      t2 = u2;
+      t3 = u3;
+    }
+    const uint4 k = *reinterpret_cast<const uint4 *>(rk + 40);
+    return make_uint4(last(t0, t1, t2, t3) ^ k.x, last(t1, t2, t3, t0) ^ k.y, last(t2, t3, t0, t1) ^ k.z,
+                      last(t3, t0, t1, t2) ^ k.w);
+  }
+
+  __device__ __forceinline__ void next(uint2 (&a)[25]) {
+    uint2 buf[22];
+    const uint32_t nb = odd ? 10u : 11u;
+#pragma unroll 1
+    for (uint32_t b = 0; b < nb; b++) {
+      const uint4 c = block(cb + b);
+      buf[2 * b] = make_uint2(c.x, c.y);
+      buf[2 * b + 1] = make_uint2(c.z, c.w);
+    }
+    cb += nb;
+    if (odd) {
+      a[0] = carry;
+#pragma unroll
+      for (int q = 0; q < 20; q++) a[q + 1] = buf[q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < 21; q++) a[q] = buf[q];
+      carry = buf[21];
+    }
+    odd ^= 1u;
+  }
+};
+using AesRowsFull = AesRows<32>;  // every lane its own bank
+using AesRowsHalf = AesRows<16>;  // half the shared memory (the dp4a / INT32 S'A stage)
+
 // V = S'B + E'' + Encode(mu): 64 outputs over 976 terms, 256 threads.  sval(k, j) yields
 // S'[k][j] sign-extended; C is written to ct (encaps) or compared with it (decaps).
 template <int MODE, typename SVal>
@@ -320,7 +499,7 @@ constexpr int DP4A_SMEM = 83200 + 4 * 64 * 4;
 
 // I32 = true is the plain INT32 form (FrodoKEM976-GPU/src/matrix_kernel.cu:75-111, the
 // reference's non-DP path): the same tiles, 32-bit multiply-adds instead of dp2a.
-template <int MODE, bool I32 = false>
+template <int MODE, bool I32 = false, class G = ShakeRows>
 __device__ __forceinline__ void sa_dp4a_cta(const Inst &v, uint8_t *smem) {
   uint32_t *acc = reinterpret_cast<uint32_t *>(smem);             // [8][976]
   uint32_t *sp8 = reinterpret_cast<uint32_t *>(smem + 31232);     // [248 quads][8 k]: S'[k][4q..4q+3]
@@ -339,14 +518,15 @@ __device__ __forceinline__ void sa_dp4a_cta(const Inst &v, uint8_t *smem) {
     }
     sp8[q] = s;
   }
-  const uint2 sa0 = ld_lane(seed), sa1 = ld_lane(seed + 8);
+  G gen;
+  gen.setup(seed, smem + DP4A_SMEM);
   __syncthreads();
   uint32_t *mt = tile + warp * 32 * 43;
   for (int c = warp; c < ROWS_PAD / 32; c += 8) {
     uint2 a[25];
-    row_init(a, 32 * c + lane, sa0, sa1);
+    gen.start(a, 32 * c + lane);
     for (int blk = 0; blk < 12; blk++) {
-      keccak_f1600(a);
+      gen.next(a);
 #pragma unroll
       for (int q = 0; q < 21; q++) {
         mt[lane * 43 + 2 * q] = a[q].x;
@@ -437,7 +617,7 @@ struct TcLayout {
 
 // TMEM columns [tbase, tbase + 192) must be allocated by the caller.  Returns false if a
 // bounded wait expired (the error word is set; the CTA still leaves TMEM idle).
-template <int MODE, int NST>
+template <int MODE, int NST, class G = ShakeRows>
 __device__ __forceinline__ bool sa_tc_cta(const Inst &v, uint8_t *smem, uint32_t tbase, uint32_t *err) {
   using L = TcLayout<NST>;
   uint8_t *sp = smem;
@@ -464,7 +644,8 @@ __device__ __forceinline__ bool sa_tc_cta(const Inst &v, uint8_t *smem, uint32_t
     mbar_init(&bars[8 * NST], 8);
     fence_mbar_init();
   }
-  const uint2 sa0 = ld_lane(seed), sa1 = ld_lane(seed + 8);
+  G gen;
+  gen.setup(seed, smem + L::total);
   if (warp < 4) {
 #pragma unroll
     for (int col = 0; col < 192; col += 16) tmem_st16_zero(tbase + ((uint32_t)(warp * 32) << 16) + col);
@@ -482,10 +663,10 @@ __device__ __forceinline__ bool sa_tc_cta(const Inst &v, uint8_t *smem, uint32_t
   uint32_t u = 0;
   for (int c = warp; c < ROWS_PAD / 32; c += 8) {
     uint2 a[25];
-    row_init(a, 32 * c + lane, sa0, sa1);
+    gen.start(a, 32 * c + lane);
     const uint64_t bdesc = sdesc(sp_addr + 256 * c, 128, 1024);
     for (int blk = 0; blk < 12; blk++, u++) {
-      keccak_f1600(a);
+      gen.next(a);
       uint32_t lo[21], hi[21];
 #pragma unroll
       for (int q = 0; q < 21; q++) {
@@ -564,7 +745,7 @@ __device__ __forceinline__ bool sa_tc_cta(const Inst &v, uint8_t *smem, uint32_t
 // 8 rows of S^T (broadcast from shared memory), so B[j][k] accumulates in registers.
 constexpr int KP_AS_SMEM = 12 * 21 * 8 * 4;
 
-template <bool I32 = false>
+template <bool I32 = false, class G = ShakeRows>
 __device__ __forceinline__ void kp_as_dp4a_cta(const Inst &v, uint8_t *smem) {
   uint32_t *st8 = reinterpret_cast<uint32_t *>(smem);  // [blk][q][k]: S^T[k][84 blk + 4q .. +3]
   const int tid = threadIdx.x;
@@ -578,16 +759,17 @@ __device__ __forceinline__ void kp_as_dp4a_cta(const Inst &v, uint8_t *smem) {
     }
     st8[x] = s;
   }
-  const uint2 sa0 = ld_lane(v.pk), sa1 = ld_lane(v.pk + 8);
+  G gen;
+  gen.setup(v.pk, smem + KP_AS_SMEM);
   __syncthreads();
   for (int j = tid; j < N; j += 256) {
     uint2 a[25];
-    row_init(a, j, sa0, sa1);
+    gen.start(a, j);
     int acc[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) acc[k] = 0;
     for (int blk = 0; blk < 12; blk++) {
-      keccak_f1600(a);
+      gen.next(a);
 #pragma unroll
       for (int q = 0; q < 21; q++) {
         const uint4 s0 = *reinterpret_cast<const uint4 *>(st8 + (blk * 21 + q) * 8);
@@ -632,23 +814,26 @@ constexpr int KPT_ST_BLK = 6 * 128;                // S^T operand per block (96 
 constexpr int KPT_PLANE = 16 * 768;                // one limb plane of a 128-row tile
 constexpr int KPT_STAGE = 2 * KPT_PLANE;
 constexpr int KPT_NST = 2;
-struct KptLayout {
+template <int NST>
+struct KptLayoutT {
   static constexpr int st = 0;
-  static constexpr int ring = 12 * KPT_ST_BLK;                       // 9216
-  static constexpr int bars = ring + 2 * KPT_NST * KPT_STAGE;        // per warpgroup: NST stage + 1 tile
-  static constexpr int total = bars + 2 * (KPT_NST + 1) * 8;
+  static constexpr int ring = 12 * KPT_ST_BLK;                   // 9216
+  static constexpr int bars = ring + 2 * NST * KPT_STAGE;        // per warpgroup: NST stage + 1 tile
+  static constexpr int total = bars + 2 * (NST + 1) * 8;
 };
+using KptLayout = KptLayoutT<KPT_NST>;
 
 __device__ __forceinline__ void wg_sync(int g) {
   asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory");
 }
 
 // TMEM columns [tbase, tbase + 48) must be allocated by the caller.
+template <int NST = KPT_NST, class G = ShakeRows>
 __device__ __forceinline__ bool kp_as_tc_cta(const Inst &v, uint8_t *smem, uint32_t tbase, uint32_t *err) {
-  using L = KptLayout;
+  using L = KptLayoutT<NST>;
   const int tid = threadIdx.x, warp = tid >> 5, g = warp >> 2, l = tid & 127;
   uint8_t *stop = smem + L::st;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bars) + g * (KPT_NST + 1);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bars) + g * (NST + 1);
   const uint16_t *rw = v.rw;
   // S^T operand of every block, zero-padded to 96 columns.
   for (int x = tid; x < 12 * 8 * 6; x += 256) {
@@ -663,10 +848,11 @@ __device__ __forceinline__ bool kp_as_tc_cta(const Inst &v, uint8_t *smem, uint3
     *reinterpret_cast<uint4 *>(stop + blk * KPT_ST_BLK + q * 128 + k * 16) = make_uint4(w[0], w[1], w[2], w[3]);
   }
   if (l == 0) {
-    for (int q = 0; q < KPT_NST + 1; q++) mbar_init(&bars[q], 1);
+    for (int q = 0; q < NST + 1; q++) mbar_init(&bars[q], 1);
     fence_mbar_init();
   }
-  const uint2 sa0 = ld_lane(v.pk), sa1 = ld_lane(v.pk + 8);
+  G gen;
+  gen.setup(v.pk, smem + L::total);
   fence_proxy_async_smem();
   tc_fence_before();
   __syncthreads();
@@ -674,7 +860,7 @@ __device__ __forceinline__ bool kp_as_tc_cta(const Inst &v, uint8_t *smem, uint3
 
   constexpr uint32_t idesc = idesc_i8(128, 8, false, true, false, false);
   const uint32_t st_addr = smem_u32(stop);
-  uint8_t *ring = smem + L::ring + g * KPT_NST * KPT_STAGE;
+  uint8_t *ring = smem + L::ring + g * NST * KPT_STAGE;
   const uint32_t tcol = tbase + 32 * g;
   const int roff = (l >> 3) * 768 + (l & 7) * 16;
   bool ok = true;
@@ -682,17 +868,17 @@ __device__ __forceinline__ bool kp_as_tc_cta(const Inst &v, uint8_t *smem, uint3
   for (int t = g; t < 8; t += 2, tiles++) {
     const int i = 128 * t + l;
     uint2 a[25];
-    row_init(a, i, sa0, sa1);
+    gen.start(a, i);
     for (int blk = 0; blk < 12; blk++, u++) {
-      keccak_f1600(a);
+      gen.next(a);
       uint32_t lo[21], hi[21];
 #pragma unroll
       for (int q = 0; q < 21; q++) {
         lo[q] = prmt(a[q].x, a[q].y, 0x6420);
         hi[q] = prmt(a[q].x, a[q].y, 0x7531);
       }
-      const int s = u % KPT_NST;
-      if (u >= KPT_NST && ok) ok = mbar_wait(&bars[s], ((u / KPT_NST) - 1) & 1);
+      const int s = u % NST;
+      if (u >= NST && ok) ok = mbar_wait(&bars[s], ((u / NST) - 1) & 1);
       uint8_t *stg = ring + s * KPT_STAGE;
 #pragma unroll
       for (int q = 0; q < 5; q++) {
@@ -717,8 +903,8 @@ __device__ __forceinline__ bool kp_as_tc_cta(const Inst &v, uint8_t *smem, uint3
         mma_commit(&bars[s]);
       }
     }
-    if (l == 0) mma_commit(&bars[KPT_NST]);
-    const bool fin = mbar_wait(&bars[KPT_NST], tiles & 1);
+    if (l == 0) mma_commit(&bars[NST]);
+    const bool fin = mbar_wait(&bars[NST], tiles & 1);
     if (!fin) ok = false;
     tc_fence_after();
     uint32_t r[16];
@@ -741,13 +927,13 @@ __device__ __forceinline__ bool kp_as_tc_cta(const Inst &v, uint8_t *smem, uint3
   }
   // Drain: observe each stage barrier's last phase before the barriers are invalidated.
   bool fin = true;
-  for (int s = 0; s < KPT_NST; s++)
-    if (ok && u > (uint32_t)s) fin &= mbar_wait(&bars[s], ((u - 1 - s) / KPT_NST) & 1);
+  for (int s = 0; s < NST; s++)
+    if (ok && u > (uint32_t)s) fin &= mbar_wait(&bars[s], ((u - 1 - s) / NST) & 1);
   if ((!ok || !fin) && l == 0) atomicOr(err, DEV_ERR_TIMEOUT);
   tc_fence_before();
   __syncthreads();
   if (l == 0 && ok && fin)
-    for (int q = 0; q < KPT_NST + 1; q++) mbar_inval(&bars[q]);
+    for (int q = 0; q < NST + 1; q++) mbar_inval(&bars[q]);
   __syncthreads();
   return ok && fin;
 }

@@ -50,7 +50,7 @@ enum Kind : int { K_THREAD = 0, K_CTA = 1, K_THREAD2 = 2 };
 __host__ __device__ constexpr int nstages(int scheme, int op) { return op == OP_DEC ? 4 : 3; }
 
 __host__ __device__ constexpr int kind_of(int scheme, int op, int stage) {
-  if (scheme == 0) {
+  if (scheme <= 1) {  // FrodoKEM-976, SHAKE (0) or AES (1)
     if (op == OP_DEC) return stage == 0 || stage == 2 ? K_CTA : stage == 1 ? K_THREAD2 : K_THREAD;
     return stage == 1 ? K_CTA : K_THREAD;
   }
@@ -112,7 +112,7 @@ struct Plan {
 __device__ __forceinline__ void draw_coins(const Plan &p, const DevReq &r, uint8_t *dst) {
   const uint8_t kp[2] = {'k', 'p'}, enc[3] = {'e', 'n', 'c'};
   const bool is_kp = r.op == OP_KEYPAIR;
-  const int len = r.scheme == 0 ? (is_kp ? frodo::KP_COINS : frodo::ENC_COINS) : (is_kp ? 96 : 32);
+  const int len = r.scheme <= 1 ? (is_kp ? frodo::KP_COINS : frodo::ENC_COINS) : (is_kp ? 96 : 32);
   coin_generate(p.key, r.coin_index, is_kp ? kp : enc, is_kp ? 2 : 3, len, dst);
 }
 
@@ -199,7 +199,7 @@ __device__ __forceinline__ void saber_thread(const Plan &p, int op, int stage, c
 
 __device__ __forceinline__ void thread_stage(const Plan &p, int code, const DevReq &r, int role) {
   const int scheme = scheme_of(code), op = op_of(code), stage = stage_of(code);
-  if (scheme == 0) {
+  if (scheme <= 1) {
     if (r.gen && stage == 0 && op != OP_DEC) draw_coins(p, r, const_cast<uint8_t *>(r.in0));
     const fdev::Inst v = frodo_view(r);
     if (op == OP_KEYPAIR) {
@@ -242,26 +242,35 @@ __device__ __forceinline__ void saber_cta(int op, int stage, int tc, const DevRe
 
 constexpr int kTcStages = 2;
 
+// Frodo CTA stages with row generator GT (tcgen05 stage, NST tile stages) / GD (others).
+template <class GT, class GD, int NST>
+__device__ __forceinline__ void frodo_cta(int op, int stage, int tc, const DevReq &r, uint8_t *smem, uint32_t tbase,
+                                          uint32_t *err) {
+  const fdev::Inst v = frodo_view(r);
+  if (op == OP_KEYPAIR) {
+    if (tc == FORM_TC) fdev::kp_as_tc_cta<NST == 2 ? fdev::KPT_NST : 1, GT>(v, smem, tbase, err);
+    else if (tc == FORM_INT32) fdev::kp_as_dp4a_cta<true, GT>(v, smem);
+    else fdev::kp_as_dp4a_cta<false, GT>(v, smem);
+  } else if (op == OP_ENC) {
+    if (tc == FORM_TC) fdev::sa_tc_cta<OP_ENC, NST, GT>(v, smem, tbase, err);
+    else if (tc == FORM_INT32) fdev::sa_dp4a_cta<OP_ENC, true, GD>(v, smem);
+    else fdev::sa_dp4a_cta<OP_ENC, false, GD>(v, smem);
+  } else if (stage == 0) {
+    fdev::dec_w_cta(v, smem);
+  } else {
+    if (tc == FORM_TC) fdev::sa_tc_cta<OP_DEC, NST, GT>(v, smem, tbase, err);
+    else if (tc == FORM_INT32) fdev::sa_dp4a_cta<OP_DEC, true, GD>(v, smem);
+    else fdev::sa_dp4a_cta<OP_DEC, false, GD>(v, smem);
+  }
+}
+
 __device__ __forceinline__ void cta_stage(int code, const DevReq &r, uint8_t *smem, uint32_t tbase, uint32_t *err) {
   const int scheme = scheme_of(code), op = op_of(code), stage = stage_of(code);
   const int tc = form_of(code);  // product form (FORM_DP4A / FORM_INT32 / FORM_TC)
   if (scheme == 0) {
-    const fdev::Inst v = frodo_view(r);
-    if (op == OP_KEYPAIR) {
-      if (tc == FORM_TC) fdev::kp_as_tc_cta(v, smem, tbase, err);
-      else if (tc == FORM_INT32) fdev::kp_as_dp4a_cta<true>(v, smem);
-      else fdev::kp_as_dp4a_cta<false>(v, smem);
-    } else if (op == OP_ENC) {
-      if (tc == FORM_TC) fdev::sa_tc_cta<OP_ENC, kTcStages>(v, smem, tbase, err);
-      else if (tc == FORM_INT32) fdev::sa_dp4a_cta<OP_ENC, true>(v, smem);
-      else fdev::sa_dp4a_cta<OP_ENC, false>(v, smem);
-    } else if (stage == 0) {
-      fdev::dec_w_cta(v, smem);
-    } else {
-      if (tc == FORM_TC) fdev::sa_tc_cta<OP_DEC, kTcStages>(v, smem, tbase, err);
-      else if (tc == FORM_INT32) fdev::sa_dp4a_cta<OP_DEC, true>(v, smem);
-      else fdev::sa_dp4a_cta<OP_DEC, false>(v, smem);
-    }
+    frodo_cta<fdev::ShakeRows, fdev::ShakeRows, kTcStages>(op, stage, tc, r, smem, tbase, err);
+  } else if (scheme == 1) {  // FrodoKEM-976-AES (one tile stage: see frodo.cu)
+    frodo_cta<fdev::AesRowsFull, fdev::AesRowsHalf, 1>(op, stage, tc, r, smem, tbase, err);
   } else if (scheme == 2) {
     saber_cta<2>(op, stage, tc, r, smem, tbase, err);
   } else if (scheme == 3) {
@@ -273,7 +282,12 @@ __device__ __forceinline__ void cta_stage(int code, const DevReq &r, uint8_t *sm
 
 constexpr int kSmem = std::max({fdev::TcLayout<kTcStages>::total, fdev::DP4A_SMEM, fdev::DEC_W_SMEM,
                                 fdev::KP_AS_SMEM, fdev::KptLayout::total, sdev::PL<4>::TC_TOTAL, sdev::PL<3>::TC_TOTAL,
-                                sdev::PL<2>::TC_TOTAL});
+                                sdev::PL<2>::TC_TOTAL,
+                                // FrodoKEM-976-AES stages: layout + AES table copies
+                                fdev::TcLayout<1>::total + fdev::AesRowsFull::SMEM,
+                                fdev::DP4A_SMEM + fdev::AesRowsHalf::SMEM, fdev::KP_AS_SMEM + fdev::AesRowsFull::SMEM,
+                                fdev::KptLayoutT<1>::total + fdev::AesRowsFull::SMEM});
+static_assert(kSmem == fdev::TcLayout<kTcStages>::total, "the AES stages must not raise the kernel's shared memory");
 
 __global__ void __launch_bounds__(256, 2) mixed_kernel(Plan p) {
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -327,7 +341,7 @@ __global__ void __launch_bounds__(256, 2) mixed_kernel(Plan p) {
 // Estimated CTA-slot time of each stage (microseconds), used only to order tasks.
 double est_us(int scheme, int op, int stage, int count) {
   const int kind = kind_of(scheme, op, stage);
-  if (scheme == 0) {
+  if (scheme <= 1) {
     if (kind == K_CTA) return op == OP_DEC && stage == 0 ? 30.0 : 1700.0;
     const bool prologue = (op == OP_DEC) ? stage == 1 : stage == 0;
     if (!prologue) return 900.0;
@@ -352,7 +366,7 @@ struct HostTask {
 // Instances per thread-level task (tuning knobs, clamped to what one CTA can hold).
 int task_size(int scheme, int kind) {
   const Tuning &t = tuning();
-  int v = kind == K_THREAD2 ? t.mixed_pair_task : scheme == 0 ? t.mixed_frodo_task : t.mixed_thread_task;
+  int v = kind == K_THREAD2 ? t.mixed_pair_task : scheme <= 1 ? t.mixed_frodo_task : t.mixed_thread_task;
   const int cap = kind == K_THREAD2 ? 128 : 256;
   return std::max(1, std::min(v, cap));
 }
@@ -362,13 +376,13 @@ size_t plan_bytes(const Req *reqs, size_t n, size_t *ntasks_out) {
   size_t scr = 0, ntasks = 0, nidx = 0;
   size_t counts[5][3] = {};
   for (size_t i = 0; i < n; i++) {
-    scr += reqs[i].scheme == 0 ? kFrodoRec : saber_rec_bytes(reqs[i].scheme);
+    scr += reqs[i].scheme <= 1 ? kFrodoRec : saber_rec_bytes(reqs[i].scheme);
     counts[reqs[i].scheme][reqs[i].op]++;
   }
   for (int s = 0; s < 5; s++)
     for (int op = 0; op < 3; op++) {
       const size_t c = counts[s][op];
-      if (!c || s == 1) continue;
+      if (!c) continue;
       for (int st = 0; st < nstages(s, op); st++) {
         const int kind = kind_of(s, op, st);
         const size_t per = kind == K_CTA ? 1 : (size_t)task_size(s, kind);
@@ -408,10 +422,10 @@ cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *
     uint8_t *rec = d_scr + off;
     hreq[i] = DevReq{r.scheme, r.op, r.in0, r.in1, r.out0, r.out1, rec, coin_first + i, 0u, 0u};
     if (coin_key && !r.in0 && r.op != OP_DEC) {  // coins drawn on the device into the record
-      hreq[i].in0 = rec + (r.scheme == 0 ? kFrodoCoins : saber_coins_off(r.scheme));
+      hreq[i].in0 = rec + (r.scheme <= 1 ? kFrodoCoins : saber_coins_off(r.scheme));
       hreq[i].gen = 1;
     }
-    off += r.scheme == 0 ? kFrodoRec : saber_rec_bytes(r.scheme);
+    off += r.scheme <= 1 ? kFrodoRec : saber_rec_bytes(r.scheme);
   }
   // Tasks per group and stage, with dependencies on the previous stage's tasks.
   std::vector<HostTask> ht;

@@ -22,8 +22,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # DPKEM_LIB selects another build of the library (the autotuner measures its variants this way).
 LIB_PATH = os.environ.get("DPKEM_LIB") or os.path.join(HERE, "libdpkem.so")
 
-FRODO976, LIGHTSABER, SABER, FIRESABER = 0, 2, 3, 4
-SCHEMES = (FRODO976, LIGHTSABER, SABER, FIRESABER)
+FRODO976, FRODO976AES, LIGHTSABER, SABER, FIRESABER = 0, 1, 2, 3, 4
+SCHEMES = (FRODO976, FRODO976AES, LIGHTSABER, SABER, FIRESABER)
 FORM_DP4A, FORM_INT32, FORM_TC = 0, 1, 2
 FLAG_DEVICE_PTRS = 1
 OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, EUNSUPPORTED, EAGAIN = 0, -1, -2, -3, -4, -5, -6

@@ -43,8 +43,12 @@ enum {
   DPKEM_EAGAIN = -6        /* non-blocking ring call: nothing to take / no room yet (dpkem_wire.h) */
 };
 
-/* Schemes: the value of a Saber scheme is its module rank l. */
-enum { DPKEM_FRODO976 = 0, DPKEM_LIGHTSABER = 2, DPKEM_SABER = 3, DPKEM_FIRESABER = 4 };
+/* Schemes: the value of a Saber scheme is its module rank l.  DPKEM_FRODO976AES is
+ * FrodoKEM-976-AES: sizes, layouts and every step as DPKEM_FRODO976 except that A is
+ * generated with AES-128 (A[i][j..j+7] = AES128(seedA, LE16(i) || LE16(j) || 0^12)); the
+ * reference declares it (FrodoKEM976-GPU/include/aes.h, gen_a_mat_mul.cuh:6-7) but never
+ * implements it. */
+enum { DPKEM_FRODO976 = 0, DPKEM_FRODO976AES = 1, DPKEM_LIGHTSABER = 2, DPKEM_SABER = 3, DPKEM_FIRESABER = 4 };
 
 /* Product forms. */
 enum { DPKEM_FORM_DP4A = 0, DPKEM_FORM_INT32 = 1, DPKEM_FORM_TC = 2 };
@@ -86,7 +90,7 @@ int dpkem_dec_batch(dpkem_ctx *ctx, int scheme, int form, size_t n, const uint8_
  * work queue; results equal those of the batched calls on the same inputs.  No
  * counterpart in the reference (one scheme per compiled program, fixed launch chains). */
 typedef struct {
-  int32_t scheme; /* DPKEM_FRODO976 / DPKEM_LIGHTSABER / DPKEM_SABER / DPKEM_FIRESABER */
+  int32_t scheme; /* DPKEM_FRODO976 / DPKEM_FRODO976AES / DPKEM_LIGHTSABER / DPKEM_SABER / DPKEM_FIRESABER */
   int32_t op;     /* 0 keypair, 1 encaps, 2 decaps */
   const uint8_t *in0, *in1;
   uint8_t *out0, *out1;

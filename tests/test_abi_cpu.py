@@ -45,8 +45,9 @@ def test_sizes():
     assert (d.sizes(2)["pk"], d.sizes(2)["sk"], d.sizes(2)["ct"]) == (672, 1568, 736)
     assert (d.sizes(3)["pk"], d.sizes(3)["sk"], d.sizes(3)["ct"]) == (992, 2304, 1088)
     assert (d.sizes(4)["pk"], d.sizes(4)["sk"], d.sizes(4)["ct"]) == (1312, 3040, 1472)
+    assert d.sizes(1) == d.sizes(0)  # FrodoKEM-976-AES: the SHAKE variant's sizes
     with pytest.raises(d.DpkemError):
-        d.sizes(1)
+        d.sizes(5)
 
 
 def test_no_silent_fallback_without_device():

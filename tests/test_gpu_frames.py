@@ -14,7 +14,7 @@ import dpcrypto_b200 as d
 from dpcrypto_b200 import frames as F
 
 pytestmark = pytest.mark.gpu
-SCHEMES = [d.FRODO976, d.LIGHTSABER, d.SABER, d.FIRESABER]
+SCHEMES = [d.FRODO976, d.FRODO976AES, d.LIGHTSABER, d.SABER, d.FIRESABER]
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 

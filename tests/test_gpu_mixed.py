@@ -7,7 +7,7 @@ import torch
 import dpcrypto_b200 as d
 
 pytestmark = pytest.mark.gpu
-SCHEMES = [d.FRODO976, d.LIGHTSABER, d.SABER, d.FIRESABER]
+SCHEMES = [d.FRODO976, d.FRODO976AES, d.LIGHTSABER, d.SABER, d.FIRESABER]
 
 
 def _mixed_case(engine, per_kind, seed, form):

@@ -76,7 +76,7 @@ def test_scan_rejects_bad_frames():
     good = F.encode(d.SABER, 2, [1, 2], **_payload(d.SABER, 2, 2, rng))
     size = F.frame_bytes(d.SABER, 2)[0]
     cases = []
-    for field, value in (("magic", 0x12345678), ("version", 2), ("scheme", 1), ("scheme", 5), ("op", 3),
+    for field, value in (("magic", 0x12345678), ("version", 2), ("scheme", 5), ("scheme", 9), ("op", 3),
                          ("frame_bytes", size + 32)):
         bad = good.copy()
         h = bad[:32].view(F.HDR_DTYPE)
