@@ -347,16 +347,27 @@ static __constant__ aes::Table kAesTable = aes::make_table();
 // C = 32 every lane reads its own bank, with C = 16 lanes l and l + 16 may meet.
 template <int C>
 struct AesRows {
-  static constexpr int SMEM = 256 * C * 4 + 48 * 4;
-  const uint32_t *T;   // this lane's copy: entry x at T[x * C]
-  const uint32_t *rk;  // 44 round-key words (LE columns), then 4 round-1 constants
+  static constexpr int SMEM = 256 * C * 4 + 52 * 4;
+  const uint32_t *rk;  // 44 round-key words (LE columns), 4 round-1 constants, the entry stride
+  uint32_t base;       // shared-window address of this lane's table copy
+  uint32_t stride;     // 4 C, read back from shared memory so it stays a multiplier
   uint32_t row, cb, odd, r0, r3;
   uint2 carry;
 
   __device__ __forceinline__ static uint32_t rot8(uint32_t x) { return __funnelshift_l(x, x, 8); }
   __device__ __forceinline__ static uint32_t rot16(uint32_t x) { return __funnelshift_l(x, x, 16); }
   __device__ __forceinline__ static uint32_t rot24(uint32_t x) { return __funnelshift_l(x, x, 24); }
-  __device__ __forceinline__ uint32_t te(uint32_t x) const { return T[x * C]; }
+  // Table entry for byte K of w: one PRMT (the byte into the low position, zeros above)
+  // and one IMAD (address = byte * stride + base) on the FMA pipe, which the Keccak-style
+  // ALU-bound loop leaves idle.
+  template <int K>
+  __device__ __forceinline__ uint32_t tb(uint32_t w) const {
+    const uint32_t b = prmt(w, 0u, 0x4440 | K);
+    uint32_t a, v;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(a) : "r"(b), "r"(stride), "r"(base));
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+    return v;
+  }
   __device__ __forceinline__ static uint32_t cte(uint32_t x) { return kAesTable.te[x]; }
 
   // Key schedule (one thread), then the round-1 terms that depend on the key alone: the
@@ -388,8 +399,11 @@ struct AesRows {
     uint32_t *tab = reinterpret_cast<uint32_t *>(mem);
     uint32_t *k = tab + 256 * C;
     for (int i = threadIdx.x; i < 256 * C; i += blockDim.x) tab[i] = kAesTable.te[i / C];
-    if (threadIdx.x == 0) expand(seed, k);
-    T = tab + (threadIdx.x & 31) % C;
+    if (threadIdx.x == 0) {
+      expand(seed, k);
+      k[48] = 4 * C;
+    }
+    base = smem_u32(tab + (threadIdx.x & 31) % C);
     rk = k;
   }
 
@@ -397,33 +411,30 @@ struct AesRows {
     row = j;
     cb = 0;
     odd = 0;
+    stride = *reinterpret_cast<const volatile uint32_t *>(rk + 48);
     const uint32_t s0 = j ^ rk[0];  // bytes 0 and 1 of the first state word depend on the row only
-    r0 = rk[44] ^ te(s0 & 0xFFu);
-    r3 = rk[47] ^ rot8(te((s0 >> 8) & 0xFFu));
+    r0 = rk[44] ^ tb<0>(s0);
+    r3 = rk[47] ^ rot8(tb<1>(s0));
   }
 
   // Bytes S(b0(a)), S(b1(b)), S(b2(c)), S(b3(d)) of the last round.
   __device__ __forceinline__ uint32_t last(uint32_t a, uint32_t b, uint32_t c, uint32_t d) const {
-    const uint32_t lo = prmt(te(a & 0xFFu), te((b >> 8) & 0xFFu), 0x0051);
-    const uint32_t hi = prmt(te((c >> 16) & 0xFFu), te(d >> 24), 0x5100);
+    const uint32_t lo = prmt(tb<0>(a), tb<1>(b), 0x0051);
+    const uint32_t hi = prmt(tb<2>(c), tb<3>(d), 0x5100);
     return prmt(lo, hi, 0x7610);
   }
 
   // AES-128 of LE16(row) || LE16(8 c) || 0^12.
   __device__ __forceinline__ uint4 block(uint32_t c) const {
     const uint32_t s0 = (row | ((8u * c) << 16)) ^ rk[0];
-    uint32_t t0 = r0, t1 = rk[45] ^ rot24(te(s0 >> 24)), t2 = rk[46] ^ rot16(te((s0 >> 16) & 0xFFu)), t3 = r3;
+    uint32_t t0 = r0, t1 = rk[45] ^ rot24(tb<3>(s0)), t2 = rk[46] ^ rot16(tb<2>(s0)), t3 = r3;
 #pragma unroll
     for (int r = 2; r < 10; r++) {
       const uint4 k = *reinterpret_cast<const uint4 *>(rk + 4 * r);
-      const uint32_t u0 = te(t0 & 0xFFu) ^ rot8(te((t1 >> 8) & 0xFFu)) ^ rot16(te((t2 >> 16) & 0xFFu)) ^
-                          rot24(te(t3 >> 24)) ^ k.x;
-      const uint32_t u1 = te(t1 & 0xFFu) ^ rot8(te((t2 >> 8) & 0xFFu)) ^ rot16(te((t3 >> 16) & 0xFFu)) ^
-                          rot24(te(t0 >> 24)) ^ k.y;
-      const uint32_t u2 = te(t2 & 0xFFu) ^ rot8(te((t3 >> 8) & 0xFFu)) ^ rot16(te((t0 >> 16) & 0xFFu)) ^
-                          rot24(te(t1 >> 24)) ^ k.z;
-      const uint32_t u3 = te(t3 & 0xFFu) ^ rot8(te((t0 >> 8) & 0xFFu)) ^ rot16(te((t1 >> 16) & 0xFFu)) ^
-                          rot24(te(t2 >> 24)) ^ k.w;
+      const uint32_t u0 = tb<0>(t0) ^ rot8(tb<1>(t1)) ^ rot16(tb<2>(t2)) ^ rot24(tb<3>(t3)) ^ k.x;
+      const uint32_t u1 = tb<0>(t1) ^ rot8(tb<1>(t2)) ^ rot16(tb<2>(t3)) ^ rot24(tb<3>(t0)) ^ k.y;
+      const uint32_t u2 = tb<0>(t2) ^ rot8(tb<1>(t3)) ^ rot16(tb<2>(t0)) ^ rot24(tb<3>(t1)) ^ k.z;
+      const uint32_t u3 = tb<0>(t3) ^ rot8(tb<1>(t0)) ^ rot16(tb<2>(t1)) ^ rot24(tb<3>(t2)) ^ k.w;
       t0 = u0;
       t1 = u1;
       t2 = u2;
