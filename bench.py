@@ -42,6 +42,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batch", type=int, default=8192)
     p.add_argument("--form", default="tc", choices=["tc", "dp4a", "int32"])
+    p.add_argument("--scheme", default="frodo976", choices=["frodo976", "frodo976aes"],
+                   help="headline workload: FrodoKEM-976-SHAKE (default) or FrodoKEM-976-AES")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-secondary", action="store_true")
@@ -54,10 +56,14 @@ def dist_env():
     return env()
 
 
+SCHEME_NAMES = {"frodo976": "FrodoKEM-976-SHAKE", "frodo976aes": "FrodoKEM-976-AES"}
+
+
 def config(args, world):
+    name = SCHEME_NAMES[args.scheme]
     return {
-        "workload": f"FrodoKEM-976-SHAKE encaps+decaps, batch {args.batch} per GPU, {args.form} product form",
-        "scheme": "FrodoKEM-976-SHAKE", "batch_per_gpu": args.batch, "global_batch": args.batch * world,
+        "workload": f"{name} encaps+decaps, batch {args.batch} per GPU, {args.form} product form",
+        "scheme": name, "batch_per_gpu": args.batch, "global_batch": args.batch * world,
         "form": args.form, "parallelism": f"instances sharded, {world} replica(s)",
         "l2": "inputs larger than L2 (pk+sk+ct per step = %d MB per GPU)" % (args.batch * (15632 + 31296 + 15744) >> 20),
     }
@@ -262,6 +268,7 @@ def main():
     pg = D.init("nccl", timeout_s=120.0, device=torch.device("cuda", local)) if world > 1 else None
     eng = d.Engine(local)
     form = {"tc": d.FORM_TC, "dp4a": d.FORM_DP4A, "int32": d.FORM_INT32}[args.form]
+    FS = {"frodo976": d.FRODO976, "frodo976aes": d.FRODO976AES}[args.scheme]
     B = args.batch
     stream = torch.cuda.current_stream()
 
@@ -271,14 +278,14 @@ def main():
     ec = torch.empty((B, 24), dtype=torch.uint8, device="cuda")
     eng.coins(B, 64, "kp", first=first, out=kc)
     eng.coins(B, 24, "enc", first=first, out=ec)
-    pk, sk = eng.keypair(d.FRODO976, kc, d.FORM_TC)
+    pk, sk = eng.keypair(FS, kc, d.FORM_TC)
     ct = torch.empty((B, 15744), dtype=torch.uint8, device="cuda")
     ss = torch.empty((B, 24), dtype=torch.uint8, device="cuda")
     ss2 = torch.empty((B, 24), dtype=torch.uint8, device="cuda")
 
     def step(f):
-        eng.enc(d.FRODO976, pk, ec, f, out=(ct, ss))
-        eng.dec(d.FRODO976, ct, sk, f, out=ss2)
+        eng.enc(FS, pk, ec, f, out=(ct, ss))
+        eng.dec(FS, ct, sk, f, out=ss2)
 
     def barrier():
         torch.cuda.synchronize()
@@ -293,10 +300,10 @@ def main():
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         for _ in range(steps):
-            eng.enc(d.FRODO976, pk, ec, f, out=(ct, ss))
+            eng.enc(FS, pk, ec, f, out=(ct, ss))
             if profile:
                 stages["enc"].append(eng.stage_times())
-            eng.dec(d.FRODO976, ct, sk, f, out=ss2)
+            eng.dec(FS, ct, sk, f, out=ss2)
             if profile:
                 stages["dec"].append(eng.stage_times())
         t1.record(stream)
@@ -351,6 +358,15 @@ def main():
         "stage_ms": stage_ms, "stage_share_of_step": {k: sum(v.values()) / kernel_total for k, v in stage_ms.items()},
         "clocks": clocks,
     }
+    if FS == d.FRODO976AES:  # A from AES-128 T-tables: integer ALU and load/store pipes, no Keccak
+        line["roofline"] = {
+            "kernel": "sa_tc_kernel<AesRows> (AES-128 A rows -> int8 tcgen05 S'A)" if form == d.FORM_TC
+            else "sa_dp4a_kernel<AesRows>", "bound": "int+lsu", "unit": "G AES blocks/s",
+            "achieved": B * FRODO_ROWS * 126 / (sa_avg * 1e-3) / 1e9, "peak": None, "frac": None,
+            "algorithmic": "126 AES-128 blocks per A row (12 x 10.5) x 976 rows x batch",
+            "avg_launch_ms": sa_avg, "traffic": None,
+            "note": "no single-pipe peak: ALU and LSU both ~73 % busy (profiles/frodo976aes_sa_tc_b1184.md)",
+        }
 
     # ---- the other product forms (tc / dp4a / int32) on the same GPU ----
     if not args.no_secondary:
@@ -532,13 +548,13 @@ def main():
         h_ss = torch.empty((B, 24), dtype=torch.uint8).pin_memory().numpy()
         h_ss2 = torch.empty((B, 24), dtype=torch.uint8).pin_memory().numpy()
         for _ in range(max(1, args.warmup)):
-            eng.enc(d.FRODO976, h_pk, h_ec, form, out=(h_ct, h_ss))
-            eng.dec(d.FRODO976, h_ct, h_sk, form, out=h_ss2)
+            eng.enc(FS, h_pk, h_ec, form, out=(h_ct, h_ss))
+            eng.dec(FS, h_ct, h_sk, form, out=h_ss2)
         barrier()
         t = time.perf_counter()
         for _ in range(args.steps):
-            eng.enc(d.FRODO976, h_pk, h_ec, form, out=(h_ct, h_ss))
-            eng.dec(d.FRODO976, h_ct, h_sk, form, out=h_ss2)
+            eng.enc(FS, h_pk, h_ec, form, out=(h_ct, h_ss))
+            eng.dec(FS, h_ct, h_sk, form, out=h_ss2)
         el = D.max_over_ranks(time.perf_counter() - t, device="cuda")
         h2d_b, d2h_b = B * (15632 + 24 + 15744 + 31296), B * (15744 + 24 + 24)
         h2d_gbs, d2h_gbs = pcie_gbs(True), pcie_gbs(False)
