@@ -562,6 +562,7 @@ def main():
                        "h2d_bytes_per_step": h2d_b, "d2h_bytes_per_step": d2h_b,
                        "roundtrip_ok": bool((h_ss == h_ss2).all()),
                        "pipeline_chunks": d.kem.get_tuning().get("pipe_chunks"),
+                       "pipeline_stream_priorities": bool(d.kem.get_tuning().get("pipe_priority")),
                        "pcie_gbs": {"h2d": h2d_gbs, "d2h": d2h_gbs},
                        "copy_ms_per_step_if_serial": 1e3 * (h2d_b / (h2d_gbs * 1e9) + d2h_b / (d2h_gbs * 1e9))}
 

@@ -192,7 +192,7 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
   if (npipe > 1) {
     if ((e = cudaEventRecord(c->pev[0], st)) != cudaSuccess) return cuda_status(e);
     for (int j = 0; j < npipe; j++) {
-      streams[j] = c->pipe[j];
+      streams[j] = tuning().pipe_priority ? c->ppipe[j] : c->pipe[j];
       if ((e = cudaStreamWaitEvent(streams[j], c->pev[0], 0)) != cudaSuccess) return cuda_status(e);
     }
   }
@@ -334,6 +334,10 @@ int dpkem_ctx_create(dpkem_ctx **out, int device, size_t hbm_budget_bytes) {
   for (int j = 0; j < kPipeChunks; j++) {
     cudaStreamCreateWithFlags(&c->pipe[j], cudaStreamNonBlocking);
     cudaEventCreateWithFlags(&c->pev[j], cudaEventDisableTiming);
+    int least = 0, greatest = 0;  // numerically, greatest <= least
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    const int prio = greatest + (least - greatest) * j / (kPipeChunks - 1);
+    cudaStreamCreateWithPriority(&c->ppipe[j], cudaStreamNonBlocking, prio);
   }
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->last, cudaEventDisableTiming) != cudaSuccess ||
@@ -358,6 +362,10 @@ int dpkem_ctx_destroy(dpkem_ctx *c) {
     if (c->pipe[j]) {
       cudaStreamSynchronize(c->pipe[j]);
       cudaStreamDestroy(c->pipe[j]);
+    }
+    if (c->ppipe[j]) {
+      cudaStreamSynchronize(c->ppipe[j]);
+      cudaStreamDestroy(c->ppipe[j]);
     }
     if (c->pev[j]) cudaEventDestroy(c->pev[j]);
   }
@@ -614,9 +622,10 @@ int dpkem_probe_int_peaks(dpkem_ctx *c, double *int_ops_per_s, double *keccak_pe
 }
 
 int dpkem_set_tuning(const char *key, int value) {
-  if (!key || value <= 0) return set_status(DPKEM_EINVAL);
+  if (!key || value < 0) return set_status(DPKEM_EINVAL);
   Tuning &t = tuning();
   const std::string k(key);
+  if (value == 0 && k != "pipe_priority") return set_status(DPKEM_EINVAL);  // the switch alone may be 0
   if (k == "thread_block") {
     if (value % 32 || value > 256) return set_status(DPKEM_EINVAL);
     t.thread_block = value;
@@ -628,6 +637,8 @@ int dpkem_set_tuning(const char *key, int value) {
     t.mixed_thread_task = std::min(value, 256);
   } else if (k == "pipe_chunks") {
     t.pipe_chunks = std::min(value, kPipeChunks);
+  } else if (k == "pipe_priority") {
+    t.pipe_priority = value != 0;
   } else {
     return set_status(DPKEM_EINVAL);
   }

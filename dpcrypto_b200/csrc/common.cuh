@@ -44,6 +44,7 @@ struct Tuning {
   int mixed_pair_task = 128;    // instances per two-role prologue task (two threads each)
   int mixed_thread_task = 256;  // instances per other thread-level task
   int pipe_chunks = 4;          // chunks (one stream each) of a pipelined host-mode batch, <= 8
+  int pipe_priority = 1;        // 1: chunk streams get descending priorities (earlier chunks finish first)
 };
 Tuning &tuning();
 

@@ -15,6 +15,7 @@ struct dpkem_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t last = nullptr;  // recorded after every launch chain that used the arena
   cudaStream_t pipe[8] = {};   // host-mode copy/compute pipeline, one stream per chunk
+  cudaStream_t ppipe[8] = {};  // the same with descending priorities (chunk 0 highest)
   cudaEvent_t pev[8] = {};
   uint8_t *arena = nullptr;
   size_t arena_bytes = 0;
