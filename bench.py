@@ -512,27 +512,33 @@ def main():
 
     # ---- serving loop: Poisson arrivals, 60 % encaps / 40 % decaps, 50/50 Frodo / Saber l=3 ----
     if not args.no_secondary and world == 1:
-        from dpcrypto_b200.serving import RequestPool, Server, poisson_arrivals
+        from dpcrypto_b200.serving import FRODO_CLASS, SABER_CLASS, RequestPool, Server, poisson_arrivals
 
         pool = RequestPool(eng, 16384, seed=0)
         serving = {"requests_per_level": pool.n, "mix": "60% encaps / 40% decaps, 50/50 FrodoKEM-976 / Saber l=3",
-                   "slots": 4, "max_batch": 4096, "unit": "KEM ops/s"}
+                   "slots": 4, "max_batch": 4096, "unit": "KEM ops/s",
+                   "modes": {"shared": "every slot takes any request",
+                             "split": "2 slots for Frodo requests, 2 for Saber requests"}}
         for name, f in (("tc", d.FORM_TC), ("dp4a", d.FORM_DP4A)):
-            srv = Server(slots=4, max_batch=4096, form=f)
-            try:
-                srv.run(pool, np.zeros(2048))  # warm-up
-                peak = srv.run(pool, np.zeros(pool.n))["ops_per_s"]
-                levels = []
-                for frac in (0.1, 0.25, 0.5, 0.75, 1.0):
-                    pool.clear()
-                    r = srv.run(pool, poisson_arrivals(pool.n, rate=frac * peak, seed=int(frac * 100)))
-                    levels.append({"load": frac, "offered_per_s": frac * peak, "ops_per_s": r["ops_per_s"],
-                                   "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "mean_batch": r["mean_batch"],
-                                   "host_max_gap_ms": r["host_max_gap_ms"]})
-                torch.cuda.synchronize()
-                serving[name] = {"peak_ops_per_s": peak, "levels": levels, "bit_exact": pool.check()}
-            finally:
-                srv.close()
+            for mode, classes in (("shared", None), ("split", [FRODO_CLASS, FRODO_CLASS, SABER_CLASS, SABER_CLASS])):
+                srv = Server(slots=4, max_batch=4096, form=f, classes=classes)
+                try:
+                    srv.run(pool, np.zeros(2048))  # warm-up
+                    peak = srv.run(pool, np.zeros(pool.n))["ops_per_s"]
+                    levels = []
+                    for frac in (0.1, 0.25, 0.5, 0.75, 1.0):
+                        pool.clear()
+                        r = srv.run(pool, poisson_arrivals(pool.n, rate=frac * peak, seed=int(frac * 100)))
+                        levels.append({"load": frac, "offered_per_s": frac * peak, "ops_per_s": r["ops_per_s"],
+                                       "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "mean_batch": r["mean_batch"],
+                                       "frodo_p50_ms": r["frodo_p50_ms"], "frodo_p99_ms": r["frodo_p99_ms"],
+                                       "saber_p50_ms": r["saber_p50_ms"], "saber_p99_ms": r["saber_p99_ms"],
+                                       "host_max_gap_ms": r["host_max_gap_ms"], "submit_ms_max": r["submit_ms_max"]})
+                    torch.cuda.synchronize()
+                    key = name if mode == "shared" else f"{name}_split"
+                    serving[key] = {"peak_ops_per_s": peak, "levels": levels, "bit_exact": pool.check()}
+                finally:
+                    srv.close()
         line["serving"] = serving
 
     # ---- wire format: 16384 mixed request frames from pinned host memory, then the same

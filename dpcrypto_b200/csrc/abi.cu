@@ -72,9 +72,13 @@ size_t chunk_for(dpkem_ctx *c, int scheme, int op, bool host) {
   return std::max<size_t>(1, usable / per);
 }
 
+// Growing the arena frees the old one (cudaFree waits for the whole device, other
+// contexts' work included), so growth is geometric (at least 1.5x, within the budget) and
+// callers on a latency path reserve the arena up front (dpkem_ctx_reserve).
 int ensure_arena(dpkem_ctx *c, size_t bytes) {
   if (bytes <= c->arena_bytes) return DPKEM_OK;
   if (bytes > c->budget) return DPKEM_ENOMEM;
+  const size_t want = std::min(c->budget, std::max(bytes, c->arena_bytes + c->arena_bytes / 2));
   if (c->arena) {
     // c->last follows every launch that used the arena, on whichever stream it ran
     cudaEventSynchronize(c->last);
@@ -82,11 +86,11 @@ int ensure_arena(dpkem_ctx *c, size_t bytes) {
     c->arena = nullptr;
     c->arena_bytes = 0;
   }
-  if (cudaMalloc(&c->arena, bytes) != cudaSuccess) {
+  if (cudaMalloc(&c->arena, want) != cudaSuccess) {
     cudaGetLastError();
     return DPKEM_ENOMEM;
   }
-  c->arena_bytes = bytes;
+  c->arena_bytes = want;
   return DPKEM_OK;
 }
 
@@ -94,6 +98,12 @@ int cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return DPKEM_OK;
   cudaGetLastError();
   return DPKEM_ECUDA;
+}
+
+cudaError_t persistent_grid(const dpkem_ctx *c, int *grid) {
+  const cudaError_t e = mixed::kernel_setup(grid);
+  if (e == cudaSuccess && c->max_ctas > 0) *grid = std::min(*grid, c->max_ctas);
+  return e;
 }
 
 }  // namespace abi
@@ -169,7 +179,7 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
   if (cudaSetDevice(c->device) != cudaSuccess) return cuda_status(cudaErrorInvalidDevice);
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
   // Host-mode batches of at least two minimum chunks, when the budget holds the whole batch,
-  // run as a pipeline: up to four chunks, each on its own stream with its own arena region,
+  // run as a pipeline: up to pipe_chunks chunks, each on its own stream with its own arena region,
   // all in flight at once.  The copies of later chunks and their latency-bound first stages
   // then overlap the long kernels of earlier chunks.
   size_t chunk = std::min(n, chunk_for(c, scheme, op, !dev));
@@ -350,6 +360,27 @@ int dpkem_ctx_create(dpkem_ctx **out, int device, size_t hbm_budget_bytes) {
   return set_status(DPKEM_OK);
 }
 
+int dpkem_ctx_reserve(dpkem_ctx *c, size_t bytes) {
+  if (!c) return set_status(DPKEM_EINVAL);
+  std::lock_guard<std::mutex> lock(c->mu);
+  if (cudaSetDevice(c->device) != cudaSuccess) return set_status(cuda_status(cudaErrorInvalidDevice));
+  return set_status(ensure_arena(c, bytes));
+}
+
+size_t dpkem_mixed_bytes(int scheme, size_t n) {
+  Sizes z;
+  if (!scheme_sizes(scheme, &z) || n == 0) return 0;
+  std::vector<mixed::Req> rq(n, mixed::Req{scheme, OP_ENC, nullptr, nullptr, nullptr, nullptr});
+  return mixed::plan_bytes(rq.data(), n, nullptr);
+}
+
+int dpkem_ctx_set_max_ctas(dpkem_ctx *c, int max_ctas) {
+  if (!c || max_ctas < 0) return set_status(DPKEM_EINVAL);
+  std::lock_guard<std::mutex> lock(c->mu);
+  c->max_ctas = max_ctas;
+  return set_status(DPKEM_OK);
+}
+
 int dpkem_ctx_destroy(dpkem_ctx *c) {
   if (!c) return set_status(DPKEM_EINVAL);
   cudaSetDevice(c->device);
@@ -456,7 +487,7 @@ static int mixed_batch(dpkem_ctx *c, int form, size_t n, const dpkem_request *re
   if ((rc = ensure_arena(c, need)) != DPKEM_OK) return set_status(rc);
   cudaError_t e = cudaStreamWaitEvent(st, c->last, 0);
   int grid = 0;
-  if (e == cudaSuccess) e = mixed::kernel_setup(&grid);
+  if (e == cudaSuccess) e = persistent_grid(c, &grid);
   std::vector<uint8_t> plan(mixed::plan_struct_bytes());
   if (e == cudaSuccess)
     e = mixed::plan_build(mr, n, form, grid, c->arena, c->arena_bytes, c->d_err, st, plan.data(), key, first);
@@ -506,7 +537,7 @@ int dpkem_mixed_graph_create(dpkem_ctx *c, int form, size_t n, const dpkem_reque
   int grid = 0;
   std::vector<uint8_t> plan(mixed::plan_struct_bytes());
   cudaStream_t cap = nullptr;
-  e = mixed::kernel_setup(&grid);
+  e = persistent_grid(c, &grid);
   if (e == cudaSuccess) e = mixed::plan_build(mr, n, form, grid, g->mem, need, c->d_err, c->stream, plan.data());
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);

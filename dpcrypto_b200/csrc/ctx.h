@@ -20,6 +20,7 @@ struct dpkem_ctx {
   uint8_t *arena = nullptr;
   size_t arena_bytes = 0;
   uint32_t *d_err = nullptr;
+  int max_ctas = 0;  // persistent launches use at most this many CTAs (0: two per SM)
   bool profile = false;
   dpkem::StageTimer timer;
   int timer_stages = 0;
@@ -42,6 +43,8 @@ int set_status(int s);                      // records the calling thread's last
 bool scheme_sizes(int scheme, Sizes *z);    // object sizes of a scheme; false if unknown
 int ensure_arena(dpkem_ctx *c, size_t bytes);  // grows the context's device arena
 int cuda_status(cudaError_t e);             // DPKEM_OK or DPKEM_ECUDA (clears the error)
+// Grid of this context's persistent launches: the device's resident CTAs, capped by max_ctas.
+cudaError_t persistent_grid(const dpkem_ctx *c, int *grid);
 
 }  // namespace abi
 }  // namespace dpkem

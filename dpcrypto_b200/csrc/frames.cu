@@ -202,7 +202,7 @@ int frames_submit(dpkem_ctx *c, int form, const uint8_t *req, size_t req_bytes, 
   if (e == cudaSuccess) e = cudaEventRecord(c->pev[0], st);
   for (int j = 0; j < npipe && e == cudaSuccess; j++) e = cudaStreamWaitEvent(c->pipe[j], c->pev[0], 0);
   int grid = 0;
-  if (e == cudaSuccess) e = mixed::kernel_setup(&grid);
+  if (e == cudaSuccess) e = persistent_grid(c, &grid);
   uint32_t rtab[15], rend[15];
   resp_table(rtab, rend);
   std::vector<std::vector<uint8_t>> plans(gs.size(), std::vector<uint8_t>(mixed::plan_struct_bytes()));

@@ -38,6 +38,9 @@ class Request(ctypes.Structure):
 EXPORTS = {
     "dpkem_ctx_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_size_t]),
     "dpkem_ctx_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dpkem_ctx_set_max_ctas": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "dpkem_ctx_reserve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t]),
+    "dpkem_mixed_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_size_t]),
     "dpkem_sizes": (ctypes.c_int, [ctypes.c_int] + [ctypes.POINTER(ctypes.c_size_t)] * 6),
     "dpkem_max_chunk": (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int]),
     "dpkem_keypair_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_size_t,
@@ -274,6 +277,14 @@ class Engine:
         self._check(self._lib.dpkem_dec_batch(self._h, scheme, form, n, _ptr(ct), _ptr(sk), _ptr(ss), flags, st),
                     "dec")
         return ss
+
+    def reserve(self, nbytes: int):
+        """Grow this engine's device arena to nbytes now, outside any latency-critical call."""
+        self._check(self._lib.dpkem_ctx_reserve(self._h, nbytes), "reserve")
+
+    def set_max_ctas(self, max_ctas: int):
+        """Cap the CTAs of this engine's persistent launches (0 = the whole GPU)."""
+        self._check(self._lib.dpkem_ctx_set_max_ctas(self._h, max_ctas), "set_max_ctas")
 
     def coins(self, n: int, length: int, tag: str, first: int = 0, out=None):
         out = out if out is not None else np.empty((n, length), np.uint8)

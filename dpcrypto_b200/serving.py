@@ -83,14 +83,43 @@ class RequestPool:
         return all(torch.equal(got, ref) for got, ref in self.expected)
 
 
+FRODO_CLASS, SABER_CLASS = 0, 1
+
+
 class Server:
+    """slots engines (a dpkem context and a CUDA stream each).  classes: None, every slot
+    takes any request; or one entry per slot, FRODO_CLASS (FrodoKEM-976, both variants) or
+    SABER_CLASS, and a request is admitted only to a slot of its class.  Splitting keeps a
+    Saber request (a ~0.3 ms chain) from waiting for the Frodo requests admitted with it
+    (a ~4 ms chain: a 348-permutation prologue sponge, then a 976-row product per CTA)."""
+
     def __init__(self, device: int = 0, slots: int = 4, max_batch: int = 4096, form: int = K.FORM_TC,
-                 hbm_budget: int = 1 << 30):
+                 hbm_budget: int = 1 << 30, classes=None, saber_share: float = 0.25):
         self.slots = [K.Engine(device, hbm_budget=hbm_budget) for _ in range(slots)]
         self.streams = [torch.cuda.Stream(device) for _ in range(slots)]
+        self.classes = list(classes) if classes is not None else [None] * slots
+        if len(self.classes) != slots:
+            raise ValueError("one class per slot")
+        if classes is not None:
+            # Each launch is a persistent kernel that holds its CTAs until its queue drains, so
+            # the classes split the GPU's resident CTAs (two per SM): saber_share of them for
+            # the Saber slots, the rest for the Frodo slots, each class's share divided among
+            # its slots.  A Saber launch then never waits for a Frodo launch's CTAs.
+            total = 2 * torch.cuda.get_device_properties(device).multi_processor_count
+            n_s = self.classes.count(SABER_CLASS)
+            n_f = self.classes.count(FRODO_CLASS)
+            saber_ctas = max(n_s, int(round(total * saber_share))) if n_s else 0
+            for k, c in enumerate(self.classes):
+                share = saber_ctas // n_s if c == SABER_CLASS else (total - saber_ctas) // max(1, n_f)
+                self.slots[k].set_max_ctas(max(1, share))
         self.max_batch = max_batch
         self.form = form
         self.lib = K.load()
+        # size every slot's arena for a full batch of the largest requests now: growing it
+        # later would wait for the whole device (all slots) in the middle of serving
+        need = int(self.lib.dpkem_mixed_bytes(K.FRODO976, max_batch))
+        for e in self.slots:
+            e.reserve(min(need, hbm_budget))
 
     def close(self):
         for e in self.slots:
@@ -109,45 +138,61 @@ class Server:
     def run(self, pool: RequestPool, arrivals: np.ndarray) -> dict:
         """Serve pool requests 0..len(arrivals)-1 arriving at the given times (seconds)."""
         n = len(arrivals)
+        req_class = np.where(pool.kind[:n] // 3 >= 2, SABER_CLASS, FRODO_CLASS)
+        keys = sorted({c for c in self.classes}, key=lambda c: -1 if c is None else c)
+        queues = {c: (np.arange(n) if c is None else np.nonzero(req_class == c)[0]) for c in keys}
+        q_arr = {c: arrivals[q] for c, q in queues.items()}
+        q_next = {c: 0 for c in keys}
         done_ms = np.full(n, np.nan)
-        busy = [None] * len(self.slots)  # (event, first, last)
+        busy = [None] * len(self.slots)  # (event, request indices)
         t_origin = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         t_origin.record(self.streams[0])
         torch.cuda.synchronize()
         host0 = time.perf_counter()
-        nxt = 0
-        batches = []
+        batches, submit_s = [], []
         prev, max_gap = 0.0, 0.0  # longest pause of this loop: a host stall, not device time
-        while nxt < n or any(b is not None for b in busy):
+        while any(q_next[c] < len(queues[c]) for c in keys) or any(b is not None for b in busy):
             now = time.perf_counter() - host0
             max_gap, prev = max(max_gap, now - prev), now
             for k, b in enumerate(busy):
                 if b is not None and b[0].query():
-                    done_ms[b[1]:b[2]] = t_origin.elapsed_time(b[0])
+                    done_ms[b[1]] = t_origin.elapsed_time(b[0])
                     busy[k] = None
-            arrived = int(np.searchsorted(arrivals, now, side="right"))
-            free = [k for k, b in enumerate(busy) if b is None]
-            if nxt < arrived and free:
-                last = min(arrived, nxt + self.max_batch)
-                k = free[0]
-                busy[k] = (self._submit(k, pool.table[nxt:last]), nxt, last)
-                batches.append(last - nxt)
-                nxt = last
+            submitted = False
+            for c in keys:
+                arrived = int(np.searchsorted(q_arr[c], now, side="right"))
+                if q_next[c] >= arrived:
+                    continue
+                free = [k for k, b in enumerate(busy) if b is None and self.classes[k] == c]
+                if not free:
+                    continue
+                last = min(arrived, q_next[c] + self.max_batch)
+                idx = queues[c][q_next[c]:last]
+                t_sub = time.perf_counter()
+                busy[free[0]] = (self._submit(free[0], np.ascontiguousarray(pool.table[idx])), idx)
+                submit_s.append(time.perf_counter() - t_sub)
+                batches.append(len(idx))
+                q_next[c] = last
+                submitted = True
+            if submitted:
                 continue
-            if nxt < n and not free:
-                time.sleep(20e-6)
-            elif nxt < n and arrived == nxt:
-                time.sleep(min(max(arrivals[nxt] - now, 0.0), 200e-6))
-            else:
-                time.sleep(20e-6)
+            waits = [q_arr[c][q_next[c]] - now for c in keys if q_next[c] < len(queues[c])]
+            time.sleep(min(max(min(waits), 0.0), 200e-6) if waits and min(waits) > 0 else 20e-6)
         for e in self.slots:
             e.sync()
         lat = done_ms - arrivals * 1e3
         span = (np.nanmax(done_ms) - arrivals[0] * 1e3) * 1e-3
-        return {"requests": n, "ops_per_s": n / span, "p50_ms": float(np.nanpercentile(lat, 50)),
-                "p99_ms": float(np.nanpercentile(lat, 99)), "mean_batch": float(np.mean(batches)),
-                "batches": len(batches), "host_max_gap_ms": max_gap * 1e3, "latency_ms": lat}
+        out = {"requests": n, "ops_per_s": n / span, "p50_ms": float(np.nanpercentile(lat, 50)),
+               "p99_ms": float(np.nanpercentile(lat, 99)), "mean_batch": float(np.mean(batches)),
+               "batches": len(batches), "host_max_gap_ms": max_gap * 1e3, "latency_ms": lat,
+               "submit_ms_max": max(submit_s) * 1e3, "submit_ms_mean": float(np.mean(submit_s)) * 1e3}
+        for c, name in ((FRODO_CLASS, "frodo"), (SABER_CLASS, "saber")):
+            m = req_class == c
+            if m.any():
+                out[name + "_p50_ms"] = float(np.nanpercentile(lat[m], 50))
+                out[name + "_p99_ms"] = float(np.nanpercentile(lat[m], 99))
+        return out
 
 
 def poisson_arrivals(n: int, rate: float, seed: int = 0) -> np.ndarray:

@@ -62,6 +62,17 @@ typedef struct dpkem_ctx dpkem_ctx;
  * (0 = default 8 GiB).  Batches larger than the budget allows run in chunks. */
 int dpkem_ctx_create(dpkem_ctx **out, int device, size_t hbm_budget_bytes);
 int dpkem_ctx_destroy(dpkem_ctx *ctx);
+/* Cap the CTAs of this context's persistent launches (mixed batches, graphs, frames):
+ * 0 (default) = two per SM, the whole GPU.  A server that runs several contexts at once
+ * gives each a share, so a launch never queues behind another one's resident CTAs. */
+int dpkem_ctx_set_max_ctas(dpkem_ctx *ctx, int max_ctas);
+
+/* Grow the context's device arena to at least `bytes` now (within its HBM budget), so
+ * that no later call has to: regrowing frees the old arena, which waits for the whole
+ * device.  dpkem_mixed_bytes(scheme, n) is the arena a mixed batch of n requests of that
+ * scheme needs (Frodo requests need the most); 0 for an unknown scheme. */
+int dpkem_ctx_reserve(dpkem_ctx *ctx, size_t bytes);
+size_t dpkem_mixed_bytes(int scheme, size_t n);
 
 /* Object sizes in bytes; any pointer may be NULL. */
 int dpkem_sizes(int scheme, size_t *pk, size_t *sk, size_t *ct, size_t *ss, size_t *kp_coins, size_t *enc_coins);

@@ -21,3 +21,21 @@ def test_serving_results_equal_alone(engine, form):
     torch.cuda.synchronize()
     assert pool.check()
     assert res["batches"] > 1 and np.isfinite(res["latency_ms"]).all() and (res["latency_ms"] > 0).all()
+
+
+def test_serving_split_classes(engine):
+    """Frodo and Saber requests on separate slots: results unchanged, Saber requests no
+    longer wait for Frodo batches."""
+    from dpcrypto_b200.serving import FRODO_CLASS, SABER_CLASS
+
+    pool = RequestPool(engine, 600, seed=4)
+    srv = Server(slots=4, max_batch=128, form=d.FORM_TC, hbm_budget=256 << 20,
+                 classes=[FRODO_CLASS, FRODO_CLASS, SABER_CLASS, SABER_CLASS])
+    try:
+        res = srv.run(pool, poisson_arrivals(pool.n, rate=20000.0, seed=2))
+    finally:
+        srv.close()
+    torch.cuda.synchronize()
+    assert pool.check()
+    assert np.isfinite(res["latency_ms"]).all()
+    assert res["saber_p50_ms"] < res["frodo_p50_ms"]
