@@ -39,6 +39,12 @@ def main(argv=None) -> int:
     engines = [K.Engine(a.device, hbm_budget=int(a.budget_gib * (1 << 30) / a.inflight)) for _ in range(a.inflight)]
     handles = (ctypes.c_void_p * len(engines))(*[e._h for e in engines])
     lib = K.load()
+    # size the arenas for a full batch of the largest frames now (Frodo decaps requests,
+    # Frodo keypair responses, Frodo records): growing one later waits for the whole GPU
+    worst = int(lib.dpkem_mixed_bytes(K.FRODO976, a.max_frames)) + a.max_frames * (
+        F.frame_bytes(K.FRODO976, 2)[0] + F.frame_bytes(K.FRODO976, 0)[1])
+    for e in engines:
+        e.reserve(min(worst, int(a.budget_gib * (1 << 30) / a.inflight)))
     rc = lib.dpkem_host_register(ring.base, ring.size)
     if rc != K.OK:
         print(f"frame_server: host_register failed: {lib.dpkem_strerror(rc).decode()}", file=sys.stderr)
