@@ -374,6 +374,27 @@ size_t dpkem_mixed_bytes(int scheme, size_t n) {
   return mixed::plan_bytes(rq.data(), n, nullptr);
 }
 
+int dpkem_selftest_timeout(dpkem_ctx *c, int which) {
+  if (!c || (which != 0 && which != 1)) return set_status(DPKEM_EINVAL);
+  std::lock_guard<std::mutex> lock(c->mu);
+  if (cudaSetDevice(c->device) != cudaSuccess) return set_status(cuda_status(cudaErrorInvalidDevice));
+  int rc = ensure_arena(c, 16 << 10);
+  if (rc) return set_status(rc);
+  cudaStream_t st = c->stream;
+  cudaError_t e = cudaStreamWaitEvent(st, c->last, 0);
+  if (e == cudaSuccess) e = mixed::selftest_timeout(which, c->arena, c->arena_bytes, c->d_err, st);
+  if (e == cudaSuccess) e = cudaEventRecord(c->last, st);
+  uint32_t err = 0;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaMemcpy(&err, c->d_err, 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_status(cuda_status(e));
+  if (err) {
+    cudaMemset(c->d_err, 0, 4);
+    return set_status(DPKEM_ETIMEOUT);
+  }
+  return set_status(DPKEM_OK);
+}
+
 int dpkem_ctx_set_max_ctas(dpkem_ctx *c, int max_ctas) {
   if (!c || max_ctas < 0) return set_status(DPKEM_EINVAL);
   std::lock_guard<std::mutex> lock(c->mu);

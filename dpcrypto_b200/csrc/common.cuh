@@ -128,6 +128,9 @@ cudaError_t plan_launch(const void *plan, size_t n, int grid, cudaStream_t st);
 cudaError_t frame_headers_launch(const void *plan, size_t n, const uint32_t *resp_bytes, const uint32_t *payload_end,
                                  cudaStream_t st);
 int slots_for_device();
+// Diagnostics: a kernel whose bounded wait cannot be satisfied (0: an mbarrier nothing
+// arrives on; 1: a persistent-kernel dependency nothing completes; needs 16 KB of arena).
+cudaError_t selftest_timeout(int which, uint8_t *arena, size_t arena_bytes, uint32_t *err, cudaStream_t st);
 }  // namespace mixed
 
 }  // namespace dpkem

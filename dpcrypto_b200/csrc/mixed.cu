@@ -157,17 +157,20 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
   return v;
 }
 
-__device__ __forceinline__ void wait_done(const Plan &p, uint32_t r, uint32_t need) {
-  if (ld_acquire(p.done + r) >= need) return;
+// true when request r has completed `need` stage roles; false on expiry (the error word is
+// set) or when an error is already recorded, in which case the caller skips its stage.
+__device__ __forceinline__ bool wait_done(const Plan &p, uint32_t r, uint32_t need) {
+  if (ld_acquire(p.done + r) >= need) return true;
   const uint64_t t0 = globaltimer_ns();
   while (ld_acquire(p.done + r) < need) {
-    if (ld_acquire(p.err) != 0) return;
+    if (ld_acquire(p.err) != 0) return false;
     __nanosleep(200);
     if (globaltimer_ns() - t0 > kDepLimitNs) {
       atomicOr(p.err, DEV_ERR_TIMEOUT);
-      return;
+      return false;
     }
   }
+  return true;
 }
 
 __device__ __forceinline__ void mark_done(const Plan &p, uint32_t r) {
@@ -291,7 +294,7 @@ static_assert(kSmem == fdev::TcLayout<kTcStages>::total, "the AES stages must no
 
 __global__ void __launch_bounds__(256, 2) mixed_kernel(Plan p) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint32_t s_task, s_tmem;
+  __shared__ uint32_t s_task, s_tmem, s_ready;
   const int tid = threadIdx.x;
   if (tid < 32) {
     tmem_alloc(&s_tmem, fdev::TC_TMEM_COLS);
@@ -313,9 +316,9 @@ __global__ void __launch_bounds__(256, 2) mixed_kernel(Plan p) {
     const uint32_t need = threshold(scheme, op, stage);
     if (kind == K_CTA) {
       const uint32_t r = p.idx[tk.first];
-      if (tid == 0) wait_done(p, r, need);
+      if (tid == 0) s_ready = wait_done(p, r, need) ? 1u : 0u;
       __syncthreads();
-      cta_stage(code, p.req[r], smem, tbase, p.err);
+      if (s_ready) cta_stage(code, p.req[r], smem, tbase, p.err);  // skipped after an error: the batch drains
       __syncthreads();
       if (tid == 0) mark_done(p, r);
     } else {
@@ -323,8 +326,7 @@ __global__ void __launch_bounds__(256, 2) mixed_kernel(Plan p) {
       const int slot = tid % per, role = tid / per;
       if (slot < tk.count) {
         const uint32_t r = p.idx[tk.first + slot];
-        wait_done(p, r, need);
-        thread_stage(p, code, p.req[r], role);
+        if (wait_done(p, r, need)) thread_stage(p, code, p.req[r], role);
         mark_done(p, r);
       }
     }
@@ -588,6 +590,46 @@ cudaError_t frame_headers_launch(const void *plan, size_t n, const uint32_t *res
     fs.payload_end[k] = payload_end[k];
   }
   frame_headers_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p.req, (uint32_t)n, fs);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- diagnostics
+// Kernels whose bounded wait cannot be satisfied, to exercise the expiry path end to end.
+__global__ void mbar_timeout_kernel(uint32_t *err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);  // one arrival expected, none ever made
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0)) atomicOr(err, DEV_ERR_TIMEOUT);
+}
+
+cudaError_t selftest_timeout(int which, uint8_t *arena, size_t arena_bytes, uint32_t *err, cudaStream_t st) {
+  if (which == 0) {
+    mbar_timeout_kernel<<<1, 32, 0, st>>>(err);
+    return cudaGetLastError();
+  }
+  // One Saber l=3 encapsulation product task whose prologue never ran: its dependency
+  // counter stays 0, the wait expires, the stage is skipped and the kernel exits.
+  constexpr size_t kReq = 0, kTask = 256, kIdx = 512, kDone = 768, kHead = 1024, kRec = 2048;
+  const size_t kBuf = kRec + ((saber_rec_bytes(3) + 255) & ~(size_t)255);
+  if (arena_bytes < kBuf + 4096) return cudaErrorInvalidValue;
+  DevReq rq{3, OP_ENC, arena + kBuf, arena + kBuf + 1024, arena + kBuf + 2048, arena + kBuf + 3328,
+            arena + kRec, 0, 0u, 0u};
+  const Task tk{(uint16_t)code_of(3, OP_ENC, 1, FORM_DP4A), 1, 0};
+  std::vector<uint8_t> host(kRec, 0);
+  std::memcpy(host.data() + kReq, &rq, sizeof rq);
+  std::memcpy(host.data() + kTask, &tk, sizeof tk);
+  cudaError_t e = cudaMemcpyAsync(arena, host.data(), host.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // pageable source
+  int grid = 0;
+  if (e == cudaSuccess) e = kernel_setup(&grid);
+  if (e != cudaSuccess) return e;
+  const Plan p{reinterpret_cast<const DevReq *>(arena + kReq), reinterpret_cast<const Task *>(arena + kTask),
+               reinterpret_cast<const uint32_t *>(arena + kIdx), 1u, reinterpret_cast<uint32_t *>(arena + kHead),
+               reinterpret_cast<uint32_t *>(arena + kDone), err, default_coin_key()};
+  mixed_kernel<<<1, 256, kSmem, st>>>(p);
   return cudaGetLastError();
 }
 

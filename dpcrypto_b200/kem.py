@@ -40,6 +40,7 @@ EXPORTS = {
     "dpkem_ctx_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "dpkem_ctx_set_max_ctas": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "dpkem_ctx_reserve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t]),
+    "dpkem_selftest_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "dpkem_mixed_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_size_t]),
     "dpkem_sizes": (ctypes.c_int, [ctypes.c_int] + [ctypes.POINTER(ctypes.c_size_t)] * 6),
     "dpkem_max_chunk": (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int]),

@@ -72,6 +72,13 @@ int dpkem_ctx_set_max_ctas(dpkem_ctx *ctx, int max_ctas);
  * device.  dpkem_mixed_bytes(scheme, n) is the arena a mixed batch of n requests of that
  * scheme needs (Frodo requests need the most); 0 for an unknown scheme. */
 int dpkem_ctx_reserve(dpkem_ctx *ctx, size_t bytes);
+
+/* Diagnostics for the failure path: runs a kernel whose bounded device wait cannot be
+ * satisfied (which = 0: an mbarrier that no thread arrives on, the tensor stages' wait;
+ * 1: a persistent-kernel task whose dependency never completes, the mixed batches' wait)
+ * and returns what a real expiry returns, DPKEM_ETIMEOUT, after the 2 s limit.  Nothing
+ * traps; the context stays usable. */
+int dpkem_selftest_timeout(dpkem_ctx *ctx, int which);
 size_t dpkem_mixed_bytes(int scheme, size_t n);
 
 /* Object sizes in bytes; any pointer may be NULL. */

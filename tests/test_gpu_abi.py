@@ -109,3 +109,27 @@ def test_host_pipeline_matches_device_mode(engine, oracle, scheme, n):
     assert (dpk.cpu().numpy() == pk).all() and (dsk.cpu().numpy() == sk).all()
     assert (dct.cpu().numpy() == ct).all() and (dss.cpu().numpy() == ss).all()
     assert (ss2 == ss).all()
+
+
+@pytest.mark.parametrize("which", [0, 1])
+def test_bounded_wait_expiry(engine, oracle, which):
+    """A device wait that nothing can satisfy expires after its limit and comes back as
+    DPKEM_ETIMEOUT (no trap, no hang); the context keeps working afterwards."""
+    assert engine._lib.dpkem_selftest_timeout(engine._h, which) == d.kem.ETIMEOUT
+    kc, ec = oracle.coins(3, 96, "kp", first=9), oracle.coins(3, 32, "enc", first=9)
+    pk, sk = engine.keypair(d.SABER, kc, d.FORM_TC)
+    pk_o, sk_o = oracle.keypair(3, kc)
+    assert (pk == pk_o).all() and (sk == sk_o).all()
+    z = d.sizes(d.SABER)
+    items, outs = [], []
+    for i in range(3):
+        oct_ = torch.empty(z["ct"], dtype=torch.uint8, device="cuda")
+        oss = torch.empty(z["ss"], dtype=torch.uint8, device="cuda")
+        items.append((d.SABER, 1, torch.from_numpy(ec[i].copy()).cuda(), torch.from_numpy(pk[i].copy()).cuda(),
+                      oct_, oss))
+        outs.append((oct_, oss))
+    engine.mixed(items, d.FORM_TC)
+    engine.sync()
+    ct_o, ss_o = oracle.enc(3, pk_o, ec)
+    for i, (c, s) in enumerate(outs):
+        assert (c.cpu().numpy() == ct_o[i]).all() and (s.cpu().numpy() == ss_o[i]).all()
