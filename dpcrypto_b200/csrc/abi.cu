@@ -106,6 +106,24 @@ cudaError_t persistent_grid(const dpkem_ctx *c, int *grid) {
   return e;
 }
 
+uint8_t *stage_for(dpkem_ctx *c, int j, size_t bytes) {
+  if (c->stage_ev[j]) cudaEventSynchronize(c->stage_ev[j]);  // its previous upload has been read
+  if (c->h_stage_bytes[j] < bytes) {
+    if (c->h_stage[j]) cudaFreeHost(c->h_stage[j]);
+    const size_t want = std::max({bytes, c->h_stage_bytes[j] + c->h_stage_bytes[j] / 2, (size_t)1 << 20});
+    if (cudaHostAlloc(&c->h_stage[j], want, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      c->h_stage[j] = nullptr;
+      c->h_stage_bytes[j] = 0;
+      return nullptr;
+    }
+    c->h_stage_bytes[j] = want;
+  }
+  return c->h_stage[j];
+}
+
+void stage_used(dpkem_ctx *c, int j, cudaStream_t st) { cudaEventRecord(c->stage_ev[j], st); }
+
 }  // namespace abi
 }  // namespace dpkem
 
@@ -348,6 +366,7 @@ int dpkem_ctx_create(dpkem_ctx **out, int device, size_t hbm_budget_bytes) {
     cudaDeviceGetStreamPriorityRange(&least, &greatest);
     const int prio = greatest + (least - greatest) * j / (kPipeChunks - 1);
     cudaStreamCreateWithPriority(&c->ppipe[j], cudaStreamNonBlocking, prio);
+    cudaEventCreateWithFlags(&c->stage_ev[j], cudaEventDisableTiming);
   }
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->last, cudaEventDisableTiming) != cudaSuccess ||
@@ -419,6 +438,11 @@ int dpkem_ctx_destroy(dpkem_ctx *c) {
       cudaStreamSynchronize(c->ppipe[j]);
       cudaStreamDestroy(c->ppipe[j]);
     }
+    if (c->stage_ev[j]) {
+      cudaEventSynchronize(c->stage_ev[j]);
+      cudaEventDestroy(c->stage_ev[j]);
+    }
+    if (c->h_stage[j]) cudaFreeHost(c->h_stage[j]);
     if (c->pev[j]) cudaEventDestroy(c->pev[j]);
   }
   for (int k = 0; k <= StageTimer::kMax; k++)
@@ -510,8 +534,12 @@ static int mixed_batch(dpkem_ctx *c, int form, size_t n, const dpkem_request *re
   int grid = 0;
   if (e == cudaSuccess) e = persistent_grid(c, &grid);
   std::vector<uint8_t> plan(mixed::plan_struct_bytes());
+  const size_t tb = mixed::plan_table_bytes(mr, n);
+  uint8_t *stage = e == cudaSuccess ? stage_for(c, 0, tb) : nullptr;
   if (e == cudaSuccess)
-    e = mixed::plan_build(mr, n, form, grid, c->arena, c->arena_bytes, c->d_err, st, plan.data(), key, first);
+    e = mixed::plan_build(mr, n, form, grid, c->arena, c->arena_bytes, c->d_err, st, plan.data(), key, first, stage,
+                          stage ? c->h_stage_bytes[0] : 0);
+  if (e == cudaSuccess && stage) stage_used(c, 0, st);
   if (e == cudaSuccess) e = mixed::plan_launch(plan.data(), n, grid, st);
   if (e == cudaSuccess) e = cudaEventRecord(c->last, st);
   return set_status(cuda_status(e));

@@ -117,9 +117,14 @@ size_t plan_bytes(const Req *reqs, size_t n, size_t *ntasks_out);
 size_t plan_struct_bytes();
 // coin_key (32 bytes, may be null): keypair / encaps requests with in0 == null draw their
 // coins on the device, SHAKE256(coin_key || LE64(coin_first + i) || "kp" / "enc").
+// The request / task / index tables are written to `stage` (pinned host memory, at least
+// plan_table_bytes) and uploaded with one asynchronous copy, the caller keeping `stage`
+// untouched until that copy has run; without a stage they go through a pageable buffer
+// and the call waits for the copy.
 cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *arena, size_t arena_bytes,
                        uint32_t *err, cudaStream_t st, void *plan_out, const uint8_t *coin_key = nullptr,
-                       uint64_t coin_first = 0);
+                       uint64_t coin_first = 0, uint8_t *stage = nullptr, size_t stage_bytes = 0);
+size_t plan_table_bytes(const Req *reqs, size_t n);
 cudaError_t kernel_setup(int *grid);
 cudaError_t plan_launch(const void *plan, size_t n, int grid, cudaStream_t st);
 // Writes the wire-format response header before each request's first output (the request

@@ -21,6 +21,9 @@ struct dpkem_ctx {
   size_t arena_bytes = 0;
   uint32_t *d_err = nullptr;
   int max_ctas = 0;  // persistent launches use at most this many CTAs (0: two per SM)
+  uint8_t *h_stage[8] = {};      // pinned plan-table images, one per pipeline slot
+  size_t h_stage_bytes[8] = {};
+  cudaEvent_t stage_ev[8] = {};  // recorded after each stage's last upload
   bool profile = false;
   dpkem::StageTimer timer;
   int timer_stages = 0;
@@ -45,6 +48,11 @@ int ensure_arena(dpkem_ctx *c, size_t bytes);  // grows the context's device are
 int cuda_status(cudaError_t e);             // DPKEM_OK or DPKEM_ECUDA (clears the error)
 // Grid of this context's persistent launches: the device's resident CTAs, capped by max_ctas.
 cudaError_t persistent_grid(const dpkem_ctx *c, int *grid);
+// Pinned stage j of at least `bytes`, once its previous upload has run (nullptr if it
+// cannot be allocated: the caller then uploads synchronously); stage_used records the
+// upload just enqueued on st.
+uint8_t *stage_for(dpkem_ctx *c, int j, size_t bytes);
+void stage_used(dpkem_ctx *c, int j, cudaStream_t st);
 
 }  // namespace abi
 }  // namespace dpkem

@@ -213,10 +213,13 @@ int frames_submit(dpkem_ctx *c, int form, const uint8_t *req, size_t req_bytes, 
     uint8_t *d_resp = d_req + up(g.req_len);
     uint8_t *d_plan = d_resp + up(g.resp_len);
     const std::vector<mixed::Req> rq = group_reqs(fr, g, d_req, d_resp);
+    const int sj_idx = (int)(k % npipe);
+    uint8_t *stage = stage_for(c, sj_idx, mixed::plan_table_bytes(rq.data(), rq.size()));
     e = cudaMemcpyAsync(d_req, req + g.req_start, g.req_len, cudaMemcpyHostToDevice, sj);
     if (e == cudaSuccess)
       e = mixed::plan_build(rq.data(), rq.size(), form, grid, d_plan, region - (size_t)(d_plan - d_req), c->d_err, sj,
-                            plans[k].data());
+                            plans[k].data(), nullptr, 0, stage, stage ? c->h_stage_bytes[sj_idx] : 0);
+    if (e == cudaSuccess && stage) stage_used(c, sj_idx, sj);
     if (e == cudaSuccess) e = mixed::plan_launch(plans[k].data(), rq.size(), grid, sj);
     if (e == cudaSuccess) e = mixed::frame_headers_launch(plans[k].data(), rq.size(), rtab, rend, sj);
     if (e == cudaSuccess) e = cudaMemcpyAsync(resp + g.resp_start, d_resp, g.resp_len, cudaMemcpyDeviceToHost, sj);

@@ -355,11 +355,13 @@ double est_us(int scheme, int op, int stage, int count) {
   return 120.0;
 }
 
+// Tasks of one stage are created in instance order, so a task's dependencies (the previous
+// stage's tasks covering its instances) and its dependents are contiguous id ranges.
 struct HostTask {
   Task t;
-  double dur, ready = 0;
-  int pending = 0;
-  std::vector<int> dependents;
+  double dur, ready;
+  int pending;       // dependencies not yet scheduled
+  int dn_lo, dn_hi;  // dependents [dn_lo, dn_hi]; empty when dn_lo > dn_hi
   int prio;
 };
 
@@ -398,26 +400,45 @@ size_t plan_bytes(const Req *reqs, size_t n, size_t *ntasks_out) {
 }
 
 // Builds the plan in host memory, uploads it into `arena` and returns the launch descriptor.
+size_t plan_table_bytes(const Req *reqs, size_t n) {
+  size_t ntasks = 0;
+  plan_bytes(reqs, n, &ntasks);
+  size_t nidx = 0;
+  for (size_t i = 0; i < n; i++) nidx += nstages(reqs[i].scheme, reqs[i].op);
+  auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  return up(n * sizeof(DevReq)) + up(ntasks * sizeof(Task)) + nidx * 4;
+}
+
 cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *arena, size_t arena_bytes,
-                       uint32_t *err, cudaStream_t st, void *plan_out, const uint8_t *coin_key, uint64_t coin_first) {
+                       uint32_t *err, cudaStream_t st, void *plan_out, const uint8_t *coin_key, uint64_t coin_first,
+                       uint8_t *stage, size_t stage_bytes) {
   size_t ntasks = 0;
   const size_t need = plan_bytes(reqs, n, &ntasks);
   if (need > arena_bytes) return cudaErrorMemoryAllocation;
   auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
-  uint8_t *d_req = arena;
-  uint8_t *d_tasks = d_req + up(n * sizeof(DevReq));
-  uint8_t *d_idx = d_tasks + up(ntasks * sizeof(Task));
-  // idx size = sum over groups and stages of c
-  size_t nidx = 0;
   std::vector<std::vector<uint32_t>> groups(5 * 3);
   for (size_t i = 0; i < n; i++) groups[reqs[i].scheme * 3 + reqs[i].op].push_back((uint32_t)i);
+  size_t nidx = 0;
   for (int g = 0; g < 15; g++)
     if (!groups[g].empty()) nidx += groups[g].size() * nstages(g / 3, g % 3);
+  // Host image of the device tables [requests | tasks | idx], uploaded in one copy.
+  const size_t o_tasks = up(n * sizeof(DevReq)), o_idx = o_tasks + up(ntasks * sizeof(Task));
+  const size_t table = o_idx + nidx * 4;
+  std::vector<uint8_t> own;
+  uint8_t *img = stage;
+  const bool pinned = stage && stage_bytes >= table;
+  if (!pinned) {
+    own.resize(table);
+    img = own.data();
+  }
+  DevReq *hreq = reinterpret_cast<DevReq *>(img);
+  Task *order = reinterpret_cast<Task *>(img + o_tasks);
+  uint32_t *idx = reinterpret_cast<uint32_t *>(img + o_idx);
+  uint8_t *d_req = arena, *d_tasks = arena + o_tasks, *d_idx = arena + o_idx;
   uint8_t *d_done = d_idx + up(nidx * 4);
   uint8_t *d_head = d_done + up(n * 4);
   uint8_t *d_scr = d_head + 256;
 
-  std::vector<DevReq> hreq(n);
   size_t off = 0;
   for (size_t i = 0; i < n; i++) {
     const Req &r = reqs[i];
@@ -429,40 +450,38 @@ cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *
     }
     off += r.scheme <= 1 ? kFrodoRec : saber_rec_bytes(r.scheme);
   }
-  // Tasks per group and stage, with dependencies on the previous stage's tasks.
+  // Tasks per group and stage; dependencies on the previous stage's tasks are id ranges.
   std::vector<HostTask> ht;
-  std::vector<uint32_t> idx;
-  idx.reserve(nidx);
+  ht.reserve(ntasks);
+  size_t nid = 0;
+  std::vector<int> owner_prev, owner;
   for (int g = 0; g < 15; g++) {
     const std::vector<uint32_t> &R = groups[g];
     if (R.empty()) continue;
     const int scheme = g / 3, op = g % 3;
-    std::vector<int> owner_prev(R.size(), -1);  // task index of each instance's previous stage
+    owner_prev.assign(R.size(), -1);
+    owner.assign(R.size(), -1);
     for (int stg = 0; stg < nstages(scheme, op); stg++) {
       const int kind = kind_of(scheme, op, stg);
       const int per = kind == K_CTA ? 1 : task_size(scheme, kind);
-      const uint32_t base = (uint32_t)idx.size();
-      idx.insert(idx.end(), R.begin(), R.end());
-      std::vector<int> owner(R.size());
+      const uint32_t base = (uint32_t)nid;
+      std::memcpy(idx + nid, R.data(), R.size() * 4);
+      nid += R.size();
       for (size_t a = 0; a < R.size(); a += per) {
         const int cnt = (int)std::min<size_t>(per, R.size() - a);
-        HostTask t;
-        t.t = Task{(uint16_t)code_of(scheme, op, stg, form), (uint16_t)cnt, base + (uint32_t)a};
-        t.dur = est_us(scheme, op, stg, cnt);
-        t.prio = kind == K_CTA ? (t.dur > 500 ? 2 : 1) : 0;  // latency-bound thread stages first
         const int id = (int)ht.size();
-        std::vector<int> deps;
-        for (int k = 0; k < cnt; k++) {
-          owner[a + k] = id;
-          if (owner_prev[a + k] >= 0) deps.push_back(owner_prev[a + k]);
+        const int lo = owner_prev[a], hi = owner_prev[a + cnt - 1];
+        const double dur = est_us(scheme, op, stg, cnt);
+        const int prio = kind == K_CTA ? (dur > 500 ? 2 : 1) : 0;  // latency-bound thread stages first
+        ht.push_back(HostTask{Task{(uint16_t)code_of(scheme, op, stg, form), (uint16_t)cnt, base + (uint32_t)a}, dur,
+                              0.0, lo >= 0 ? hi - lo + 1 : 0, INT32_MAX, -1, prio});
+        for (int k = 0; k < cnt; k++) owner[a + k] = id;
+        for (int d = lo; lo >= 0 && d <= hi; d++) {
+          ht[d].dn_lo = std::min(ht[d].dn_lo, id);
+          ht[d].dn_hi = std::max(ht[d].dn_hi, id);
         }
-        std::sort(deps.begin(), deps.end());
-        deps.erase(std::unique(deps.begin(), deps.end()), deps.end());
-        t.pending = (int)deps.size();
-        ht.push_back(t);
-        for (int d : deps) ht[d].dependents.push_back(id);
       }
-      owner_prev = owner;
+      std::swap(owner_prev, owner);
     }
   }
   // List scheduling on `slots` CTA slots: the fetch order is the simulated start order.
@@ -477,14 +496,21 @@ cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *
     int prio, id;
     bool operator>(const ByPrio &o) const { return prio != o.prio ? prio > o.prio : id > o.id; }
   };
-  std::priority_queue<ByReady, std::vector<ByReady>, std::greater<ByReady>> waiting;
-  std::priority_queue<ByPrio, std::vector<ByPrio>, std::greater<ByPrio>> ready;
-  std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
+  std::vector<ByReady> wv;
+  std::vector<ByPrio> rv;
+  std::vector<double> fv;
+  wv.reserve(ht.size());
+  rv.reserve(ht.size());
+  fv.reserve(std::max(1, slots));
+  std::priority_queue<ByReady, std::vector<ByReady>, std::greater<ByReady>> waiting(std::greater<ByReady>(),
+                                                                                   std::move(wv));
+  std::priority_queue<ByPrio, std::vector<ByPrio>, std::greater<ByPrio>> ready(std::greater<ByPrio>(), std::move(rv));
+  std::priority_queue<double, std::vector<double>, std::greater<double>> free_at(std::greater<double>(),
+                                                                                 std::move(fv));
   for (int s = 0; s < std::max(1, slots); s++) free_at.push(0.0);
   for (size_t i = 0; i < ht.size(); i++)
     if (ht[i].pending == 0) waiting.push({0.0, (int)i});
-  std::vector<Task> order;
-  order.reserve(ht.size());
+  size_t placed = 0;
   while (!waiting.empty() || !ready.empty()) {
     const double w = free_at.top();
     free_at.pop();
@@ -502,20 +528,19 @@ cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *
     }
     const double start = std::max(w, ht[id].ready), fin = start + ht[id].dur;
     free_at.push(fin);
-    order.push_back(ht[id].t);
-    for (int d : ht[id].dependents) {
+    order[placed++] = ht[id].t;
+    for (int d = ht[id].dn_lo; d <= ht[id].dn_hi; d++) {
       ht[d].ready = std::max(ht[d].ready, fin);
       if (--ht[d].pending == 0) waiting.push({ht[d].ready, d});
     }
   }
-  if (order.size() != ntasks) return cudaErrorInvalidValue;
-  cudaError_t e;
-  if ((e = cudaMemcpyAsync(d_req, hreq.data(), n * sizeof(DevReq), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
-  if ((e = cudaMemcpyAsync(d_tasks, order.data(), ntasks * sizeof(Task), cudaMemcpyHostToDevice, st)) != cudaSuccess)
-    return e;
-  if ((e = cudaMemcpyAsync(d_idx, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
-  // Pageable sources: make sure the copies have consumed them before the vectors go away.
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  if (placed != ntasks) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemcpyAsync(d_req, img, table, cudaMemcpyHostToDevice, st);
+  // A pageable image must be consumed before the vector goes away; a pinned stage is the
+  // caller's to keep until the copy has run.
+  if (e == cudaSuccess && !pinned) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return e;
+  (void)d_tasks;
   Plan *p = static_cast<Plan *>(plan_out);
   *p = Plan{reinterpret_cast<const DevReq *>(d_req), reinterpret_cast<const Task *>(d_tasks),
             reinterpret_cast<const uint32_t *>(d_idx), (uint32_t)ntasks, reinterpret_cast<uint32_t *>(d_head),
