@@ -1,4 +1,5 @@
-// FrodoKEM-976-SHAKE device routines, written per instance so that the batched kernels
+// FrodoKEM-976 device routines (SHAKE and AES variants: they differ only in the A-row
+// generator, see ShakeRows / AesRows), written per instance so that the batched kernels
 // (frodo.cu) and the persistent mixed-batch kernel (mixed.cu) run the same code.
 //
 // Stages per operation (all instances independent):
