@@ -84,6 +84,20 @@ def cpu_sample(n_inst: int, threads: int):
     return n_inst / dt, dt
 
 
+def cpu_sample_saber(n_inst: int, threads: int):
+    """Time the oracle's Saber l=3 encaps+decaps on n_inst instances over `threads` host threads."""
+    from oracle import oracle as O
+
+    pk, sk = O.keypair(3, O.coins(n_inst, 96, "kp"), threads=threads)
+    ec = O.coins(n_inst, 32, "enc")
+    t0 = time.perf_counter()
+    ct, ss = O.enc(3, pk, ec, threads=threads)
+    ss2 = O.dec(3, ct, sk, threads=threads)
+    dt = time.perf_counter() - t0
+    assert (ss == ss2).all()
+    return n_inst / dt, dt
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
@@ -358,6 +372,14 @@ def main():
         "stage_ms": stage_ms, "stage_share_of_step": {k: sum(v.values()) / kernel_total for k, v in stage_ms.items()},
         "clocks": clocks,
     }
+    # tensor pipe: the products' algorithmic int8 MACs (two u8 limbs per 16-bit entry of A)
+    # against the measured kind::i8 MMA peak; tiny for Frodo, whose kernel is Keccak-bound
+    i8_peak = eng.probe_i8_mma_peak()
+    frodo_macs = B * FRODO_ROWS * FRODO_ROWS * 8 * 2
+    line["tensor"] = {"i8_mma_peak_macs_per_s": i8_peak, "peak_source": "measured in-process (dpkem_probe_i8_mma_peak)",
+                      "frodo_sa_int8_macs_per_s": frodo_macs / (sa_avg * 1e-3),
+                      "frodo_sa_frac": frodo_macs / (sa_avg * 1e-3) / i8_peak,
+                      "algorithmic": "S'A: 8 x 976 x 976 MACs x 2 limbs per instance"}
     if FS == d.FRODO976AES:  # A from AES-128 T-tables: integer ALU and load/store pipes, no Keccak
         line["roofline"] = {
             "kernel": "sa_tc_kernel<AesRows> (AES-128 A rows -> int8 tcgen05 S'A)" if form == d.FORM_TC
@@ -455,6 +477,10 @@ def main():
         sres["tc_over_dp4a"] = sres["tc"] / sres["dp4a"]
         sres["product_stage_tc_over_dp4a"] = sres["dp4a_product_ms"] / sres["tc_product_ms"]
         sres["tc_over_int32"] = sres["tc"] / sres["int32"]
+        # int8 MACs of the product stages (enc 786,432 + dec 983,040 ring MACs, x 2 limbs)
+        s_macs = SB * (786432 + 983040) * 2
+        sres["tc_product_int8_macs_per_s"] = s_macs / (sres["tc_product_ms"] * 1e-3)
+        sres["tc_product_tensor_frac"] = sres["tc_product_int8_macs_per_s"] / line["tensor"]["i8_mma_peak_macs_per_s"]
         sres["product_stage_tc_over_int32"] = sres["int32_product_ms"] / sres["tc_product_ms"]
         line["saber_l3_batch4096"] = dict(sres, unit=UNIT)
 
@@ -578,8 +604,11 @@ def main():
         n_inst = 24 * threads
         cv, dt = cpu_sample(n_inst, threads)
         cv1, dt1 = cpu_sample(8, 1)
+        sv, sdt = cpu_sample_saber(4096, threads)
         line["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
                                 "value_1core": cv1, "sample_1core": f"8 instances on 1 thread, {dt1:.2f} s wall",
+                                "saber_l3_value": sv, "saber_l3_sample": f"4096 Saber l=3 encaps+decaps on {threads} threads, "
+                                                                        f"{sdt:.2f} s wall",
                                 "sample": f"{n_inst} FrodoKEM-976 encaps+decaps (24 per host thread), "
                                           f"oracle C restatement, {dt:.1f} s wall",
                                 "note": "reported baseline, not the target"}

@@ -701,6 +701,22 @@ int dpkem_probe_int_peaks(dpkem_ctx *c, double *int_ops_per_s, double *keccak_pe
   return set_status(cuda_status(probe_int_peaks(c->stream, int_ops_per_s, keccak_per_s)));
 }
 
+int dpkem_probe_i8_mma_peak(dpkem_ctx *c, double *macs_per_s) {
+  if (!c || !macs_per_s) return set_status(DPKEM_EINVAL);
+  std::lock_guard<std::mutex> lock(c->mu);
+  cudaSetDevice(c->device);
+  cudaError_t e = cudaStreamWaitEvent(c->stream, c->last, 0);
+  if (e == cudaSuccess) e = probe_i8_mma_peak(c->stream, c->d_err, macs_per_s);
+  uint32_t err = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&err, c->d_err, 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_status(cuda_status(e));
+  if (err) {
+    cudaMemset(c->d_err, 0, 4);
+    return set_status(DPKEM_ETIMEOUT);
+  }
+  return set_status(DPKEM_OK);
+}
+
 int dpkem_set_tuning(const char *key, int value) {
   if (!key || value < 0) return set_status(DPKEM_EINVAL);
   Tuning &t = tuning();

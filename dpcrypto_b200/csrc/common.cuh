@@ -106,6 +106,9 @@ cudaError_t saber_dec(const SaberBatch &b, int form, cudaStream_t st);
 size_t saber_scratch_bytes(int level);
 cudaError_t coins_generate(const CoinsBatch &b, cudaStream_t st);
 cudaError_t probe_int_peaks(cudaStream_t st, double *int_ops_per_s, double *keccak_per_s);
+// int8 tcgen05 MMA throughput (MACs/s) of the device; err receives DEV_ERR_TIMEOUT if the
+// probe's bounded wait expires.
+cudaError_t probe_i8_mma_peak(cudaStream_t st, uint32_t *err, double *macs_per_s);
 
 namespace mixed {
 struct Req {

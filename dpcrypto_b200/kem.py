@@ -68,6 +68,7 @@ EXPORTS = {
     "dpkem_profile_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
     "dpkem_probe_int_peaks": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_double)]),
+    "dpkem_probe_i8_mma_peak": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     "dpkem_saber_enc_batch_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_void_p]),
@@ -306,6 +307,12 @@ class Engine:
         if n < 0:
             raise DpkemError(n, "profile_read")
         return [float(buf[k]) for k in range(n)]
+
+    def probe_i8_mma_peak(self) -> float:
+        """int8 tcgen05 MMA multiply-adds per second (one CTA per SM, back-to-back MMAs)."""
+        v = ctypes.c_double()
+        self._check(self._lib.dpkem_probe_i8_mma_peak(self._h, ctypes.byref(v)), "probe_i8_mma_peak")
+        return v.value
 
     def probe_int_peaks(self):
         """(32-bit LOP3/SHF ops per second in Keccak's mix, Keccak-f[1600] per second)."""

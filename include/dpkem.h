@@ -150,6 +150,9 @@ int dpkem_profile_read(dpkem_ctx *ctx, float *stage_ms, int max_stages);
 /* Integer-pipe roofline probes on the context's device: 32-bit LOP3/SHF ops per second
  * in Keccak's instruction mix, and register-resident Keccak-f[1600] permutations per second. */
 int dpkem_probe_int_peaks(dpkem_ctx *ctx, double *int_ops_per_s, double *keccak_per_s);
+/* int8 tensor-core peak of this GPU: one CTA per SM issuing back-to-back 128 x 256 x 32
+ * tcgen05.mma kind::i8 (u8 x s8, s32 accumulators in TMEM); int8 multiply-adds per second. */
+int dpkem_probe_i8_mma_peak(dpkem_ctx *ctx, double *macs_per_s);
 
 /* Saber encapsulation that allocates no device memory (no counterpart in the reference).
  * For callers that may not call cudaMalloc on their request path (allocator calls are

@@ -133,3 +133,10 @@ def test_bounded_wait_expiry(engine, oracle, which):
     ct_o, ss_o = oracle.enc(3, pk_o, ec)
     for i, (c, s) in enumerate(outs):
         assert (c.cpu().numpy() == ct_o[i]).all() and (s.cpu().numpy() == ss_o[i]).all()
+
+
+def test_i8_mma_peak_probe(engine):
+    """The tensor-peak probe runs (valid descriptors, bounded wait) and reports a plausible
+    int8 MAC rate for a B200-class GPU (dense int8 is ~2 P MAC/s)."""
+    macs = engine.probe_i8_mma_peak()
+    assert 1e14 < macs < 1e16
