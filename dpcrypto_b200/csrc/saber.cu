@@ -69,11 +69,11 @@ cudaError_t launch_product(const SaberBatch &b, int form, cudaStream_t st) {
     if ((e = prep(product_tc_kernel<L, MODE>, bytes)) != cudaSuccess) return e;
     product_tc_kernel<L, MODE><<<b.n, 256, bytes, st>>>(b);
   } else if (form == FORM_INT32) {
-    constexpr int bytes = Y::COMMON;
+    constexpr int bytes = Y::DP4A_TOTAL;
     if ((e = prep(product_dp4a_kernel<L, MODE, true>, bytes)) != cudaSuccess) return e;
     product_dp4a_kernel<L, MODE, true><<<b.n, 256, bytes, st>>>(b);
   } else {
-    constexpr int bytes = Y::COMMON;
+    constexpr int bytes = Y::DP4A_TOTAL;
     if ((e = prep(product_dp4a_kernel<L, MODE, false>, bytes)) != cudaSuccess) return e;
     product_dp4a_kernel<L, MODE, false><<<b.n, 256, bytes, st>>>(b);
   }

@@ -246,12 +246,52 @@ __device__ __forceinline__ void finish_inst(const Inst &v) {
 }
 
 // ---------------------------------------------------------------- bit packing helpers
+// Coefficient c of `bits` bits from a little-endian packed array in shared memory that is
+// 4-byte aligned and readable 8 bytes past the coefficient: two aligned words, one funnel
+// shift (sh <= 31 and sh + bits <= 44, so two words always suffice).
+__device__ __forceinline__ uint32_t unpack_smem(const uint8_t *src, int c, int bits) {
+  const int bit = c * bits, by = bit >> 3;
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(src + (by & ~3));
+  return __funnelshift_r(w[0], w[1], (bit & 7) + 8 * (by & 3)) & ((1u << bits) - 1u);
+}
+
 __device__ __forceinline__ uint32_t unpack_coef(const uint8_t *src, int nbytes, int c, int bits) {
   const int bit = c * bits, by = bit >> 3, sh = bit & 7;
   uint32_t w = src[by];
   if (by + 1 < nbytes) w |= (uint32_t)src[by + 1] << 8;
   if (by + 2 < nbytes) w |= (uint32_t)src[by + 2] << 16;
   return (w >> sh) & ((1u << bits) - 1u);
+}
+
+// Packs the G = 8 / gcd(BITS, 8) coefficients v[0..G) (each < 2^BITS) little-endian into
+// G * BITS / 8 bytes at out: the smallest group that ends on a byte boundary, unrolled.
+template <int BITS>
+__device__ __forceinline__ constexpr int group_coefs() {
+  return BITS % 8 == 0 ? 1 : BITS % 4 == 0 ? 2 : BITS % 2 == 0 ? 4 : 8;
+}
+template <int BITS>
+__device__ __forceinline__ void pack_group(const uint16_t *v, uint8_t *out) {
+  constexpr int G = group_coefs<BITS>();
+  uint64_t acc = 0;
+  int nb = 0, o = 0;
+#pragma unroll
+  for (int i = 0; i < G; i++) {
+    acc |= (uint64_t)v[i] << nb;
+    nb += BITS;
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+      if (nb >= 8) {
+        out[o++] = (uint8_t)acc;
+        acc >>= 8;
+        nb -= 8;
+      }
+  }
+}
+// n coefficients (a multiple of the group size) into `out` (shared memory), CTA-wide.
+template <int BITS>
+__device__ __forceinline__ void pack_poly(const uint16_t *v, int n, uint8_t *out) {
+  constexpr int G = group_coefs<BITS>(), NB = G * BITS / 8;
+  for (int g = threadIdx.x; g < n / G; g += blockDim.x) pack_group<BITS>(v + g * G, out + g * NB);
 }
 
 __device__ __forceinline__ uint32_t pack_byte(const uint16_t *v, int q, int bits) {
@@ -282,9 +322,12 @@ __device__ __forceinline__ int cbd_coef(const uint8_t *raw, int c) {
 template <int L>
 struct PL {
   static constexpr int NO_MAX = L + 1;
-  static constexpr int A16 = 0;                               // u16 [L*L][256]
-  static constexpr int B16 = A16 + L * L * SN * 2;            // u16 [L][256] public b / b'
-  static constexpr int SEC = B16 + L * SN * 2;                // s8  [L][256]
+  // Public polynomials are 264 u16 apart (528 B): polynomials read at the same offset
+  // by neighbouring threads start 4 banks apart.
+  static constexpr int PS = SN + 8;
+  static constexpr int A16 = 0;                               // u16 [L*L][PS]
+  static constexpr int B16 = A16 + L * L * PS * 2;            // u16 [L][PS] public b / b'
+  static constexpr int SEC = B16 + L * PS * 2;                // s8  [L][256]
   static constexpr int RES = SEC + L * SN;                    // u16 [L+1][256]
   static constexpr int CM = RES + NO_MAX * SN * 2;            // u16 [256]
   static constexpr int SEQ = CM + SN * 2;                     // s8  [L][528] secret sequences
@@ -299,6 +342,17 @@ struct PL {
   static constexpr int BAR = BOP + (NPAD / 8) * BOP_GROUP;
   static constexpr int TSLOT = BAR + 8;
   static constexpr int TC_TOTAL = TSLOT + 8;
+  // Packed operands copied in from global memory before unpacking; the Hankel matrices
+  // are built after the unpack, so the staging area reuses their space.  Each piece is
+  // followed by 8 readable bytes (unpack_smem).
+  static constexpr int ST_A = HANK;                                         // GenMatrix bytes
+  static constexpr int ST_S = ST_A + SP<L>::ARAW + 8;                       // GenSecret bytes
+  static constexpr int ST_P = ST_S + SP<L>::SRAW + 8;                       // packed b (pk)
+  static constexpr int ST_END = ST_P + SP<L>::POLYVECCOMP + 8;
+  static constexpr int ST_SK = HANK;                                        // decaps inner: 13-bit s
+  static constexpr int ST_CT = ST_SK + SP<L>::POLYVEC + 8;                  // and the ciphertext
+  static constexpr int ST_END_INNER = ST_CT + SP<L>::CT + 8;
+  static constexpr int DP4A_TOTAL = ST_END > ST_END_INNER ? ST_END : ST_END_INNER;
 };
 
 template <int L, int MODE>
@@ -306,12 +360,24 @@ __device__ __forceinline__ constexpr int n_out() {
   return MODE == PM_KEYPAIR ? L : MODE == PM_DEC_INNER ? 1 : L + 1;
 }
 
-// Phase 1: secrets and public polynomials into shared memory.
+// 8-byte copy of `bytes` (a multiple of 8, both ends 8-byte aligned) by the whole CTA.
+__device__ __forceinline__ void copy8(uint8_t *dst, const uint8_t *src, int bytes) {
+  for (int q = threadIdx.x; q < bytes / 8; q += blockDim.x)
+    reinterpret_cast<uint2 *>(dst)[q] = reinterpret_cast<const uint2 *>(src)[q];
+}
+
+// Phase 1: secrets and public polynomials into shared memory.  The packed inputs are
+// first copied in with 8-byte loads (a handful per thread), then unpacked from shared
+// memory, instead of up to three byte loads from global memory per coefficient.
 template <int L, int MODE>
 __device__ __forceinline__ void load_operands(const Inst &v, uint8_t *sm) {
   using P = SP<L>;
   using S = Scr<L>;
   using Y = PL<L>;
+  static_assert(P::ARAW % 8 == 0 && P::SRAW % 8 == 0 && P::POLYVECCOMP % 8 == 0 && P::POLYVEC % 8 == 0 &&
+                    P::CT % 8 == 0,
+                "8-byte staging");
+  static_assert(Y::DP4A_TOTAL <= Y::TC_TOTAL, "staging must fit the tensor form's layout");
   const int tid = threadIdx.x;
   const uint8_t *scr = v.scr;
   int8_t *sec = reinterpret_cast<int8_t *>(sm + Y::SEC);
@@ -319,23 +385,31 @@ __device__ __forceinline__ void load_operands(const Inst &v, uint8_t *sm) {
   uint16_t *b16 = reinterpret_cast<uint16_t *>(sm + Y::B16);
   uint16_t *cm = reinterpret_cast<uint16_t *>(sm + Y::CM);
   if (MODE == PM_DEC_INNER) {
-    const uint8_t *sk = v.sk;
-    const uint8_t *ct = v.ct;
+    copy8(sm + Y::ST_SK, v.sk, P::POLYVEC);
+    copy8(sm + Y::ST_CT, v.ct, P::CT);
+    __syncthreads();
+    const uint8_t *sk = sm + Y::ST_SK, *ct = sm + Y::ST_CT;
     for (int c = tid; c < L * SN; c += blockDim.x) {
-      const uint32_t x = unpack_coef(sk, P::POLYVEC, c, EQ);
+      const uint32_t x = unpack_smem(sk, c, EQ);
       sec[c] = (int8_t)(int32_t)(((x ^ 0x1000u) - 0x1000u));  // centred 13-bit secret
-      b16[c] = (uint16_t)unpack_coef(ct, P::POLYVECCOMP, c, EP);
+      b16[(c / SN) * Y::PS + c % SN] = (uint16_t)unpack_smem(ct, c, EP);
     }
-    for (int c = tid; c < SN; c += blockDim.x)
-      cm[c] = (uint16_t)unpack_coef(ct + P::POLYVECCOMP, P::ET * SN / 8, c, P::ET);
+    for (int c = tid; c < SN; c += blockDim.x) cm[c] = (uint16_t)unpack_smem(ct + P::POLYVECCOMP, c, P::ET);
   } else {
-    const uint8_t *sraw = scr + S::SRAW, *araw = scr + S::ARAW;
-    for (int c = tid; c < L * SN; c += blockDim.x) sec[c] = (int8_t)cbd_coef<P::MU>(sraw + (c / SN) * (P::MU * SN / 8), c % SN);
-    for (int c = tid; c < L * L * SN; c += blockDim.x)
-      a16[c] = (uint16_t)unpack_coef(araw + (c / SN) * (EQ * SN / 8), EQ * SN / 8, c % SN, EQ);
+    copy8(sm + Y::ST_A, scr + S::ARAW, P::ARAW);
+    copy8(sm + Y::ST_S, scr + S::SRAW, P::SRAW);
+    if (MODE != PM_KEYPAIR) copy8(sm + Y::ST_P, MODE == PM_ENC ? v.pk : v.sk + P::POLYVEC, P::POLYVECCOMP);
+    __syncthreads();
+    const uint8_t *sraw = sm + Y::ST_S, *araw = sm + Y::ST_A;
+    constexpr uint32_t hm = (1u << (P::MU / 2)) - 1u;
+    for (int c = tid; c < L * SN; c += blockDim.x) {  // CBD_mu from the GenSecret bytes
+      const uint32_t x = unpack_smem(sraw, c, P::MU);
+      sec[c] = (int8_t)(__popc(x & hm) - __popc((x >> (P::MU / 2)) & hm));
+    }
+    for (int c = tid; c < L * L * SN; c += blockDim.x) a16[(c / SN) * Y::PS + c % SN] = (uint16_t)unpack_smem(araw, c, EQ);
     if (MODE != PM_KEYPAIR) {
-      const uint8_t *pk = MODE == PM_ENC ? v.pk : v.sk + P::POLYVEC;
-      for (int c = tid; c < L * SN; c += blockDim.x) b16[c] = (uint16_t)unpack_coef(pk, P::POLYVECCOMP, c, EP);
+      const uint8_t *pkc = sm + Y::ST_P;
+      for (int c = tid; c < L * SN; c += blockDim.x) b16[(c / SN) * Y::PS + c % SN] = (uint16_t)unpack_smem(pkc, c, EP);
     }
   }
 }
@@ -346,9 +420,9 @@ __device__ __forceinline__ const uint16_t *pub_poly(const uint8_t *sm, int o, in
   using Y = PL<L>;
   const uint16_t *a16 = reinterpret_cast<const uint16_t *>(sm + Y::A16);
   const uint16_t *b16 = reinterpret_cast<const uint16_t *>(sm + Y::B16);
-  if (MODE == PM_DEC_INNER) return b16 + j * SN;
-  if (MODE == PM_KEYPAIR) return a16 + (j * L + o) * SN;  // transposed: b = A^T s
-  return o < L ? a16 + (o * L + j) * SN : b16 + j * SN;
+  if (MODE == PM_DEC_INNER) return b16 + j * Y::PS;
+  if (MODE == PM_KEYPAIR) return a16 + (j * L + o) * Y::PS;  // transposed: b = A^T s
+  return o < L ? a16 + (o * L + j) * Y::PS : b16 + j * Y::PS;
 }
 
 // Phase 3: rounding, packing / comparison.  res holds the products mod 2^16.
@@ -378,25 +452,31 @@ __device__ __forceinline__ void epilogue(const Inst &v, uint8_t *sm) {
     }
   }
   __syncthreads();
+  // Pack into shared memory (the staging area, free again), then 8-byte stores / compares.
+  uint8_t *stg = sm + Y::ST_A;
   if (MODE == PM_KEYPAIR) {
-    uint8_t *pk = v.pk;
-    uint8_t *sk = v.sk;
     const int8_t *sec = reinterpret_cast<const int8_t *>(sm + Y::SEC);
-    for (int q = tid; q < P::POLYVECCOMP; q += nt) pk[q] = (uint8_t)pack_byte(res, q, EP);
+    pack_poly<EP>(res, L * SN, stg);  // POLYVECCOMP bytes
     uint16_t *s13 = reinterpret_cast<uint16_t *>(sm + Y::A16);  // A no longer needed
     for (int c = tid; c < L * SN; c += nt) s13[c] = (uint16_t)((int32_t)sec[c] & 0x1FFF);
     __syncthreads();
-    for (int q = tid; q < P::POLYVEC; q += nt) sk[q] = (uint8_t)pack_byte(s13, q, EQ);
+    pack_poly<EQ>(s13, L * SN, stg + P::POLYVECCOMP);  // POLYVEC bytes
+    __syncthreads();
+    copy8(v.pk, stg, P::POLYVECCOMP);
+    copy8(v.sk, stg + P::POLYVECCOMP, P::POLYVEC);
     return;
   }
-  uint8_t *ct = v.ct;
-  uint32_t diff = 0;
-  for (int q = tid; q < P::CT; q += nt) {
-    const uint32_t v = q < P::POLYVECCOMP ? pack_byte(res, q, EP) : pack_byte(res + L * SN, q - P::POLYVECCOMP, P::ET);
-    if (MODE == PM_ENC) ct[q] = (uint8_t)v;
-    else diff |= v ^ ct[q];
-  }
-  if (MODE == PM_DEC_CMP) {
+  pack_poly<EP>(res, L * SN, stg);
+  pack_poly<P::ET>(res + L * SN, SN, stg + P::POLYVECCOMP);
+  __syncthreads();
+  if (MODE == PM_ENC) {
+    copy8(v.ct, stg, P::CT);
+  } else {
+    uint32_t diff = 0;
+    for (int q = tid; q < P::CT / 8; q += nt) {
+      const uint2 a = reinterpret_cast<const uint2 *>(stg)[q], b = reinterpret_cast<const uint2 *>(v.ct)[q];
+      diff |= (a.x ^ b.x) | (a.y ^ b.y);
+    }
     const int any = __syncthreads_or(diff != 0);
     if (tid == 0) *v.fail = (uint32_t)any;
   }
@@ -502,22 +582,22 @@ __device__ __forceinline__ bool product_tc_cta(const Inst &v, uint8_t *sm, uint3
         make_uint4(__funnelshift_r(x0, x1, sh), __funnelshift_r(x1, x2, sh), __funnelshift_r(x2, x3, sh),
                    __funnelshift_r(x3, x4, sh));
   }
-  // B operand: row n = o + NO*limb, K = 256 j + k', value = limb(P_{o,j}[255 - k']).
+  // B operand: row n = o + NO*limb, K = 256 j + k', value = limb(P_{o,j}[255 - k']).  One
+  // thread per (row n, 16-column chunk kc): coefficients 255-k0 .. 240-k0 are two aligned
+  // 16-byte reads (8 little-endian pairs); a PRMT turns two pairs into 4 output bytes,
+  // reversed.  Threads n = 0..7 of a chunk write its 128 bytes contiguously.
   for (int x = tid; x < NPAD * L * (SN / 16); x += 256) {
-    const int n = x / (L * SN / 16), kc = x % (L * SN / 16), j = kc / (SN / 16), k0 = 16 * (kc % (SN / 16));
-    uint32_t w[4] = {0, 0, 0, 0};
+    const int n = (x & 7) + 8 * (x / (8 * L * (SN / 16))), kc = (x >> 3) % (L * SN / 16);
+    const int j = kc / (SN / 16), k0 = 16 * (kc % (SN / 16));
+    uint4 out = make_uint4(0, 0, 0, 0);
     if (n < 2 * NO) {
-      const int o = n % NO, limb = n / NO;
-      const uint16_t *pp = pub_poly<L, MODE>(sm, o, j);
-#pragma unroll
-      for (int c = 0; c < 16; c++) {
-        const uint32_t y = pp[255 - (k0 + c)];
-        const uint32_t byte = limb ? (y >> 8) : (y & 0xFFu);
-        w[c >> 2] |= byte << (8 * (c & 3));
-      }
+      const int o = n % NO;
+      const uint32_t sel = n < NO ? 0x4602u : 0x5713u;  // low / high byte of each coefficient
+      const uint4 *pw = reinterpret_cast<const uint4 *>(pub_poly<L, MODE>(sm, o, j) + 240 - k0);
+      const uint4 w0 = pw[0], w1 = pw[1];  // coefficients 240-k0 .. 247-k0 and 248-k0 .. 255-k0
+      out = make_uint4(prmt(w1.w, w1.z, sel), prmt(w1.y, w1.x, sel), prmt(w0.w, w0.z, sel), prmt(w0.y, w0.x, sel));
     }
-    *reinterpret_cast<uint4 *>(sm + Y::BOP + (n >> 3) * Y::BOP_GROUP + kc * 128 + (n & 7) * 16) =
-        make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4 *>(sm + Y::BOP + (n >> 3) * Y::BOP_GROUP + kc * 128 + (n & 7) * 16) = out;
   }
   fence_proxy_async_smem();
   tc_fence_before();
