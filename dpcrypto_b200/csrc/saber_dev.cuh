@@ -263,6 +263,29 @@ __device__ __forceinline__ uint32_t unpack_coef(const uint8_t *src, int nbytes, 
   return (w >> sh) & ((1u << bits) - 1u);
 }
 
+// Unpacks NC little-endian BITS-bit fields from whole words (NC * BITS a multiple of 32)
+// and calls f(i, value) for each; all bit offsets are compile-time after unrolling.
+template <int BITS, int NC, class F>
+__device__ __forceinline__ void unpack_words(const uint32_t *w, F &&f) {
+  static_assert(NC * BITS % 32 == 0, "whole words");
+  constexpr int NW = NC * BITS / 32;
+  uint32_t r[NW + 1];
+#pragma unroll
+  for (int k = 0; k < NW; k++) r[k] = w[k];
+  r[NW] = 0;
+#pragma unroll
+  for (int i = 0; i < NC; i++) {
+    const int bit = i * BITS, k = bit >> 5, sh = bit & 31;
+    const uint32_t v = sh + BITS <= 32 ? r[k] >> sh : __funnelshift_r(r[k], r[k + 1], sh);
+    f(i, v & ((1u << BITS) - 1u));
+  }
+}
+
+// Byte-wise two's-complement negation of four int8 lanes.
+__device__ __forceinline__ uint32_t neg_bytes(uint32_t x) {
+  return ((~x & 0x7F7F7F7Fu) + 0x01010101u) ^ (~x & 0x80808080u);
+}
+
 // Packs the G = 8 / gcd(BITS, 8) coefficients v[0..G) (each < 2^BITS) little-endian into
 // G * BITS / 8 bytes at out: the smallest group that ends on a byte boundary, unrolled.
 template <int BITS>
@@ -380,37 +403,98 @@ __device__ __forceinline__ void load_operands(const Inst &v, uint8_t *sm) {
   static_assert(Y::DP4A_TOTAL <= Y::TC_TOTAL, "staging must fit the tensor form's layout");
   const int tid = threadIdx.x;
   const uint8_t *scr = v.scr;
-  int8_t *sec = reinterpret_cast<int8_t *>(sm + Y::SEC);
+  uint32_t *secw = reinterpret_cast<uint32_t *>(sm + Y::SEC);  // 4 int8 coefficients per word
   uint16_t *a16 = reinterpret_cast<uint16_t *>(sm + Y::A16);
   uint16_t *b16 = reinterpret_cast<uint16_t *>(sm + Y::B16);
   uint16_t *cm = reinterpret_cast<uint16_t *>(sm + Y::CM);
+  // Public polynomials with 10-bit coefficients: 16 coefficients (5 words) per thread, two
+  // 16-byte stores.
+  auto unpack_p = [&](const uint8_t *src) {
+    for (int g = tid; g < L * SN / 16; g += blockDim.x) {
+      uint32_t o[8];
+      unpack_words<EP, 16>(reinterpret_cast<const uint32_t *>(src) + 5 * g, [&](int i, uint32_t x) {
+        if (i & 1) o[i >> 1] |= x << 16;
+        else o[i >> 1] = x;
+      });
+      uint4 *d = reinterpret_cast<uint4 *>(b16 + (g >> 4) * Y::PS + 16 * (g & 15));
+      d[0] = make_uint4(o[0], o[1], o[2], o[3]);
+      d[1] = make_uint4(o[4], o[5], o[6], o[7]);
+    }
+  };
   if (MODE == PM_DEC_INNER) {
     copy8(sm + Y::ST_SK, v.sk, P::POLYVEC);
     copy8(sm + Y::ST_CT, v.ct, P::CT);
     __syncthreads();
-    const uint8_t *sk = sm + Y::ST_SK, *ct = sm + Y::ST_CT;
-    for (int c = tid; c < L * SN; c += blockDim.x) {
-      const uint32_t x = unpack_smem(sk, c, EQ);
-      sec[c] = (int8_t)(int32_t)(((x ^ 0x1000u) - 0x1000u));  // centred 13-bit secret
-      b16[(c / SN) * Y::PS + c % SN] = (uint16_t)unpack_smem(ct, c, EP);
+    const uint8_t *ct = sm + Y::ST_CT;
+    // 13-bit secret from sk, centred: 32 coefficients (13 words) per thread.
+    for (int g = tid; g < L * SN / 32; g += blockDim.x) {
+      uint32_t o[8];
+      unpack_words<EQ, 32>(reinterpret_cast<const uint32_t *>(sm + Y::ST_SK) + 13 * g, [&](int i, uint32_t x) {
+        const uint32_t b = x & 0xFFu;  // low byte of the centred value (|s| < 128)
+        if ((i & 3) == 0) o[i >> 2] = b;
+        else o[i >> 2] |= b << (8 * (i & 3));
+      });
+      uint4 *d = reinterpret_cast<uint4 *>(secw + 8 * g);
+      d[0] = make_uint4(o[0], o[1], o[2], o[3]);
+      d[1] = make_uint4(o[4], o[5], o[6], o[7]);
     }
+    unpack_p(ct);
     for (int c = tid; c < SN; c += blockDim.x) cm[c] = (uint16_t)unpack_smem(ct + P::POLYVECCOMP, c, P::ET);
   } else {
     copy8(sm + Y::ST_A, scr + S::ARAW, P::ARAW);
     copy8(sm + Y::ST_S, scr + S::SRAW, P::SRAW);
     if (MODE != PM_KEYPAIR) copy8(sm + Y::ST_P, MODE == PM_ENC ? v.pk : v.sk + P::POLYVEC, P::POLYVECCOMP);
     __syncthreads();
-    const uint8_t *sraw = sm + Y::ST_S, *araw = sm + Y::ST_A;
+    // CBD_mu from the GenSecret bytes: 16 coefficients (mu/2 words) per thread.
     constexpr uint32_t hm = (1u << (P::MU / 2)) - 1u;
-    for (int c = tid; c < L * SN; c += blockDim.x) {  // CBD_mu from the GenSecret bytes
-      const uint32_t x = unpack_smem(sraw, c, P::MU);
-      sec[c] = (int8_t)(__popc(x & hm) - __popc((x >> (P::MU / 2)) & hm));
+    for (int g = tid; g < L * SN / 16; g += blockDim.x) {
+      uint32_t o[4];
+      unpack_words<P::MU, 16>(reinterpret_cast<const uint32_t *>(sm + Y::ST_S) + (P::MU / 2) * g,
+                              [&](int i, uint32_t x) {
+                                const uint32_t b = (uint32_t)(__popc(x & hm) - __popc((x >> (P::MU / 2)) & hm)) & 0xFFu;
+                                if ((i & 3) == 0) o[i >> 2] = b;
+                                else o[i >> 2] |= b << (8 * (i & 3));
+                              });
+      reinterpret_cast<uint4 *>(secw)[g] = make_uint4(o[0], o[1], o[2], o[3]);
     }
-    for (int c = tid; c < L * L * SN; c += blockDim.x) a16[(c / SN) * Y::PS + c % SN] = (uint16_t)unpack_smem(araw, c, EQ);
-    if (MODE != PM_KEYPAIR) {
-      const uint8_t *pkc = sm + Y::ST_P;
-      for (int c = tid; c < L * SN; c += blockDim.x) b16[(c / SN) * Y::PS + c % SN] = (uint16_t)unpack_smem(pkc, c, EP);
+    // GenMatrix: 13-bit coefficients, 32 (13 words) per thread, four 16-byte stores.
+    for (int g = tid; g < L * L * SN / 32; g += blockDim.x) {
+      uint32_t o[16];
+      unpack_words<EQ, 32>(reinterpret_cast<const uint32_t *>(sm + Y::ST_A) + 13 * g, [&](int i, uint32_t x) {
+        if (i & 1) o[i >> 1] |= x << 16;
+        else o[i >> 1] = x;
+      });
+      uint4 *d = reinterpret_cast<uint4 *>(a16 + (g >> 3) * Y::PS + 32 * (g & 7));
+#pragma unroll
+      for (int q = 0; q < 4; q++) d[q] = make_uint4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
     }
+    if (MODE != PM_KEYPAIR) unpack_p(sm + Y::ST_P);
+  }
+}
+
+// Secret sequences, one 32-bit word (4 int8) per thread step, from the secrets in SEC.
+//   TC  : E_j[e] = s_ext[e - 255], e in [0, 528): -s[e + 1] for e < 255, s[e - 255] for
+//         255 <= e < 511, 0 above (the Hankel generating sequence).
+//   dp4a: R_j[t] = s_ext[255 - t]: s[255 - t] for t < 256, -s[511 - t] below 512, 0 above.
+template <int L, bool TC>
+__device__ __forceinline__ void build_seq(uint8_t *sm) {
+  using Y = PL<L>;
+  constexpr int NW = Y::SEQ_STRIDE / 4;  // 132
+  const uint32_t *secw = reinterpret_cast<const uint32_t *>(sm + Y::SEC);
+  uint32_t *seqw = reinterpret_cast<uint32_t *>(sm + Y::SEQ);
+  for (int x = threadIdx.x; x < L * NW; x += blockDim.x) {
+    const int j = x / NW, k = x - j * NW;
+    const uint32_t *sw = secw + 64 * j;
+    uint32_t e = 0;
+    if (TC) {
+      if (k <= 63) e = neg_bytes(__funnelshift_r(sw[k], k < 63 ? sw[k + 1] : 0u, 8));
+      else if (k <= 127) e = __funnelshift_r(sw[k - 64], k < 127 ? sw[k - 63] : 0u, 8);
+      if (k == 63) e |= sw[0] << 24;
+    } else {
+      if (k < 64) e = __byte_perm(sw[63 - k], 0, 0x0123);
+      else if (k < 128) e = neg_bytes(__byte_perm(sw[127 - k], 0, 0x0123));
+    }
+    seqw[x] = e;
   }
 }
 
@@ -495,14 +579,7 @@ __device__ __forceinline__ void product_dp4a_cta(const Inst &v, uint8_t *sm) {
   const int tid = threadIdx.x;
   load_operands<L, MODE>(v, sm);
   __syncthreads();
-  const int8_t *sec = reinterpret_cast<const int8_t *>(sm + Y::SEC);
-  for (int x = tid; x < L * Y::SEQ_STRIDE; x += 256) {
-    const int j = x / Y::SEQ_STRIDE, t = x % Y::SEQ_STRIDE;
-    int8_t r = 0;
-    if (t < 256) r = sec[j * SN + 255 - t];
-    else if (t < 512) r = (int8_t)(-sec[j * SN + 511 - t]);
-    reinterpret_cast<int8_t *>(sm + Y::SEQ)[x] = r;
-  }
+  build_seq<L, false>(sm);
   __syncthreads();
   const int base = 255 - tid, wb = base >> 2, sh = 8 * (base & 3);
   int acc[NO];
@@ -561,26 +638,26 @@ __device__ __forceinline__ bool product_tc_cta(const Inst &v, uint8_t *sm, uint3
   }
   load_operands<L, MODE>(v, sm);
   __syncthreads();
-  // E_j[e] = s_ext[e - 255], e in [0, 511): the Hankel generating sequence.
-  const int8_t *sec = reinterpret_cast<const int8_t *>(sm + Y::SEC);
-  int8_t *seq = reinterpret_cast<int8_t *>(sm + Y::SEQ);
-  for (int x = tid; x < L * Y::SEQ_STRIDE; x += 256) {
-    const int j = x / Y::SEQ_STRIDE, e = x % Y::SEQ_STRIDE;
-    int8_t r = 0;
-    if (e >= 255 && e < 511) r = sec[j * SN + e - 255];
-    else if (e < 255) r = (int8_t)(-sec[j * SN + e + 1]);
-    seq[x] = r;
-  }
+  build_seq<L, true>(sm);
   __syncthreads();
-  // Hankel core matrices: H_j[t][r][c] = E_j[8t + r + c].
-  for (int x = tid; x < L * 62 * 8; x += 256) {
-    const int j = x / (62 * 8), t = (x / 8) % 62, r = x & 7, e0 = 8 * t + r;
-    const uint32_t *sw = reinterpret_cast<const uint32_t *>(seq + j * Y::SEQ_STRIDE);
-    const int wb = e0 >> 2, sh = 8 * (e0 & 3);
-    const uint32_t x0 = sw[wb], x1 = sw[wb + 1], x2 = sw[wb + 2], x3 = sw[wb + 3], x4 = sw[wb + 4];
-    *reinterpret_cast<uint4 *>(sm + Y::HANK + j * Y::HANK_STRIDE + t * 128 + r * 16) =
-        make_uint4(__funnelshift_r(x0, x1, sh), __funnelshift_r(x1, x2, sh), __funnelshift_r(x2, x3, sh),
-                   __funnelshift_r(x3, x4, sh));
+  // Hankel core matrices: H_j[t][r][c] = E_j[8t + r + c].  Row r = tid % 8 is fixed per
+  // thread; (j, t) advance by 32 core matrices per step, and 8 consecutive threads write one
+  // 128-byte core matrix.
+  {
+    const int r = tid & 7, sh = 8 * (r & 3);
+    int j = 0, t = tid >> 3;
+    while (j < L) {
+      const uint32_t *sw = reinterpret_cast<const uint32_t *>(sm + Y::SEQ + j * Y::SEQ_STRIDE) + 2 * t + (r >> 2);
+      const uint32_t x0 = sw[0], x1 = sw[1], x2 = sw[2], x3 = sw[3], x4 = sw[4];
+      *reinterpret_cast<uint4 *>(sm + Y::HANK + j * Y::HANK_STRIDE + t * 128 + r * 16) =
+          make_uint4(__funnelshift_r(x0, x1, sh), __funnelshift_r(x1, x2, sh), __funnelshift_r(x2, x3, sh),
+                     __funnelshift_r(x3, x4, sh));
+      t += 32;
+      if (t >= 62) {
+        t -= 62;
+        j++;
+      }
+    }
   }
   // B operand: row n = o + NO*limb, K = 256 j + k', value = limb(P_{o,j}[255 - k']).  One
   // thread per (row n, 16-column chunk kc): coefficients 255-k0 .. 240-k0 are two aligned
@@ -605,16 +682,16 @@ __device__ __forceinline__ bool product_tc_cta(const Inst &v, uint8_t *sm, uint3
   tc_fence_after();
   if (tid == 0) {
     constexpr uint32_t idesc = idesc_i8(128, NPAD, true, false, false, false);
-    const uint32_t h0 = smem_u32(sm + Y::HANK), b0 = smem_u32(sm + Y::BOP);
+    // Base descriptors; a step moves only the start-address field (address / 16, low word).
+    const uint64_t a0 = sdesc(smem_u32(sm + Y::HANK), 256, 128), b0 = sdesc(smem_u32(sm + Y::BOP), 128, Y::BOP_GROUP);
 #pragma unroll
     for (int mt = 0; mt < 2; mt++)
+#pragma unroll
       for (int j = 0; j < L; j++)
 #pragma unroll
-        for (int ks = 0; ks < 8; ks++) {
-          const uint64_t ad = sdesc(h0 + j * Y::HANK_STRIDE + (16 * mt + 4 * ks) * 128, 256, 128);
-          const uint64_t bd = sdesc(b0 + (16 * j + 2 * ks) * 128, 128, Y::BOP_GROUP);
-          mma_i8(tbase + mt * NPAD, ad, bd, idesc, (j | ks) ? 1u : 0u);
-        }
+        for (int ks = 0; ks < 8; ks++)
+          mma_i8(tbase + mt * NPAD, a0 + (uint64_t)((j * Y::HANK_STRIDE + (16 * mt + 4 * ks) * 128) >> 4),
+                 b0 + (uint64_t)(((16 * j + 2 * ks) * 128) >> 4), idesc, (j | ks) ? 1u : 0u);
     mma_commit(bar);
   }
   const bool ok = mbar_wait(bar, 0);
