@@ -22,11 +22,15 @@
 
 #include "../../include/dpkem.h"
 #include "common.cuh"
+#include "saber_dev.cuh"
 
 namespace {
 
 constexpr size_t kMaxInst = DPKEM_SABER_ENC_STATIC_MAX;
-constexpr size_t kRecord = 7520;  // largest Saber scratch record (FireSaber, l = 4)
+constexpr size_t kRecord = dpkem::sdev::Scr<4>::BYTES;  // largest Saber scratch record (FireSaber)
+static_assert(dpkem::sdev::Scr<4>::BYTES >= dpkem::sdev::Scr<3>::BYTES &&
+                  dpkem::sdev::Scr<4>::BYTES >= dpkem::sdev::Scr<2>::BYTES,
+              "FireSaber has the largest record");
 constexpr size_t kScratchBytes = kMaxInst * kRecord;
 constexpr size_t kErrOffset = kScratchBytes + kMaxInst * 4;  // after the per-instance fail words
 

@@ -4,11 +4,11 @@
 //
 // Kernel chain per operation:
 //   prologue  (64 threads = 32 instances: warp 0 runs the hash chain and GenSecret's
-//              SHAKE128, warp 1 runs GenMatrix's SHAKE128, in parallel; raw XOF bytes
-//              go to the scratch arena)
+//              SHAKE128 (decaps: then SHA3-256 of the input ciphertext), warp 1 runs
+//              GenMatrix's SHAKE128, in parallel; raw XOF bytes go to the scratch arena)
 //   product   (CTA/instance: CBD sampling, 13/10-bit unpacking, the negacyclic
 //              matrix-vector and inner products, rounding, packing / comparison)
-//   finish    (thread/instance: SHA3-256(c), final key, or H(pk) for keypair)
+//   finish    (thread/instance: SHA3-256(c) (encaps), final key, or H(pk) for keypair)
 // Decaps runs the product kernel twice: first the inner product v = b'^T s with the
 // secret from sk (-> m'), then the re-encryption in compare mode.
 //
@@ -59,7 +59,8 @@ struct Scr {
   static constexpr int SRAW = (SP<L>::ARAW + 15) & ~15;
   static constexpr int KR = SRAW + ((SP<L>::SRAW + 15) & ~15);
   static constexpr int MTXT = KR + 64;
-  static constexpr int BYTES = MTXT + 32;
+  static constexpr int HC = MTXT + 32;  // decaps: SHA3-256(c), hashed by the prologue
+  static constexpr int BYTES = HC + 32;
 };
 
 // Pointers of one instance, already offset into the caller's arrays and the scratch arena.
@@ -205,6 +206,15 @@ __device__ __forceinline__ void prologue_inst(const Inst &v, int role) {
     for (int q = 0; q < 4; q++) seed[q] = kr[4 + q];
   }
   shake128_seed32(seed, scr + S::SRAW, P::SRAW);
+  if (OP == OP_DEC) {
+    // H(c) of the input ciphertext does not wait for the products: hashing it here keeps
+    // this role (15 permutations at l = 3) shorter than GenMatrix's, and the finish stage
+    // down to one permutation.
+    uint2 hc[4];
+    sha3_256_msg(v.ct, P::CT, hc);
+#pragma unroll
+    for (int q = 0; q < 4; q++) *reinterpret_cast<uint2 *>(scr + S::HC + 8 * q) = hc[q];
+  }
 }
 
 // ---------------------------------------------------------------- finish
@@ -227,7 +237,12 @@ __device__ __forceinline__ void finish_inst(const Inst &v) {
   }
   const uint8_t *scr = v.scr;
   uint2 m[8], hc[4], k[4];
-  sha3_256_msg(v.ct, P::CT, hc);
+  if (OP == OP_DEC) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) hc[q] = ld_lane(scr + S::HC + 8 * q);
+  } else {
+    sha3_256_msg(v.ct, P::CT, hc);
+  }
   const uint32_t msk = OP == OP_DEC ? 0u - (uint32_t)(*v.fail != 0u) : 0u;
   const uint8_t *z = v.sk + P::SK - 32;
 #pragma unroll
@@ -253,14 +268,6 @@ __device__ __forceinline__ uint32_t unpack_smem(const uint8_t *src, int c, int b
   const int bit = c * bits, by = bit >> 3;
   const uint32_t *w = reinterpret_cast<const uint32_t *>(src + (by & ~3));
   return __funnelshift_r(w[0], w[1], (bit & 7) + 8 * (by & 3)) & ((1u << bits) - 1u);
-}
-
-__device__ __forceinline__ uint32_t unpack_coef(const uint8_t *src, int nbytes, int c, int bits) {
-  const int bit = c * bits, by = bit >> 3, sh = bit & 7;
-  uint32_t w = src[by];
-  if (by + 1 < nbytes) w |= (uint32_t)src[by + 1] << 8;
-  if (by + 2 < nbytes) w |= (uint32_t)src[by + 2] << 16;
-  return (w >> sh) & ((1u << bits) - 1u);
 }
 
 // Unpacks NC little-endian BITS-bit fields from whole words (NC * BITS a multiple of 32)
@@ -330,14 +337,6 @@ __device__ __forceinline__ uint32_t pack_byte(const uint16_t *v, int q, int bits
     have += bits;
   }
   return acc & 0xFFu;
-}
-
-// CBD_mu: coefficient c = popcount(bits [mu c, mu c + mu/2)) - popcount(next mu/2 bits).
-template <int MU>
-__device__ __forceinline__ int cbd_coef(const uint8_t *raw, int c) {
-  const uint32_t v = unpack_coef(raw, MU * SN / 8, c, MU);
-  constexpr uint32_t hm = (1u << (MU / 2)) - 1u;
-  return __popc(v & hm) - __popc((v >> (MU / 2)) & hm);
 }
 
 // ---------------------------------------------------------------- product kernel
