@@ -10,11 +10,18 @@ using sdev::inst_of;
 using sdev::PL;
 using sdev::Scr;
 
-// blockDim 64: warp 0 = hash chain + GenSecret XOF, warp 1 = GenMatrix XOF, 32 instances.
+// blockDim 96, 32 instances: warp 0 = hash chain + GenSecret XOF (a thread per instance),
+// warps 1-2 = GenMatrix XOF (a lane pair per instance).
 template <int L, int OP>
-__global__ void __launch_bounds__(64) prologue_kernel(SaberBatch b) {
-  const int i = blockIdx.x * 32 + (threadIdx.x & 31);
-  if (i < b.n) sdev::prologue_inst<L, OP>(inst_of<L>(b, i, OP), threadIdx.x >> 5);
+__global__ void __launch_bounds__(96) prologue_kernel(SaberBatch b) {
+  if (threadIdx.x < 32) {
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    if (i < b.n) sdev::prologue_inst<L, OP>(inst_of<L>(b, i, OP), 0);
+    return;
+  }
+  const int t = threadIdx.x - 32, i = blockIdx.x * 32 + (t >> 1);
+  const bool live = i < b.n;
+  sdev::matrix_pair<L, OP>(inst_of<L>(b, live ? i : b.n - 1, OP), t & 1, live);
 }
 
 template <int L, int OP>
@@ -92,14 +99,14 @@ cudaError_t run(const SaberBatch &b, int op, int form, cudaStream_t st) {
   mark(b, st);
   switch (op) {
     case OP_KEYPAIR:
-      prologue_kernel<L, OP_KEYPAIR><<<pb, 64, 0, st>>>(b);
+      prologue_kernel<L, OP_KEYPAIR><<<pb, 96, 0, st>>>(b);
       mark(b, st);
       if ((e = launch_product<L, sdev::PM_KEYPAIR>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
       finish_kernel<L, OP_KEYPAIR><<<fb, tb, 0, st>>>(b);
       break;
     case OP_ENC:
-      prologue_kernel<L, OP_ENC><<<pb, 64, 0, st>>>(b);
+      prologue_kernel<L, OP_ENC><<<pb, 96, 0, st>>>(b);
       mark(b, st);
       if ((e = launch_product<L, sdev::PM_ENC>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
@@ -108,7 +115,7 @@ cudaError_t run(const SaberBatch &b, int op, int form, cudaStream_t st) {
     default:
       if ((e = launch_product<L, sdev::PM_DEC_INNER>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
-      prologue_kernel<L, OP_DEC><<<pb, 64, 0, st>>>(b);
+      prologue_kernel<L, OP_DEC><<<pb, 96, 0, st>>>(b);
       mark(b, st);
       if ((e = launch_product<L, sdev::PM_DEC_CMP>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);

@@ -30,6 +30,7 @@
 #pragma once
 #include "common.cuh"
 #include "keccak.cuh"
+#include "keccak_pair.cuh"
 #include "tc.cuh"
 
 namespace dpkem {
@@ -215,6 +216,39 @@ __device__ __forceinline__ void prologue_inst(const Inst &v, int role) {
 #pragma unroll
     for (int q = 0; q < 4; q++) *reinterpret_cast<uint2 *>(scr + S::HC + 8 * q) = hc[q];
   }
+}
+
+// GenMatrix (prologue role 1) on a lane pair (p = lane parity): its 10 / 23 / 40 permutations are
+// the longest chain of the prologue.  live = false keeps a padding pair of a partial warp in
+// step (its reads are valid, its writes are skipped).
+template <int L, int OP>
+__device__ __forceinline__ void matrix_pair(const Inst &v, int p, bool live) {
+  using P = SP<L>;
+  using S = Scr<L>;
+  uint32_t a[25];
+  kpair::zero(a);
+  if (OP == OP_KEYPAIR) {
+    // seed_A = SHAKE128(coins[0:32], 32), published in pk.
+#pragma unroll
+    for (int q = 0; q < 4; q++) a[q] = kpair::to_slice(ld_lane(v.coins + 8 * q), p);
+    kpair::absorb_finish<168>(a, 32, 0x1Fu, p);
+    uint32_t seed[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      seed[q] = a[q];
+      const uint32_t h = kpair::from_slice(a[q], p);
+      if (live) *reinterpret_cast<uint32_t *>(v.pk + P::POLYVECCOMP + 8 * q + 4 * p) = h;
+    }
+    kpair::zero(a);
+#pragma unroll
+    for (int q = 0; q < 4; q++) a[q] = seed[q];
+  } else {
+    const uint8_t *src = OP == OP_ENC ? v.pk + P::POLYVECCOMP : v.sk + P::POLYVEC + P::POLYVECCOMP;
+#pragma unroll
+    for (int q = 0; q < 4; q++) a[q] = kpair::to_slice(ld_lane(src + 8 * q), p);
+  }
+  kpair::absorb_finish<168>(a, 32, 0x1Fu, p);
+  kpair::squeeze<168>(a, v.scr + S::ARAW, P::ARAW, p, live);
 }
 
 // ---------------------------------------------------------------- finish
