@@ -199,15 +199,24 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
   // Host-mode batches of at least two minimum chunks, when the budget holds the whole batch,
   // run as a pipeline: up to pipe_chunks chunks, each on its own stream with its own arena region,
   // all in flight at once.  The copies of later chunks and their latency-bound first stages
-  // then overlap the long kernels of earlier chunks.
+  // then overlap the long kernels of earlier chunks.  With three or more chunks the first and
+  // the last are a quarter of the others: the first upload and the last download are the
+  // copies that no kernel overlaps.
   size_t chunk = std::min(n, chunk_for(c, scheme, op, !dev));
   int npipe = 1;
+  size_t edge = 0;  // pipelined: size of the first and the last chunk (0: all equal)
   if (!dev && !c->profile && n >= 2 * kPipeChunkMin) {
     const int want = (int)std::min<size_t>(std::min(tuning().pipe_chunks, kPipeChunks), n / kPipeChunkMin);
-    const size_t each = (n + want - 1) / want;
+    size_t each = (n + want - 1) / want, e = 0;
+    if (want >= 3) {
+      const size_t w = 2 + 4 * (size_t)(want - 2);  // weights 1, 4, ..., 4, 1
+      e = std::max<size_t>(1, n / w);
+      each = (n - 2 * e + want - 3) / (want - 2);
+    }
     if (each * want <= chunk_for(c, scheme, op, true) && want > 1) {
       npipe = want;
       chunk = each;
+      edge = e;
     }
   }
   const size_t per_pipe = (arena_need(scheme, op, chunk, !dev) + kAlign - 1) & ~(kAlign - 1);
@@ -231,9 +240,10 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
     case OP_ENC: in0_sz = z.encc; in1_sz = z.pk; out0_sz = z.ct; out1_sz = z.ss; break;
     default: in0_sz = z.ct; in1_sz = z.sk; out0_sz = z.ss; break;
   }
-  size_t k = 0;
-  for (size_t first = 0; first < n; first += chunk, k++) {
-    const size_t m = std::min(chunk, n - first);
+  size_t k = 0, m = 0;
+  for (size_t first = 0; first < n; first += m, k++) {
+    m = std::min(chunk, n - first);
+    if (edge && (k == 0 || k + 1 == (size_t)npipe)) m = std::min(edge, n - first);
     const int j = (int)(k % (size_t)npipe);
     cudaStream_t sj = streams[j];
     Carver cv{c->arena + (size_t)j * per_pipe};
