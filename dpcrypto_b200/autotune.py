@@ -8,10 +8,15 @@ Knobs:
   mixed_thread_task  instances per other thread-level task
   pipe_chunks        chunks (one stream each) of a pipelined host-buffer batch
   pipe_priority      chunk streams with descending priorities (earlier chunks finish first)
+  saber_pair_max     Keccak lanes per state in the Saber prologue: batches of up to this many
+                     instances run GenMatrix on lane pairs (shorter chain while SM
+                     sub-partitions idle), larger ones on one lane (fewer issue slots per
+                     state); the sweep times both at 2k-16k instances and keeps the crossover
 Not knobs, with the measured reason recorded in the output: the MMA tile shape (the int8
 MMAs are <1 % of the tensor pipe: M = 128 is the smallest tile that keeps one TMEM lane per
-output row) and Keccak lanes per thread (one state per thread; the kernels are bound by the
-integer pipe, and splitting a state across threads adds shuffles to the same pipe).
+output row) and Keccak lanes per state in the throughput-bound kernels (the fused S'A
+stages and the persistent mixed kernel keep one state per thread: a pair costs more issue
+slots per state on an integer pipe those kernels already saturate).
 
     python -m dpcrypto_b200.autotune --build          # build variants (CPU, nvcc)
     python -m dpcrypto_b200.autotune --measure        # on a B200: sweep, write tuning.json
@@ -137,6 +142,32 @@ def _child(u: int) -> dict:
                 eng.dec(d.FRODO976, h_ct, h_sk, d.FORM_TC)
             psweep[f"{pc}/{prio}"] = (time.perf_counter() - t0) / 3 * 1e3
     res["pipe_chunks_priority_ms"] = psweep
+    # Keccak lanes per state in the Saber l=3 prologue, by batch size: encaps + decaps, device buffers
+    def saber_time(n: int) -> float:
+        kc = torch.empty((n, 96), dtype=torch.uint8, device="cuda")
+        sc = torch.empty((n, 32), dtype=torch.uint8, device="cuda")
+        eng.coins(n, 96, "tune-kp", out=kc)
+        eng.coins(n, 32, "tune-enc", out=sc)
+        spk, ssk = eng.keypair(d.SABER, kc, d.FORM_TC)
+        sct = torch.empty((n, 1088), dtype=torch.uint8, device="cuda")
+        sss = torch.empty((n, 32), dtype=torch.uint8, device="cuda")
+        for _ in range(2):
+            eng.enc(d.SABER, spk, sc, d.FORM_TC, out=(sct, sss))
+            eng.dec(d.SABER, sct, ssk, d.FORM_TC)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(10):
+            eng.enc(d.SABER, spk, sc, d.FORM_TC, out=(sct, sss))
+            eng.dec(d.SABER, sct, ssk, d.FORM_TC)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / 10 * 1e3
+
+    lsweep = {}
+    for n in (2048, 4096, 8192, 16384):
+        for name, val in (("one", 0), ("pair", 1 << 30)):
+            kem.set_tuning("saber_pair_max", val)
+            lsweep[f"{n}/{name}"] = saber_time(n)
+    res["saber_lanes_ms"] = lsweep
     return res
 
 
@@ -159,19 +190,27 @@ def measure() -> dict:
     mk = min(best["mixed_task_ms"], key=best["mixed_task_ms"].get)
     pc, prio = (int(x) for x in min(best["pipe_chunks_priority_ms"], key=best["pipe_chunks_priority_ms"].get).split("/"))
     ft, stt, tt = (int(x) for x in mk.split("/"))
+    ls = best["saber_lanes_ms"]
+    pair_max = max([int(k.split("/")[0]) for k in ls if k.endswith("/pair") and ls[k] < ls[k.replace("/pair", "/one")]],
+                   default=0)
     import torch
 
     out = {
         "device": torch.cuda.get_device_name(0),
         "chosen": {"keccak_unroll": best["keccak_unroll"], "thread_block": int(tb), "mixed_frodo_task": ft,
                    "mixed_pair_task": stt, "mixed_thread_task": tt, "pipe_chunks": pc,
-                   "pipe_priority": prio},
+                   "pipe_priority": prio, "saber_pair_max": pair_max},
         "fixed": {"mma_tile": "M=128 (N=8 Frodo, N=8/16 Saber), K=32: int8 MMA <1% of the tensor pipe",
-                  "keccak_lanes_per_thread": 1},
+                  "keccak_lanes_per_state_throughput_kernels": 1},
         "measurements": results,
         "command": "python -m dpcrypto_b200.autotune --measure",
         "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
     }
+    if os.path.exists(OUT):  # keep the end-to-end sweeps recorded beside earlier runs
+        with open(OUT) as f:
+            extra = json.load(f).get("measurements_extra")
+        if extra:
+            out["measurements_extra"] = extra
     with open(OUT, "w") as f:
         json.dump(out, f, indent=1)
     return out

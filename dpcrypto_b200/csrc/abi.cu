@@ -731,7 +731,7 @@ int dpkem_set_tuning(const char *key, int value) {
   if (!key || value < 0) return set_status(DPKEM_EINVAL);
   Tuning &t = tuning();
   const std::string k(key);
-  if (value == 0 && k != "pipe_priority") return set_status(DPKEM_EINVAL);  // the switch alone may be 0
+  if (value == 0 && k != "pipe_priority" && k != "saber_pair_max") return set_status(DPKEM_EINVAL);
   if (k == "thread_block") {
     if (value % 32 || value > 256) return set_status(DPKEM_EINVAL);
     t.thread_block = value;
@@ -745,6 +745,8 @@ int dpkem_set_tuning(const char *key, int value) {
     t.pipe_chunks = std::min(value, kPipeChunks);
   } else if (k == "pipe_priority") {
     t.pipe_priority = value != 0;
+  } else if (k == "saber_pair_max") {
+    t.saber_pair_max = value;
   } else {
     return set_status(DPKEM_EINVAL);
   }

@@ -45,6 +45,7 @@ struct Tuning {
   int mixed_thread_task = 256;  // instances per other thread-level task
   int pipe_chunks = 4;          // chunks (one stream each) of a pipelined host-mode batch, <= 8
   int pipe_priority = 1;        // 1: chunk streams get descending priorities (earlier chunks finish first)
+  int saber_pair_max = 6144;    // largest Saber batch whose prologue runs GenMatrix on lane pairs (0: never)
 };
 Tuning &tuning();
 

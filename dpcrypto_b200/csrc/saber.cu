@@ -10,18 +10,28 @@ using sdev::inst_of;
 using sdev::PL;
 using sdev::Scr;
 
-// blockDim 96, 32 instances: warp 0 = hash chain + GenSecret XOF (a thread per instance),
-// warps 1-2 = GenMatrix XOF (a lane pair per instance).
-template <int L, int OP>
+// 32 instances per block.  Warp 0 = hash chain + GenSecret XOF (a thread per instance);
+// GenMatrix XOF on warp 1 (a thread per instance, PAIR = false, blockDim 64) or on warps 1-2
+// (a lane pair per instance, PAIR = true, blockDim 96).  Pairs shorten the longest chain
+// while the batch leaves SM sub-partitions idle, and cost more issue slots per state once
+// it does not (tuning knob saber_pair_max).
+template <int L, int OP, bool PAIR>
 __global__ void __launch_bounds__(96) prologue_kernel(SaberBatch b) {
-  if (threadIdx.x < 32) {
-    const int i = blockIdx.x * 32 + threadIdx.x;
-    if (i < b.n) sdev::prologue_inst<L, OP>(inst_of<L>(b, i, OP), 0);
+  if (!PAIR || threadIdx.x < 32) {
+    const int i = blockIdx.x * 32 + (threadIdx.x & 31);
+    if (i < b.n) sdev::prologue_inst<L, OP>(inst_of<L>(b, i, OP), threadIdx.x >> 5);
     return;
   }
   const int t = threadIdx.x - 32, i = blockIdx.x * 32 + (t >> 1);
   const bool live = i < b.n;
   sdev::matrix_pair<L, OP>(inst_of<L>(b, live ? i : b.n - 1, OP), t & 1, live);
+}
+
+template <int L, int OP>
+void launch_prologue(const SaberBatch &b, cudaStream_t st) {
+  const int pb = (b.n + 31) / 32;
+  if (b.n <= tuning().saber_pair_max) prologue_kernel<L, OP, true><<<pb, 96, 0, st>>>(b);
+  else prologue_kernel<L, OP, false><<<pb, 64, 0, st>>>(b);
 }
 
 template <int L, int OP>
@@ -94,19 +104,19 @@ inline void mark(const SaberBatch &b, cudaStream_t st) {
 template <int L>
 cudaError_t run(const SaberBatch &b, int op, int form, cudaStream_t st) {
   const int tb = tuning().thread_block;
-  const int pb = (b.n + 31) / 32, fb = (b.n + tb - 1) / tb;
+  const int fb = (b.n + tb - 1) / tb;
   cudaError_t e;
   mark(b, st);
   switch (op) {
     case OP_KEYPAIR:
-      prologue_kernel<L, OP_KEYPAIR><<<pb, 96, 0, st>>>(b);
+      launch_prologue<L, OP_KEYPAIR>(b, st);
       mark(b, st);
       if ((e = launch_product<L, sdev::PM_KEYPAIR>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
       finish_kernel<L, OP_KEYPAIR><<<fb, tb, 0, st>>>(b);
       break;
     case OP_ENC:
-      prologue_kernel<L, OP_ENC><<<pb, 96, 0, st>>>(b);
+      launch_prologue<L, OP_ENC>(b, st);
       mark(b, st);
       if ((e = launch_product<L, sdev::PM_ENC>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
@@ -115,7 +125,7 @@ cudaError_t run(const SaberBatch &b, int op, int form, cudaStream_t st) {
     default:
       if ((e = launch_product<L, sdev::PM_DEC_INNER>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
-      prologue_kernel<L, OP_DEC><<<pb, 96, 0, st>>>(b);
+      launch_prologue<L, OP_DEC>(b, st);
       mark(b, st);
       if ((e = launch_product<L, sdev::PM_DEC_CMP>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);

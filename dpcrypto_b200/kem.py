@@ -132,7 +132,7 @@ def load() -> ctypes.CDLL:
 
 TUNING_PATH = os.path.join(HERE, "tuning.json")
 RUNTIME_KNOBS = ("thread_block", "mixed_frodo_task", "mixed_pair_task", "mixed_thread_task", "pipe_chunks",
-                 "pipe_priority")
+                 "pipe_priority", "saber_pair_max")
 
 
 _tuning: dict = {}

@@ -59,3 +59,26 @@ def test_no_silent_fallback_without_device():
         pytest.skip("a GPU is present")
     with pytest.raises(d.DpkemError):
         d.Engine(0)
+
+
+def test_tuning_knobs():
+    """Every knob the autotuner writes is accepted within its range; unknown keys and values
+    out of range are rejected (dpkem_set_tuning is host-only)."""
+    from dpcrypto_b200 import kem
+
+    lib = kem.load()
+    saved = kem.get_tuning()
+    try:
+        for k in kem.RUNTIME_KNOBS:
+            assert lib.dpkem_set_tuning(k.encode(), 32 if k == "thread_block" else 1) == kem.OK, k
+        assert lib.dpkem_set_tuning(b"saber_pair_max", 0) == kem.OK  # 0 = one lane per state always
+        assert lib.dpkem_set_tuning(b"pipe_priority", 0) == kem.OK
+        assert lib.dpkem_set_tuning(b"thread_block", 0) == kem.EINVAL
+        assert lib.dpkem_set_tuning(b"thread_block", 48) == kem.EINVAL
+        assert lib.dpkem_set_tuning(b"saber_pair_max", -1) == kem.EINVAL
+        assert lib.dpkem_set_tuning(b"no_such_knob", 1) == kem.EINVAL
+    finally:
+        defaults = {"thread_block": 64, "mixed_frodo_task": 256, "mixed_pair_task": 128, "mixed_thread_task": 256,
+                    "pipe_chunks": 4, "pipe_priority": 1, "saber_pair_max": 6144}
+        for k in kem.RUNTIME_KNOBS:
+            lib.dpkem_set_tuning(k.encode(), saved.get(k, defaults[k]))

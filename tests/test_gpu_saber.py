@@ -42,3 +42,26 @@ def test_saber_reference_fixture(engine, oracle, saber_tv, form):
     ct_o, ss_o = oracle.enc(3, pk, buf)
     assert (ct == ct_o).all() and (ss == ss_o).all()
     assert (engine.dec(d.SABER, ct, sk, form) == ss).all()
+
+
+@pytest.mark.parametrize("level", LEVELS)
+@pytest.mark.parametrize("pair_max", [0, 1 << 30])
+def test_saber_prologue_lanes_per_state(engine, oracle, level, pair_max):
+    """GenMatrix on one lane per state and on a lane pair (the saber_pair_max knob) give the
+    oracle's bytes, a partial last warp included."""
+    from dpcrypto_b200 import kem
+
+    before = kem.get_tuning().get("saber_pair_max", 6144)
+    kem.set_tuning("saber_pair_max", pair_max)
+    try:
+        n = 45
+        kc, ec = oracle.coins(n, 96, "kp", first=77), oracle.coins(n, 32, "enc", first=77)
+        pk_o, sk_o = oracle.keypair(level, kc, threads=8)
+        ct_o, ss_o = oracle.enc(level, pk_o, ec, threads=8)
+        pk, sk = engine.keypair(level, kc, d.FORM_TC)
+        assert (pk == pk_o).all() and (sk == sk_o).all()
+        ct, ss = engine.enc(level, pk_o, ec, d.FORM_TC)
+        assert (ct == ct_o).all() and (ss == ss_o).all()
+        assert (engine.dec(level, ct_o, sk_o, d.FORM_TC) == ss_o).all()
+    finally:
+        kem.set_tuning("saber_pair_max", before)
