@@ -550,7 +550,11 @@ def main():
                 srv = Server(slots=4, max_batch=4096, form=f, classes=classes)
                 try:
                     srv.run(pool, np.zeros(2048))  # warm-up
-                    peak = srv.run(pool, np.zeros(pool.n))["ops_per_s"]
+                    peaks = []
+                    for _ in range(2):  # best of two saturated runs: one host or device hiccup
+                        pool.clear()    # would otherwise scale every load level down
+                        peaks.append(srv.run(pool, np.zeros(pool.n))["ops_per_s"])
+                    peak = max(peaks)
                     levels = []
                     for frac in (0.1, 0.25, 0.5, 0.75, 1.0):
                         pool.clear()
