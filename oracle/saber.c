@@ -15,7 +15,7 @@
  *  - encaps flow (m = SHA3-256(coins), kr = SHA3-512(m||H(pk)), enc with kr[32:],
  *    k = SHA3-256(kr[0:32]||SHA3-256(c))): SABER-GPU/src/cuda_kernel.cu:19-153
  *  - decaps flow: cuda_kernel.cu:155-299, in the specification order (cmov of z
- *    before the final hash; the reference hashes first, SURVEY defect D12)
+ *    before the final hash; the reference hashes first, cuda_kernel.cu:272-273)
  *  - LSB-first bit packing at 13/10/eT/1 bits: pack.cu:8-212
  *  - keygen uses the transposed product (b = A^T s), encaps the plain one.
  */
