@@ -39,7 +39,7 @@ enum {
   DPKEM_ENOMEM = -2,       /* allocation failed or the request exceeds the HBM budget */
   DPKEM_ECUDA = -3,        /* a CUDA runtime call failed */
   DPKEM_ETIMEOUT = -4,     /* a bounded device wait expired (the kernel unwound) */
-  DPKEM_EUNSUPPORTED = -5, /* valid request this build does not implement */
+  DPKEM_EUNSUPPORTED = -5, /* valid request the library does not implement */
   DPKEM_EAGAIN = -6        /* non-blocking ring call: nothing to take / no room yet (dpkem_wire.h) */
 };
 
