@@ -95,9 +95,10 @@ def test_reference_named_shims(oracle):
     d.set_compat(batch=768)
 
 
-@pytest.mark.parametrize("scheme,n", [(d.SABER, 1100), (d.FRODO976, 600)])
+@pytest.mark.parametrize("scheme,n", [(d.SABER, 1100), (d.FRODO976, 600), (d.FRODO976, 1100)])
 def test_host_pipeline_matches_device_mode(engine, oracle, scheme, n):
-    """Host-mode batches of several chunks run on a two-stream copy/compute pipeline."""
+    """Host-mode batches of several chunks run as a copy/compute pipeline, one stream per
+    chunk (600: two equal chunks; 1100: four, the first and last a quarter of the others)."""
     z = d.sizes(scheme)
     kc, ec = oracle.coins(n, z["kp_coins"], "kp", first=77), oracle.coins(n, z["enc_coins"], "enc", first=77)
     pk, sk = engine.keypair(scheme, kc, d.FORM_TC)
