@@ -34,6 +34,14 @@ void launch_prologue(const SaberBatch &b, cudaStream_t st) {
   else prologue_kernel<L, OP, false><<<pb, 64, 0, st>>>(b);
 }
 
+// Encaps finish on lane pairs, 64 threads = 32 instances.
+template <int L>
+__global__ void __launch_bounds__(64) finish_enc_pair_kernel(SaberBatch b) {
+  const int t = blockIdx.x * 64 + threadIdx.x, i = t >> 1;
+  const bool live = i < b.n;
+  sdev::finish_enc_pair<L>(inst_of<L>(b, live ? i : b.n - 1, OP_ENC), t & 1, live);
+}
+
 template <int L, int OP>
 __global__ void __launch_bounds__(256) finish_kernel(SaberBatch b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -120,7 +128,8 @@ cudaError_t run(const SaberBatch &b, int op, int form, cudaStream_t st) {
       mark(b, st);
       if ((e = launch_product<L, sdev::PM_ENC>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
-      finish_kernel<L, OP_ENC><<<fb, tb, 0, st>>>(b);
+      if (b.n <= tuning().saber_pair_max) finish_enc_pair_kernel<L><<<(b.n + 31) / 32, 64, 0, st>>>(b);
+      else finish_kernel<L, OP_ENC><<<fb, tb, 0, st>>>(b);
       break;
     default:
       if ((e = launch_product<L, sdev::PM_DEC_INNER>(b, form, st)) != cudaSuccess) return e;

@@ -251,6 +251,32 @@ __device__ __forceinline__ void matrix_pair(const Inst &v, int p, bool live) {
   kpair::squeeze<168>(a, v.scr + S::ARAW, P::ARAW, p, live);
 }
 
+// Encaps finish on a lane pair: k = SHA3-256(kr[0:32] || SHA3-256(c)), the same bytes as
+// finish_inst<L, OP_ENC>; 10 dependent permutations at l = 3.
+template <int L>
+__device__ __forceinline__ void finish_enc_pair(const Inst &v, int p, bool live) {
+  using P = SP<L>;
+  using S = Scr<L>;
+  uint32_t a[25], hc[4];
+  kpair::zero(a);
+  const int pos = kpair::absorb_aligned<136>(a, 0, v.ct, P::CT, p);
+  kpair::absorb_finish<136>(a, pos, 0x06u, p);
+#pragma unroll
+  for (int q = 0; q < 4; q++) hc[q] = a[q];
+  kpair::zero(a);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    a[q] = kpair::to_slice(ld_lane(v.scr + S::KR + 8 * q), p);
+    a[4 + q] = hc[q];
+  }
+  kpair::absorb_finish<136>(a, 64, 0x06u, p);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const uint32_t h = kpair::from_slice(a[q], p);
+    if (live) *reinterpret_cast<uint32_t *>(v.ss + 8 * q + 4 * p) = h;
+  }
+}
+
 // ---------------------------------------------------------------- finish
 template <int L, int OP>
 __device__ __forceinline__ void finish_inst(const Inst &v) {
