@@ -785,8 +785,10 @@ void dpkem_set_compat_batch(size_t n) { g_compat_batch = n; }
 void dpkem_set_compat_saber_level(int l) { g_compat_level = l; }
 void dpkem_set_compat_form(int form) { g_compat_form = form; }
 
+// The reference's mode byte (0 = DP, anything else INT32: SABER-GPU/src/cuda_kernel.cu:80,106)
+// as 0 / 1, plus 2 for the tensor-core form; any other value is rejected (-1).
 static int compat_form_from_mode(uint8_t mode) {
-  return mode == 0 ? DPKEM_FORM_DP4A : mode == 2 ? DPKEM_FORM_TC : DPKEM_FORM_INT32;
+  return mode == 0 ? DPKEM_FORM_DP4A : mode == 1 ? DPKEM_FORM_INT32 : mode == 2 ? DPKEM_FORM_TC : -1;
 }
 
 void frodoKEMKeypair(uint8_t *h_pk, uint8_t *h_sk) {
@@ -816,6 +818,7 @@ void frodoKEMDecap(uint8_t *ss, const uint8_t *ct, const uint8_t *sk) {
 }
 
 void saber_enc(uint8_t mode, uint8_t *h_k, uint8_t *h_pk, uint8_t *h_c) {
+  if (compat_form_from_mode(mode) < 0) return (void)set_status(DPKEM_EINVAL);
   dpkem_ctx *c = compat_ctx();
   if (!c) return (void)set_status(DPKEM_ECUDA);
   std::vector<uint8_t> coins(g_compat_batch * 32);
@@ -828,6 +831,7 @@ void saber_enc(uint8_t mode, uint8_t *h_k, uint8_t *h_pk, uint8_t *h_c) {
 
 void saber_dec(uint8_t mode, uint8_t *h_c, uint8_t *h_pk, uint8_t *h_sk, uint8_t *h_k) {
   (void)h_pk;  // the public key travels inside sk
+  if (compat_form_from_mode(mode) < 0) return (void)set_status(DPKEM_EINVAL);
   dpkem_ctx *c = compat_ctx();
   if (!c) return (void)set_status(DPKEM_ECUDA);
   set_status(dpkem_dec_batch(c, g_compat_level, compat_form_from_mode(mode), g_compat_batch, h_c, h_sk, h_k, 0, nullptr));

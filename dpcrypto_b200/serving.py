@@ -40,6 +40,7 @@ class RequestPool:
         self.table = np.zeros(n, REQ_DTYPE)
         self.expected, self.outputs = [], []
         self.kind = np.zeros(n, np.int32)  # scheme * 3 + op
+        self._views = [None] * n
         for scheme, mask in ((K.FRODO976, is_frodo), (K.SABER, ~is_frodo)):
             z = K.sizes(scheme)
             idx_enc = np.nonzero(mask & is_enc)[0]
@@ -74,6 +75,10 @@ class RequestPool:
             t["out0"][idx_dec], t["out1"][idx_dec] = rows(oss, j_dec), 0
             self.kind[idx_enc] = scheme * 3 + 1
             self.kind[idx_dec] = scheme * 3 + 2
+            for j, r in enumerate(idx_enc):
+                self._views[r] = (scheme, 1, ec[j], pk[j], oct_[j], oss[j])
+            for j, r in zip(j_dec, idx_dec):
+                self._views[r] = (scheme, 2, ct[j], sk[j], oss[j], None)
 
     def clear(self):
         for t in self.outputs:
@@ -81,6 +86,11 @@ class RequestPool:
 
     def check(self) -> bool:
         return all(torch.equal(got, ref) for got, ref in self.expected)
+
+    def items(self) -> list:
+        """Request i as (scheme, op, in0, in1, out0, out1) device tensors, in the order the
+        mixed entry points take them (out1 None for decaps)."""
+        return list(self._views)
 
 
 FRODO_CLASS, SABER_CLASS = 0, 1

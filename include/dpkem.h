@@ -160,11 +160,13 @@ int dpkem_probe_i8_mma_peak(dpkem_ctx *ctx, double *macs_per_s);
  * quota applies).  Scratch is a fixed __device__ array inside the library, sized for
  * DPKEM_SABER_ENC_STATIC_MAX instances (about 3.9 MB, held on every GPU that loads the
  * library until exit); n above that returns DPKEM_EINVAL.  coins, pk, ct, ss are device
- * pointers (8-byte aligned), laid out as in dpkem_enc_batch; stream NULL is the legacy
- * default stream.  The call returns when the work has finished.  The first call on each
- * device resolves the array's address (make it before any stream capture).  All calls on
- * a device share the array: the library serialises its own calls, and work that overlaps
- * them on the GPU would race. */
+ * pointers (8-byte aligned) on the device that owns `stream`, laid out as in
+ * dpkem_enc_batch; stream NULL is the current device's legacy default stream.  The call
+ * returns when the work has finished and records its status for dpkem_last_status().
+ * The first call on each device (and again after a device reset) resolves the array's
+ * address on that device (make it before any stream capture).  All calls on a device
+ * share the array: the library serialises its own calls per device, and work that
+ * overlaps them on the GPU would race. */
 #define DPKEM_SABER_ENC_STATIC_MAX 512
 int dpkem_saber_enc_batch_static(int scheme, int form, size_t n, const uint8_t *coins, const uint8_t *pk,
                                  uint8_t *ct, uint8_t *ss, void *stream);
@@ -191,7 +193,9 @@ void dpkem_set_compat_form(int form);      /* default DPKEM_FORM_TC */
 void frodoKEMKeypair(uint8_t *h_pk, uint8_t *h_sk);
 void frodoKEMEncap(uint8_t *ct, uint8_t *ss, const uint8_t *pk);
 void frodoKEMDecap(uint8_t *ss, const uint8_t *ct, const uint8_t *sk);
-/* Reference: keys from tv.h, overwriting h_pk / h_sk.  Here caller data is used as given. */
+/* Reference: keys from tv.h, overwriting h_pk / h_sk.  Here caller data is used as given.
+ * mode 0 = dp4a, 1 = INT32, 2 = tcgen05; any other mode computes nothing and records
+ * DPKEM_EINVAL (the reference runs its INT32 path for every mode other than 0). */
 void saber_enc(uint8_t mode, uint8_t *h_k, uint8_t *h_pk, uint8_t *h_c);
 void saber_dec(uint8_t mode, uint8_t *h_c, uint8_t *h_pk, uint8_t *h_sk, uint8_t *h_k);
 

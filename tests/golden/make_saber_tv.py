@@ -5,8 +5,8 @@ keypair with GenMatrix output, encaps coins, the message and the encaps secret.
 This script parses those C array initialisers as data and stores them as numpy
 arrays, so the tests never need the reference tree at run time.
 
-Run (in a container that has the reference mounted):
-    python tests/golden/make_saber_tv.py /root/reference/SABER-GPU/include/tv.h
+Run where the reference tree is present, giving the path of its tv.h:
+    python tests/golden/make_saber_tv.py <reference>/SABER-GPU/include/tv.h
 """
 import os
 import re
@@ -26,7 +26,9 @@ def parse(path: str) -> dict:
 
 
 def main() -> None:
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/SABER-GPU/include/tv.h"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_saber_tv.py <path of SABER-GPU/include/tv.h>")
+    src = sys.argv[1]
     arrays = parse(src)
     expected = {"A": 2304, "sp": 768, "pk": 992, "m_tv": 32, "sk_tv": 2304, "buf_tv": 64}
     for k, n in expected.items():

@@ -83,15 +83,24 @@ def test_reference_named_shims(oracle):
     d.frodoKEMDecap(ssa, ct, sk)
     assert (ssa == ssb).all()
     spk, ssk = oracle.keypair(3, oracle.coins(n, 96, "kp"), threads=4)
-    k_enc, c = np.zeros((n, 32), np.uint8), np.zeros((n, 1088), np.uint8)
-    c0 = None
+    # the shims draw their encaps coins from the same seeded stream (instances 0..n-1, "enc")
+    c_o, k_o = oracle.enc(3, spk, oracle.coins(n, 32, "enc"), threads=4)
     for mode in (0, 1, 2):  # the reference's modes: 0 dp4a, 1 INT32 schoolbook, 2 tensor cores
+        k_enc, c = np.zeros((n, 32), np.uint8), np.zeros((n, 1088), np.uint8)
         d.saber_enc(mode, k_enc, spk, c)
+        assert (c == c_o).all() and (k_enc == k_o).all(), mode
         k_dec = np.zeros((n, 32), np.uint8)
         d.saber_dec(mode, c, spk, ssk, k_dec)
-        assert (k_dec == k_enc).all()
-        c0 = c.copy() if c0 is None else c0
-        assert (c == c0).all()  # the compat coins are fixed, so every mode gives the same ciphertext
+        assert (k_dec == k_o).all(), mode
+    # a mode byte the reference does not define is rejected and nothing is written
+    for mode in (3, 7, 255):
+        k_enc, c = np.zeros((n, 32), np.uint8), np.zeros((n, 1088), np.uint8)
+        with pytest.raises(d.DpkemError) as e:
+            d.saber_enc(mode, k_enc, spk, c)
+        assert e.value.status == d.kem.EINVAL and not c.any() and not k_enc.any()
+        with pytest.raises(d.DpkemError) as e:
+            d.saber_dec(mode, c_o, spk, ssk, k_enc)
+        assert e.value.status == d.kem.EINVAL and not k_enc.any()
     d.set_compat(batch=768)
 
 

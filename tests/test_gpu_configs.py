@@ -103,7 +103,7 @@ def test_frodo_8192_spot_and_forms(engine, oracle):
 
 
 @pytest.mark.parametrize("form", FORMS)
-def test_mixed_16384(engine, form):
+def test_mixed_16384(engine, form, oracle_check_items):
     from dpcrypto_b200.workloads import MixedBatch
 
     mb = MixedBatch(engine, 16384, seed=3)
@@ -111,3 +111,5 @@ def test_mixed_16384(engine, form):
     engine.sync()
     torch.cuda.synchronize()
     assert mb.check()
+    # a stride sample (every scheme and op) recomputed by the oracle from the request inputs
+    assert oracle_check_items(mb.items, stride=97, offset=FORMS.index(form)) >= 160

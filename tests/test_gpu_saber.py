@@ -65,3 +65,72 @@ def test_saber_prologue_lanes_per_state(engine, oracle, level, pair_max):
         assert (engine.dec(level, ct_o, sk_o, d.FORM_TC) == ss_o).all()
     finally:
         kem.set_tuning("saber_pair_max", before)
+
+
+def _unpack13(b):
+    bits = np.unpackbits(b, bitorder="little").reshape(-1, 13)
+    return (bits.astype(np.int64) << np.arange(13)).sum(axis=1)
+
+
+def _pack(v, width):
+    bits = ((np.asarray(v, np.int64)[:, None] >> np.arange(width)) & 1).astype(np.uint8)
+    return np.packbits(bits.ravel(), bitorder="little")
+
+
+def _keypair_with_secret(oracle, level, seed_a, s, z):
+    """A Saber key pair for a given secret vector s (centred integers), built from the
+    oracle's GenMatrix and matrix-vector product: b = ((A^T s + h1) >> 3) mod 2^10,
+    pk = pack10(b) || seed_A, sk = pack13(s) || pk || SHA3-256(pk) || z."""
+    a = oracle.saber_genmatrix(level, seed_a)
+    b = oracle.saber_matvec(level, a, (np.asarray(s) % 65536).astype(np.uint16), True)
+    b = ((b.astype(np.int64) + 4) >> 3) & 0x3FF
+    pk = np.concatenate([_pack(b, 10), np.frombuffer(seed_a, np.uint8)])
+    sk = np.concatenate([_pack(np.asarray(s) % 8192, 13), pk, np.frombuffer(oracle.sha3_256(pk.tobytes()), np.uint8),
+                         np.frombuffer(z, np.uint8)])
+    return pk, sk
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("level", LEVELS)
+def test_saber_malformed_secret_key(engine, oracle, level, form):
+    """Secret keys whose secret coefficients lie outside the CBD range [-mu/2, mu/2] (a
+    malformed sk; key generation never makes one).  Every form reads a secret coefficient as
+    the low byte of its 13-bit field, sign-extended (the reference's DP path reads int8
+    secrets the same way, SABER-GPU/src/poly.cu:56-68).  Recorded here:
+    - coefficients inside [-128, 127]: the oracle's bytes, and decapsulation succeeds when the
+      key pair was built for that secret (the secret is read exactly);
+    - larger coefficients: the oracle's bytes for the key whose coefficients are replaced by
+      their low byte."""
+    n = 12
+    kc, ec = oracle.coins(n, 96, "kp", first=31), oracle.coins(n, 32, "enc", first=31)
+    rng = np.random.default_rng(level)
+    mu_half = {2: 5, 3: 4, 4: 3}[level]
+    nsec = 416 * level  # packed secret bytes at the start of sk
+    pks, sks, wide, wide_lo = [], [], [], []
+    for i in range(n):
+        s = oracle.saber_gensecret(level, kc[i, 32:64].tobytes()).astype(np.int64)
+        s = ((s + 4096) % 8192) - 4096  # centred
+        pos = rng.choice(s.size, size=1 + i % 6, replace=False)
+        # a few coefficients just outside the CBD range (small enough that decryption succeeds)
+        s[pos] = rng.integers(mu_half + 1, mu_half + 12, size=pos.size) * rng.choice([-1, 1], size=pos.size)
+        seed_a = oracle.shake128(kc[i, :32].tobytes(), 32)  # seed_A as key generation derives it
+        pk, sk = _keypair_with_secret(oracle, level, seed_a, s, kc[i, 64:96].tobytes())
+        pks.append(pk)
+        sks.append(sk)
+        w = s.copy()
+        big = rng.integers(128, 4096, size=pos.size) * rng.choice([-1, 1], size=pos.size)
+        w[pos] = big
+        wk = sk.copy()
+        wk[:nsec] = _pack(w % 8192, 13)
+        wide.append(wk)
+        w[pos] = ((big + 128) % 256) - 128  # the sign-extended low byte
+        lk = sk.copy()
+        lk[:nsec] = _pack(w % 8192, 13)
+        wide_lo.append(lk)
+    pk, sk, wide, wide_lo = (np.stack(x) for x in (pks, sks, wide, wide_lo))
+    ct, ss = oracle.enc(level, pk, ec, threads=8)
+    assert (oracle.dec(level, ct, sk, threads=8) == ss).all()  # the malformed key pairs work
+    assert (engine.dec(level, ct, sk, form) == ss).all()
+    ct_g, ss_g = engine.enc(level, pk, ec, form)
+    assert (ct_g == ct).all() and (ss_g == ss).all()
+    assert (engine.dec(level, ct, wide, form) == oracle.dec(level, ct, wide_lo, threads=8)).all()

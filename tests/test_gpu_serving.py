@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("form", [d.FORM_TC, d.FORM_DP4A])
-def test_serving_results_equal_alone(engine, form):
+def test_serving_results_equal_alone(engine, form, oracle_check_items):
     pool = RequestPool(engine, 700, seed=3)
     srv = Server(slots=3, max_batch=128, form=form, hbm_budget=256 << 20)
     try:
@@ -20,10 +20,11 @@ def test_serving_results_equal_alone(engine, form):
         srv.close()
     torch.cuda.synchronize()
     assert pool.check()
+    assert oracle_check_items(pool.items(), stride=11) >= 60
     assert res["batches"] > 1 and np.isfinite(res["latency_ms"]).all() and (res["latency_ms"] > 0).all()
 
 
-def test_serving_split_classes(engine):
+def test_serving_split_classes(engine, oracle_check_items):
     """Frodo and Saber requests on separate slots: results unchanged, Saber requests no
     longer wait for Frodo batches."""
     from dpcrypto_b200.serving import FRODO_CLASS, SABER_CLASS
@@ -37,5 +38,6 @@ def test_serving_split_classes(engine):
         srv.close()
     torch.cuda.synchronize()
     assert pool.check()
+    assert oracle_check_items(pool.items(), stride=13, offset=5) >= 40
     assert np.isfinite(res["latency_ms"]).all()
     assert res["saber_p50_ms"] < res["frodo_p50_ms"]
