@@ -28,6 +28,12 @@ def build() -> str:
     return _LIB_PATH
 
 
+def build_ref() -> None:
+    """Build oracle/_ref (the reference's own kernels as host C++, oracle/ref/Makefile) when
+    the reference tree is on this machine; a no-op elsewhere.  Checker code only."""
+    subprocess.run(["make", "-s", "-C", os.path.join(_HERE, "ref")], check=True)
+
+
 def lib():
     global _lib
     if _lib is None:

@@ -1,0 +1,3 @@
+/* Stand-in for <cuda_fp16.h> when the reference kernels are compiled as host C++ (cuda_emu.h). */
+#pragma once
+#include "../cuda_emu.h"
