@@ -30,7 +30,8 @@ typedef struct {
   int squeezing;
 } oracle_sponge;
 
-void oracle_keccak_f1600(uint64_t a[25]);
+void oracle_keccak_f1600(uint64_t a[25]);        /* unrolled, used by the sponge */
+void oracle_keccak_f1600_plain(uint64_t a[25]);  /* loop form, the cross-check */
 void oracle_sponge_init(oracle_sponge *s, unsigned rate, uint8_t domain);
 void oracle_sponge_absorb(oracle_sponge *s, const uint8_t *in, size_t len);
 void oracle_sponge_squeeze(oracle_sponge *s, uint8_t *out, size_t len);

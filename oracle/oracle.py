@@ -14,7 +14,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_NATIVE_PATH = os.path.join(_HERE, "_build", "native", "liboracle.so")
 _lib = None
+_native = False
 
 FRODO = 0
 FRODO_AES = 1
@@ -34,14 +36,29 @@ def build_ref() -> None:
     subprocess.run(["make", "-s", "-C", os.path.join(_HERE, "ref")], check=True)
 
 
+def use_native() -> str:
+    """Switch this process to the CPU-baseline build of the oracle: the same sources compiled
+    with -march=native on (and for) this machine, built here on first use.  Call before the
+    first oracle call; the portable build stays the one the tests check."""
+    global _native
+    if _lib is not None and not _native:
+        raise RuntimeError("use_native() must come before the first oracle call")
+    subprocess.run(["make", "-s", "-C", _HERE, "native"], check=True)
+    _native = True
+    return _NATIVE_PATH
+
+
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB_PATH):
+        path = _NATIVE_PATH if _native else _LIB_PATH
+        if not os.path.exists(path):
             build()
-        L = ctypes.CDLL(_LIB_PATH)
+        L = ctypes.CDLL(path)
         u8p = ctypes.c_void_p
         for name, args in {
+            "oracle_keccak_f1600": [u8p],
+            "oracle_keccak_f1600_plain": [u8p],
             "oracle_shake128": [u8p, ctypes.c_size_t, u8p, ctypes.c_size_t],
             "oracle_shake256": [u8p, ctypes.c_size_t, u8p, ctypes.c_size_t],
             "oracle_sha3_256": [u8p, u8p, ctypes.c_size_t],
@@ -65,7 +82,8 @@ def lib():
         }.items():
             fn = getattr(L, name)
             fn.argtypes = args
-            fn.restype = ctypes.c_int if name not in ("oracle_shake128", "oracle_shake256", "oracle_sha3_256",
+            fn.restype = ctypes.c_int if name not in ("oracle_keccak_f1600", "oracle_keccak_f1600_plain",
+                                                     "oracle_shake128", "oracle_shake256", "oracle_sha3_256",
                                                      "oracle_sha3_512", "oracle_coins_batch",
                                                      "oracle_frodo_gen_row", "oracle_frodo_sample",
                                                      "oracle_frodo_gen_row_aes", "oracle_aes128_ecb",

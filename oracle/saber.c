@@ -81,13 +81,13 @@ static void bitunpack(uint16_t *out, const uint8_t *in, size_t n, int bits) {
 void oracle_saber_polmul_acc(const uint16_t *a, const uint16_t *b, uint16_t *res) {
   uint32_t acc[SN];
   for (int i = 0; i < SN; i++) acc[i] = res[i];
-  for (int i = 0; i < SN; i++)
-    for (int j = 0; j < SN; j++) {
-      uint32_t prod = (uint32_t)a[i] * b[j];
-      int k = i + j;
-      if (k < SN) acc[k] += prod;
-      else acc[k - SN] -= prod;
-    }
+  /* x^i * x^j = x^(i+j), and x^(i+j) = -x^(i+j-256) once i + j wraps: two branch-free
+   * loops per a[i], the second subtracting. */
+  for (int i = 0; i < SN; i++) {
+    const uint32_t ai = a[i];
+    for (int j = 0; j < SN - i; j++) acc[i + j] += ai * b[j];
+    for (int j = SN - i; j < SN; j++) acc[i + j - SN] -= ai * b[j];
+  }
   for (int i = 0; i < SN; i++) res[i] = (uint16_t)acc[i];
 }
 

@@ -23,3 +23,19 @@ def test_coins_stream(oracle):
     for i in range(5):
         ref = hashlib.shake_256(bytes(range(32)) + (7 + i).to_bytes(8, "little") + b"kp").digest(64)
         assert c[i].tobytes() == ref
+
+
+def test_unrolled_permutation_equals_loop_form(oracle):
+    """The sponge's unrolled Keccak-f (constant indices and rotations) against the loop form
+    restated over the (x, y) grid, on random and edge states."""
+    import numpy as np
+
+    lib = oracle.lib()
+    rng = np.random.default_rng(5)
+    states = [np.zeros(25, np.uint64), np.full(25, np.uint64(0xFFFFFFFFFFFFFFFF), np.uint64)]
+    states += [rng.integers(0, 2**63, size=25, dtype=np.uint64) * np.uint64(2) + np.uint64(k & 1) for k in range(300)]
+    for st in states:
+        a, b = st.copy(), st.copy()
+        lib.oracle_keccak_f1600(a.ctypes.data)
+        lib.oracle_keccak_f1600_plain(b.ctypes.data)
+        assert (a == b).all()
