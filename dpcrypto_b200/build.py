@@ -17,7 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdpkem.so")
-SOURCES = ["frodo.cu", "saber.cu", "coins.cu", "peak.cu", "abi.cu", "noalloc.cu", "mixed.cu", "frames.cu"]
+SOURCES = ["frodo.cu", "saber.cu", "coins.cu", "peak.cu", "keccak_lanes.cu", "abi.cu", "noalloc.cu", "mixed.cu",
+           "frames.cu"]
 # The persistent mixed-batch kernel reads data other CTAs wrote in the same launch: its
 # global loads bypass the (non-coherent) L1.
 EXTRA = {"mixed.cu": ["-Xptxas", "-dlcm=cg"]}

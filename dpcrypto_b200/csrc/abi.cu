@@ -711,6 +711,27 @@ int dpkem_probe_int_peaks(dpkem_ctx *c, double *int_ops_per_s, double *keccak_pe
   return set_status(cuda_status(probe_int_peaks(c->stream, int_ops_per_s, keccak_per_s)));
 }
 
+int dpkem_keccak_f1600_lanes(dpkem_ctx *c, int lanes, size_t n, const uint64_t *in, uint64_t *out, int perms) {
+  if (!c || (lanes != 1 && lanes != 2 && lanes != 5) || perms < 0 || n > (size_t)INT32_MAX) return set_status(DPKEM_EINVAL);
+  if (n == 0) return set_status(DPKEM_OK);
+  if (!in || !out || (reinterpret_cast<uintptr_t>(in) & 7) || (reinterpret_cast<uintptr_t>(out) & 7))
+    return set_status(DPKEM_EINVAL);
+  std::lock_guard<std::mutex> lock(c->mu);
+  cudaSetDevice(c->device);
+  cudaError_t e = keccak_lanes(lanes, in, out, (int)n, perms, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return set_status(cuda_status(e));
+}
+
+int dpkem_probe_keccak_chain(dpkem_ctx *c, int lanes, int states, int perms, double *ms) {
+  if (!c || !ms || (lanes != 1 && lanes != 2 && lanes != 5) || states <= 0 || perms <= 0) return set_status(DPKEM_EINVAL);
+  std::lock_guard<std::mutex> lock(c->mu);
+  cudaSetDevice(c->device);
+  cudaError_t e = cudaStreamWaitEvent(c->stream, c->last, 0);
+  if (e == cudaSuccess) e = probe_keccak_chain(lanes, states, perms, c->stream, ms);
+  return set_status(cuda_status(e));
+}
+
 int dpkem_probe_i8_mma_peak(dpkem_ctx *c, double *macs_per_s) {
   if (!c || !macs_per_s) return set_status(DPKEM_EINVAL);
   std::lock_guard<std::mutex> lock(c->mu);
@@ -731,7 +752,9 @@ int dpkem_set_tuning(const char *key, int value) {
   if (!key || value < 0) return set_status(DPKEM_EINVAL);
   Tuning &t = tuning();
   const std::string k(key);
-  if (value == 0 && k != "pipe_priority" && k != "saber_pair_max") return set_status(DPKEM_EINVAL);
+  const bool zero_ok = k == "pipe_priority" || k == "saber_pair_max" || k == "saber_five_max" ||
+                       k == "saber_finish_five_max" || k == "frodo_five_max" || k == "frodo_ss_five_max";
+  if (value == 0 && !zero_ok) return set_status(DPKEM_EINVAL);
   if (k == "thread_block") {
     if (value % 32 || value > 256) return set_status(DPKEM_EINVAL);
     t.thread_block = value;
@@ -747,6 +770,14 @@ int dpkem_set_tuning(const char *key, int value) {
     t.pipe_priority = value != 0;
   } else if (k == "saber_pair_max") {
     t.saber_pair_max = value;
+  } else if (k == "saber_five_max") {
+    t.saber_five_max = value;
+  } else if (k == "saber_finish_five_max") {
+    t.saber_finish_five_max = value;
+  } else if (k == "frodo_five_max") {
+    t.frodo_five_max = value;
+  } else if (k == "frodo_ss_five_max") {
+    t.frodo_ss_five_max = value;
   } else {
     return set_status(DPKEM_EINVAL);
   }

@@ -46,6 +46,10 @@ struct Tuning {
   int pipe_chunks = 4;          // chunks (one stream each) of a pipelined host-mode batch, <= 8
   int pipe_priority = 1;        // 1: chunk streams get descending priorities (earlier chunks finish first)
   int saber_pair_max = 6144;    // largest Saber batch whose prologue runs GenMatrix on lane pairs (0: never)
+  int saber_five_max = 8192;    // largest Saber batch whose prologue sponges run on five lanes per state (0: never)
+  int saber_finish_five_max = 8192;  // the same for the encaps / keypair finish
+  int frodo_five_max = 0;       // largest Frodo batch whose prologues run on five lanes per state (0: never)
+  int frodo_ss_five_max = 0;    // the same for H(pk) and the final hash
 };
 Tuning &tuning();
 
@@ -107,6 +111,10 @@ cudaError_t saber_dec(const SaberBatch &b, int form, cudaStream_t st);
 size_t saber_scratch_bytes(int level);
 cudaError_t coins_generate(const CoinsBatch &b, cudaStream_t st);
 cudaError_t probe_int_peaks(cudaStream_t st, double *int_ops_per_s, double *keccak_per_s);
+// keccak_lanes.cu: `perms` Keccak-f[1600] permutations on each of n states (25 LE lanes each)
+// with 1, 2 or 5 lanes per state; and the device time of such a dependent chain.
+cudaError_t keccak_lanes(int lanes, const uint64_t *in, uint64_t *out, int n, int perms, cudaStream_t st);
+cudaError_t probe_keccak_chain(int lanes, int n, int perms, cudaStream_t st, double *ms);
 // int8 tcgen05 MMA throughput (MACs/s) of the device; err receives DEV_ERR_TIMEOUT if the
 // probe's bounded wait expires.
 cudaError_t probe_i8_mma_peak(cudaStream_t st, uint32_t *err, double *macs_per_s);

@@ -69,6 +69,10 @@ EXPORTS = {
     "dpkem_probe_int_peaks": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_double)]),
     "dpkem_probe_i8_mma_peak": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    "dpkem_keccak_f1600_lanes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_int]),
+    "dpkem_probe_keccak_chain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.POINTER(ctypes.c_double)]),
     "dpkem_saber_enc_batch_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_void_p]),
@@ -132,7 +136,8 @@ def load() -> ctypes.CDLL:
 
 TUNING_PATH = os.path.join(HERE, "tuning.json")
 RUNTIME_KNOBS = ("thread_block", "mixed_frodo_task", "mixed_pair_task", "mixed_thread_task", "pipe_chunks",
-                 "pipe_priority", "saber_pair_max")
+                 "pipe_priority", "saber_pair_max", "saber_five_max", "saber_finish_five_max", "frodo_five_max",
+                 "frodo_ss_five_max")
 
 
 _tuning: dict = {}
@@ -312,6 +317,24 @@ class Engine:
         """int8 tcgen05 MMA multiply-adds per second (one CTA per SM, back-to-back MMAs)."""
         v = ctypes.c_double()
         self._check(self._lib.dpkem_probe_i8_mma_peak(self._h, ctypes.byref(v)), "probe_i8_mma_peak")
+        return v.value
+
+    def keccak_lanes(self, lanes: int, states, perms: int = 1):
+        """`perms` Keccak-f[1600] permutations of each row of `states` (an n x 25 torch CUDA
+        tensor of 64-bit lanes) in the given lanes-per-state layout (1, 2 or 5); returns a new
+        tensor.  The calling torch stream's pending work is synchronised first."""
+        import torch
+
+        torch.cuda.current_stream(states.device).synchronize()
+        out = states.new_empty(states.shape)
+        self._check(self._lib.dpkem_keccak_f1600_lanes(self._h, lanes, states.shape[0], ctypes.c_void_p(states.data_ptr()),
+                                                      ctypes.c_void_p(out.data_ptr()), perms), "keccak_lanes")
+        return out
+
+    def probe_keccak_chain(self, lanes: int, states: int, perms: int) -> float:
+        """Device ms of `perms` dependent permutations on each of `states` states."""
+        v = ctypes.c_double()
+        self._check(self._lib.dpkem_probe_keccak_chain(self._h, lanes, states, perms, ctypes.byref(v)), "probe_keccak_chain")
         return v.value
 
     def probe_int_peaks(self):

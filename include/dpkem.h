@@ -154,6 +154,16 @@ int dpkem_probe_int_peaks(dpkem_ctx *ctx, double *int_ops_per_s, double *keccak_
  * tcgen05.mma kind::i8 (u8 x s8, s32 accumulators in TMEM); int8 multiply-adds per second. */
 int dpkem_probe_i8_mma_peak(dpkem_ctx *ctx, double *macs_per_s);
 
+/* Keccak-f[1600] in each lanes-per-state layout the sponge stages use (1: a thread per state,
+ * 2: a bit-interleaved lane pair, 5: five lanes of a warp per state): `perms` permutations
+ * applied to each of n states (25 little-endian 64-bit lanes each, device pointers, 8-byte
+ * aligned); returns when done.  No counterpart in the reference (its permutation is
+ * KeccakF1600_StatePermute, FrodoKEM976-GPU/src/shake.cu:66-331, one thread per state). */
+int dpkem_keccak_f1600_lanes(dpkem_ctx *ctx, int lanes, size_t n, const uint64_t *in, uint64_t *out, int perms);
+/* Device time (ms, CUDA events) of `perms` dependent permutations on each of `states` states
+ * in the given layout: the latency of a sponge chain per layout and batch size. */
+int dpkem_probe_keccak_chain(dpkem_ctx *ctx, int lanes, int states, int perms, double *ms);
+
 /* Saber encapsulation that allocates no device memory (no counterpart in the reference).
  * For callers that may not call cudaMalloc on their request path (allocator calls are
  * forbidden there, all device memory belongs to a host framework, or a fixed memory

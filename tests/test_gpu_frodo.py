@@ -54,3 +54,31 @@ def test_frodo_forms_agree_at_scale(engine, oracle):
     assert (pk[idx] == pk_o).all()
     ct_o, ss_o = oracle.enc(0, pk[idx], ec[idx], threads=3)
     assert (ct[idx] == ct_o).all() and (ss[idx] == ss_o).all()
+
+
+@pytest.mark.parametrize("form", [d.FORM_TC, d.FORM_DP4A])
+def test_frodo_sponges_on_five_lanes(engine, oracle, form):
+    """Every thread-level sponge stage (keypair prologue, H(pk), both prologues, the
+    ciphertext pre-absorb and both final hashes) on five lanes per state, against the oracle;
+    n = 7 leaves a partial group of lanes, and tampered ciphertexts take the reject path."""
+    from dpcrypto_b200 import kem
+
+    knobs = ("frodo_five_max", "frodo_ss_five_max")
+    before = {k: kem.get_tuning().get(k, 0) for k in knobs}
+    for k in knobs:
+        kem.set_tuning(k, 1 << 30)
+    try:
+        n = 7
+        kc, ec = oracle.coins(n, 64, "kp", first=61), oracle.coins(n, 24, "enc", first=61)
+        pk_o, sk_o = oracle.keypair(0, kc, threads=8)
+        ct_o, ss_o = oracle.enc(0, pk_o, ec, threads=8)
+        pk, sk = engine.keypair(d.FRODO976, kc, form)
+        assert (pk == pk_o).all() and (sk == sk_o).all()
+        ct, ss = engine.enc(d.FRODO976, pk_o, ec, form)
+        assert (ct == ct_o).all() and (ss == ss_o).all()
+        assert (engine.dec(d.FRODO976, ct_o, sk_o, form) == ss_o).all()
+        bad = _tamper(ct_o)
+        assert (engine.dec(d.FRODO976, bad, sk_o, form) == oracle.dec(0, bad, sk_o, threads=8)).all()
+    finally:
+        for k, v in before.items():
+            kem.set_tuning(k, v)

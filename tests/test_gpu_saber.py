@@ -134,3 +134,32 @@ def test_saber_malformed_secret_key(engine, oracle, level, form):
     ct_g, ss_g = engine.enc(level, pk, ec, form)
     assert (ct_g == ct).all() and (ss_g == ss).all()
     assert (engine.dec(level, ct, wide, form) == oracle.dec(level, ct, wide_lo, threads=8)).all()
+
+
+@pytest.mark.parametrize("level", LEVELS)
+@pytest.mark.parametrize("five", [0, 1 << 30])
+def test_saber_sponges_on_five_lanes(engine, oracle, level, five):
+    """The prologue and finish sponges on five lanes per state (saber_five_max /
+    saber_finish_five_max) or not, against the oracle, with batch sizes that leave partial
+    groups and partial warps (n = 1, 7, 45)."""
+    from dpcrypto_b200 import kem
+
+    before = {k: kem.get_tuning().get(k, 8192) for k in ("saber_five_max", "saber_finish_five_max")}
+    for k in before:
+        kem.set_tuning(k, five)
+    try:
+        for n in (1, 7, 45):
+            kc, ec = oracle.coins(n, 96, "kp", first=91), oracle.coins(n, 32, "enc", first=91)
+            pk_o, sk_o = oracle.keypair(level, kc, threads=8)
+            ct_o, ss_o = oracle.enc(level, pk_o, ec, threads=8)
+            for form in (d.FORM_TC, d.FORM_DP4A):
+                pk, sk = engine.keypair(level, kc, form)
+                assert (pk == pk_o).all() and (sk == sk_o).all()
+                ct, ss = engine.enc(level, pk_o, ec, form)
+                assert (ct == ct_o).all() and (ss == ss_o).all()
+                assert (engine.dec(level, ct_o, sk_o, form) == ss_o).all()
+                bad = _tamper(ct_o)
+                assert (engine.dec(level, bad, sk_o, form) == oracle.dec(level, bad, sk_o, threads=8)).all()
+    finally:
+        for k, v in before.items():
+            kem.set_tuning(k, v)
