@@ -753,7 +753,8 @@ int dpkem_set_tuning(const char *key, int value) {
   Tuning &t = tuning();
   const std::string k(key);
   const bool zero_ok = k == "pipe_priority" || k == "saber_pair_max" || k == "saber_five_max" ||
-                       k == "saber_finish_five_max" || k == "frodo_five_max" || k == "frodo_ss_five_max";
+                       k == "saber_finish_five_max" || k == "frodo_five_max" || k == "frodo_ss_five_max" ||
+                       k == "saber_tc_ctas_per_sm";
   if (value == 0 && !zero_ok) return set_status(DPKEM_EINVAL);
   if (k == "thread_block") {
     if (value % 32 || value > 256) return set_status(DPKEM_EINVAL);
@@ -778,6 +779,8 @@ int dpkem_set_tuning(const char *key, int value) {
     t.frodo_five_max = value;
   } else if (k == "frodo_ss_five_max") {
     t.frodo_ss_five_max = value;
+  } else if (k == "saber_tc_ctas_per_sm") {
+    t.saber_tc_ctas_per_sm = std::min(value, 8);
   } else {
     return set_status(DPKEM_EINVAL);
   }

@@ -1,6 +1,8 @@
 // Saber (LightSaber l=2, Saber l=3, FireSaber l=4) batched keypair / encaps / decaps: one
 // launch per stage over n instances.  The stage bodies live in saber_dev.cuh (shared with
 // the persistent mixed-batch kernel); these wrappers only map blockIdx/threadIdx to instances.
+#include <algorithm>
+
 #include "saber_dev.cuh"
 
 namespace dpkem {
@@ -108,6 +110,53 @@ __global__ void __launch_bounds__(256) product_tc_kernel(SaberBatch b) {
   }
 }
 
+// Persistent tensor-core product: each CTA keeps its TMEM columns and mbarrier across the
+// instances it takes (i = blockIdx.x, + gridDim.x, ...) and loads the next instance's
+// packed operands into registers while the current one is processed, so an instance's
+// global-load latency hides behind the previous instance's work.
+template <int L, int MODE>
+__global__ void __launch_bounds__(256, 4) product_tc_persistent_kernel(SaberBatch b) {
+  using Y = PL<L>;
+  extern __shared__ __align__(1024) uint8_t sm[];
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + Y::TSLOT);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Y::BAR);
+  if (threadIdx.x < 32) {
+    tmem_alloc(tslot, 32);
+    tmem_relinquish();
+  }
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tslot;
+  constexpr int op = op_of(MODE);
+  sdev::OperandPrefetch<L, MODE> pf;
+  int i = blockIdx.x;
+  if (i < b.n) pf.load(inst_of<L>(b, i, op));
+  uint32_t phase = 0;
+  bool ok = true;
+  for (; i < b.n; i += gridDim.x) {
+    pf.store(sm);  // the staging area is free: the previous instance ended with a CTA barrier
+    __syncthreads();
+    if (i + (int)gridDim.x < b.n) pf.load(inst_of<L>(b, i + gridDim.x, op));
+    const sdev::Inst v = inst_of<L>(b, i, op);
+    sdev::unpack_operands<L, MODE>(v, sm);
+    __syncthreads();
+    ok = sdev::tc_mma_epilogue<L, MODE>(v, sm, tbase, b.err, phase) && ok;
+    phase ^= 1u;
+  }
+  if (threadIdx.x == 0 && ok) mbar_inval(bar);
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    tc_fence_after();
+    tmem_dealloc(tbase, 32);
+  }
+}
+
 template <typename K>
 cudaError_t prep(K kernel, int bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -119,8 +168,26 @@ cudaError_t launch_product(const SaberBatch &b, int form, cudaStream_t st) {
   cudaError_t e;
   if (form == FORM_TC) {
     constexpr int bytes = Y::TC_TOTAL;
-    if ((e = prep(product_tc_kernel<L, MODE>, bytes)) != cudaSuccess) return e;
-    product_tc_kernel<L, MODE><<<b.n, 256, bytes, st>>>(b);
+    const int per_sm = tuning().saber_tc_ctas_per_sm;
+    if (per_sm > 0) {
+      // persistent: at most per_sm CTAs per SM (capped by what fits), several instances each
+      static int fits = 0, sms = 0;  // per process and instantiation: the kernel's resources are fixed
+      if (!fits) {
+        if ((e = prep(product_tc_persistent_kernel<L, MODE>, bytes)) != cudaSuccess) return e;
+        int dev = 0, f = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f, product_tc_persistent_kernel<L, MODE>, 256,
+                                                                bytes)) != cudaSuccess)
+          return e;
+        fits = f > 0 ? f : 1;
+      }
+      const int grid = std::min(b.n, sms * std::min(per_sm, fits));
+      product_tc_persistent_kernel<L, MODE><<<grid, 256, bytes, st>>>(b);
+    } else {
+      if ((e = prep(product_tc_kernel<L, MODE>, bytes)) != cudaSuccess) return e;
+      product_tc_kernel<L, MODE><<<b.n, 256, bytes, st>>>(b);
+    }
   } else if (form == FORM_INT32) {
     constexpr int bytes = Y::DP4A_TOTAL;
     if ((e = prep(product_dp4a_kernel<L, MODE, true>, bytes)) != cudaSuccess) return e;

@@ -574,17 +574,83 @@ __device__ __forceinline__ void copy8(uint8_t *dst, const uint8_t *src, int byte
 // Phase 1: secrets and public polynomials into shared memory.  The packed inputs are
 // first copied in with 8-byte loads (a handful per thread), then unpacked from shared
 // memory, instead of up to three byte loads from global memory per coefficient.
+// The packed inputs of one instance as 8-byte words: source in global memory and
+// destination in the staging area.
 template <int L, int MODE>
-__device__ __forceinline__ void load_operands(const Inst &v, uint8_t *sm) {
+struct Staged {
   using P = SP<L>;
-  using S = Scr<L>;
   using Y = PL<L>;
   static_assert(P::ARAW % 8 == 0 && P::SRAW % 8 == 0 && P::POLYVECCOMP % 8 == 0 && P::POLYVEC % 8 == 0 &&
                     P::CT % 8 == 0,
                 "8-byte staging");
+  static constexpr bool INNER = MODE == PM_DEC_INNER;
+  static constexpr int W0 = (INNER ? P::POLYVEC : P::ARAW) / 8;                      // words of piece 0
+  static constexpr int W1 = (INNER ? P::CT : P::SRAW) / 8;                            // piece 1
+  static constexpr int W2 = (INNER || MODE == PM_KEYPAIR) ? 0 : P::POLYVECCOMP / 8;  // piece 2
+  static constexpr int WORDS = W0 + W1 + W2;
+  static constexpr int PER_THREAD = (WORDS + 255) / 256;  // with 256 threads
+  __device__ __forceinline__ static const uint2 *src(const Inst &v, int w) {
+    if (INNER)
+      return w < W0 ? reinterpret_cast<const uint2 *>(v.sk) + w : reinterpret_cast<const uint2 *>(v.ct) + (w - W0);
+    if (w < W0) return reinterpret_cast<const uint2 *>(v.scr + Scr<L>::ARAW) + w;
+    if (w < W0 + W1) return reinterpret_cast<const uint2 *>(v.scr + Scr<L>::SRAW) + (w - W0);
+    return reinterpret_cast<const uint2 *>(MODE == PM_ENC ? v.pk : v.sk + P::POLYVEC) + (w - W0 - W1);
+  }
+  __device__ __forceinline__ static uint2 *dst(uint8_t *sm, int w) {
+    if (INNER)
+      return w < W0 ? reinterpret_cast<uint2 *>(sm + Y::ST_SK) + w : reinterpret_cast<uint2 *>(sm + Y::ST_CT) + (w - W0);
+    if (w < W0) return reinterpret_cast<uint2 *>(sm + Y::ST_A) + w;
+    if (w < W0 + W1) return reinterpret_cast<uint2 *>(sm + Y::ST_S) + (w - W0);
+    return reinterpret_cast<uint2 *>(sm + Y::ST_P) + (w - W0 - W1);
+  }
+};
+
+// Copy one instance's packed inputs into the staging area (CTA-wide, 8-byte accesses).
+template <int L, int MODE>
+__device__ __forceinline__ void stage_operands(const Inst &v, uint8_t *sm) {
+  using T = Staged<L, MODE>;
+  for (int w = threadIdx.x; w < T::WORDS; w += blockDim.x) *T::dst(sm, w) = *T::src(v, w);
+}
+
+// The same copy split in two for a persistent loop (256 threads): load() into registers
+// early, store() into the staging area once it is free.
+template <int L, int MODE>
+struct OperandPrefetch {
+  using T = Staged<L, MODE>;
+  uint2 r[T::PER_THREAD];
+  __device__ __forceinline__ void load(const Inst &v) {
+#pragma unroll
+    for (int k = 0; k < T::PER_THREAD; k++) {
+      const int w = threadIdx.x + 256 * k;
+      if (w < T::WORDS) r[k] = *T::src(v, w);
+    }
+  }
+  __device__ __forceinline__ void store(uint8_t *sm) const {
+#pragma unroll
+    for (int k = 0; k < T::PER_THREAD; k++) {
+      const int w = threadIdx.x + 256 * k;
+      if (w < T::WORDS) *T::dst(sm, w) = r[k];
+    }
+  }
+};
+
+template <int L, int MODE>
+__device__ __forceinline__ void unpack_operands(const Inst &v, uint8_t *sm);
+
+template <int L, int MODE>
+__device__ __forceinline__ void load_operands(const Inst &v, uint8_t *sm) {
+  stage_operands<L, MODE>(v, sm);
+  __syncthreads();
+  unpack_operands<L, MODE>(v, sm);
+}
+
+// Unpack the staged inputs (after stage_operands or a prefetch's store, and a CTA barrier).
+template <int L, int MODE>
+__device__ __forceinline__ void unpack_operands(const Inst &v, uint8_t *sm) {
+  using P = SP<L>;
+  using Y = PL<L>;
   static_assert(Y::DP4A_TOTAL <= Y::TC_TOTAL, "staging must fit the tensor form's layout");
   const int tid = threadIdx.x;
-  const uint8_t *scr = v.scr;
   uint32_t *secw = reinterpret_cast<uint32_t *>(sm + Y::SEC);  // 4 int8 coefficients per word
   uint16_t *a16 = reinterpret_cast<uint16_t *>(sm + Y::A16);
   uint16_t *b16 = reinterpret_cast<uint16_t *>(sm + Y::B16);
@@ -604,9 +670,6 @@ __device__ __forceinline__ void load_operands(const Inst &v, uint8_t *sm) {
     }
   };
   if (MODE == PM_DEC_INNER) {
-    copy8(sm + Y::ST_SK, v.sk, P::POLYVEC);
-    copy8(sm + Y::ST_CT, v.ct, P::CT);
-    __syncthreads();
     const uint8_t *ct = sm + Y::ST_CT;
     // 13-bit secret from sk, centred: 32 coefficients (13 words) per thread.
     for (int g = tid; g < L * SN / 32; g += blockDim.x) {
@@ -623,10 +686,6 @@ __device__ __forceinline__ void load_operands(const Inst &v, uint8_t *sm) {
     unpack_p(ct);
     for (int c = tid; c < SN; c += blockDim.x) cm[c] = (uint16_t)unpack_smem(ct + P::POLYVECCOMP, c, P::ET);
   } else {
-    copy8(sm + Y::ST_A, scr + S::ARAW, P::ARAW);
-    copy8(sm + Y::ST_S, scr + S::SRAW, P::SRAW);
-    if (MODE != PM_KEYPAIR) copy8(sm + Y::ST_P, MODE == PM_ENC ? v.pk : v.sk + P::POLYVEC, P::POLYVECCOMP);
-    __syncthreads();
     // CBD_mu from the GenSecret bytes: 16 coefficients (mu/2 words) per thread.
     constexpr uint32_t hm = (1u << (P::MU / 2)) - 1u;
     for (int g = tid; g < L * SN / 16; g += blockDim.x) {
@@ -807,19 +866,36 @@ __device__ __forceinline__ void product_dp4a_cta(const Inst &v, uint8_t *sm) {
 // ---------------------------------------------------------------- tcgen05 form
 // TMEM columns [tbase, tbase + 32) must be allocated by the caller; the mbarrier in
 // shared memory is initialised here.  Returns false if the bounded wait expired.
+// From unpacked operands to the stored result: secret sequences, Hankel and B operand
+// tiles, the MMAs (completion on the mbarrier at Y::BAR, parity `phase`), the TMEM
+// read-back and the epilogue.  Returns false if the bounded wait expired.
+template <int L, int MODE>
+__device__ __forceinline__ bool tc_mma_epilogue(const Inst &v, uint8_t *sm, uint32_t tbase, uint32_t *err,
+                                                uint32_t phase);
+
 template <int L, int MODE>
 __device__ __forceinline__ bool product_tc_cta(const Inst &v, uint8_t *sm, uint32_t tbase, uint32_t *err) {
   using Y = PL<L>;
-  constexpr int NO = n_out<L, MODE>();
-  constexpr int NPAD = 2 * NO <= 8 ? 8 : 16;
   uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Y::BAR);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (tid == 0) {
+  if (threadIdx.x == 0) {
     mbar_init(bar, 1);
     fence_mbar_init();
   }
   load_operands<L, MODE>(v, sm);
   __syncthreads();
+  const bool ok = tc_mma_epilogue<L, MODE>(v, sm, tbase, err, 0);
+  if (threadIdx.x == 0 && ok) mbar_inval(bar);
+  return ok;
+}
+
+template <int L, int MODE>
+__device__ __forceinline__ bool tc_mma_epilogue(const Inst &v, uint8_t *sm, uint32_t tbase, uint32_t *err,
+                                                uint32_t phase) {
+  using Y = PL<L>;
+  constexpr int NO = n_out<L, MODE>();
+  constexpr int NPAD = 2 * NO <= 8 ? 8 : 16;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Y::BAR);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   build_seq<L, true>(sm);
   __syncthreads();
   // Hankel core matrices: H_j[t][r][c] = E_j[8t + r + c].  Row r = tid % 8 is fixed per
@@ -876,7 +952,7 @@ __device__ __forceinline__ bool product_tc_cta(const Inst &v, uint8_t *sm, uint3
                  b0 + (uint64_t)(((16 * j + 2 * ks) * 128) >> 4), idesc, (j | ks) ? 1u : 0u);
     mma_commit(bar);
   }
-  const bool ok = mbar_wait(bar, 0);
+  const bool ok = mbar_wait(bar, phase);
   if (!ok && lane == 0) atomicOr(err, DEV_ERR_TIMEOUT);
   tc_fence_after();
   // Warp w reads TMEM lanes 32 (w % 4) .. of M tile w / 4: coefficient = tid.
@@ -889,7 +965,6 @@ __device__ __forceinline__ bool product_tc_cta(const Inst &v, uint8_t *sm, uint3
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (tid == 0 && ok) mbar_inval(bar);
   epilogue<L, MODE>(v, sm);
   __syncthreads();
   return ok;

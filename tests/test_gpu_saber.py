@@ -144,7 +144,7 @@ def test_saber_sponges_on_five_lanes(engine, oracle, level, five):
     groups and partial warps (n = 1, 7, 45)."""
     from dpcrypto_b200 import kem
 
-    before = {k: kem.get_tuning().get(k, 8192) for k in ("saber_five_max", "saber_finish_five_max")}
+    before = {k: kem.get_tuning().get(k, 0) for k in ("saber_five_max", "saber_finish_five_max")}
     for k in before:
         kem.set_tuning(k, five)
     try:
@@ -163,3 +163,29 @@ def test_saber_sponges_on_five_lanes(engine, oracle, level, five):
     finally:
         for k, v in before.items():
             kem.set_tuning(k, v)
+
+
+@pytest.mark.parametrize("level", LEVELS)
+@pytest.mark.parametrize("per_sm", [0, 1, 4])
+def test_saber_tc_product_persistent(engine, oracle, level, per_sm):
+    """The tensor-core product with a CTA per instance (0) or as persistent CTAs that each
+    take several instances and prefetch the next one's operands (1: 148 CTAs, so n = 333
+    gives every CTA two or three instances), against the oracle, reject path included."""
+    from dpcrypto_b200 import kem
+
+    before = kem.get_tuning().get("saber_tc_ctas_per_sm", 4)
+    kem.set_tuning("saber_tc_ctas_per_sm", per_sm)
+    try:
+        n = 333
+        kc, ec = oracle.coins(n, 96, "kp", first=123), oracle.coins(n, 32, "enc", first=123)
+        pk_o, sk_o = oracle.keypair(level, kc, threads=8)
+        ct_o, ss_o = oracle.enc(level, pk_o, ec, threads=8)
+        pk, sk = engine.keypair(level, kc, d.FORM_TC)
+        assert (pk == pk_o).all() and (sk == sk_o).all()
+        ct, ss = engine.enc(level, pk_o, ec, d.FORM_TC)
+        assert (ct == ct_o).all() and (ss == ss_o).all()
+        assert (engine.dec(level, ct_o, sk_o, d.FORM_TC) == ss_o).all()
+        bad = _tamper(ct_o)
+        assert (engine.dec(level, bad, sk_o, d.FORM_TC) == oracle.dec(level, bad, sk_o, threads=8)).all()
+    finally:
+        kem.set_tuning("saber_tc_ctas_per_sm", before)
