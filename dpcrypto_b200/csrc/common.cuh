@@ -50,7 +50,7 @@ struct Tuning {
   int saber_finish_five_max = 0;  // the same for the encaps / keypair finish
   int frodo_five_max = 0;       // largest Frodo batch whose prologues run on five lanes per state (0: never)
   int frodo_ss_five_max = 0;    // the same for H(pk) and the final hash
-  int saber_tc_ctas_per_sm = 4; // persistent Saber tensor-core product CTAs per SM (0: a CTA per instance)
+  int saber_tc_ctas_per_sm = 0; // persistent Saber tensor-core product CTAs per SM (0: a CTA per instance)
 };
 Tuning &tuning();
 

@@ -83,6 +83,6 @@ def test_tuning_knobs():
         defaults = {"thread_block": 64, "mixed_frodo_task": 256, "mixed_pair_task": 128, "mixed_thread_task": 256,
                     "pipe_chunks": 4, "pipe_priority": 1, "saber_pair_max": 6144, "saber_five_max": 0,
                     "saber_finish_five_max": 0, "frodo_five_max": 0, "frodo_ss_five_max": 0,
-                    "saber_tc_ctas_per_sm": 4}
+                    "saber_tc_ctas_per_sm": 0}
         for k in kem.RUNTIME_KNOBS:
             lib.dpkem_set_tuning(k.encode(), saved.get(k, defaults[k]))

@@ -173,7 +173,7 @@ def test_saber_tc_product_persistent(engine, oracle, level, per_sm):
     gives every CTA two or three instances), against the oracle, reject path included."""
     from dpcrypto_b200 import kem
 
-    before = kem.get_tuning().get("saber_tc_ctas_per_sm", 4)
+    before = kem.get_tuning().get("saber_tc_ctas_per_sm", 0)
     kem.set_tuning("saber_tc_ctas_per_sm", per_sm)
     try:
         n = 333
