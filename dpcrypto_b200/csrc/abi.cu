@@ -712,7 +712,8 @@ int dpkem_probe_int_peaks(dpkem_ctx *c, double *int_ops_per_s, double *keccak_pe
 }
 
 int dpkem_keccak_f1600_lanes(dpkem_ctx *c, int lanes, size_t n, const uint64_t *in, uint64_t *out, int perms) {
-  if (!c || (lanes != 1 && lanes != 2 && lanes != 5) || perms < 0 || n > (size_t)INT32_MAX) return set_status(DPKEM_EINVAL);
+  if (!c || (lanes != 1 && lanes != 2 && lanes != 5 && lanes != 25) || perms < 0 || n > (size_t)INT32_MAX)
+    return set_status(DPKEM_EINVAL);
   if (n == 0) return set_status(DPKEM_OK);
   if (!in || !out || (reinterpret_cast<uintptr_t>(in) & 7) || (reinterpret_cast<uintptr_t>(out) & 7))
     return set_status(DPKEM_EINVAL);
@@ -724,7 +725,8 @@ int dpkem_keccak_f1600_lanes(dpkem_ctx *c, int lanes, size_t n, const uint64_t *
 }
 
 int dpkem_probe_keccak_chain(dpkem_ctx *c, int lanes, int states, int perms, double *ms) {
-  if (!c || !ms || (lanes != 1 && lanes != 2 && lanes != 5) || states <= 0 || perms <= 0) return set_status(DPKEM_EINVAL);
+  if (!c || !ms || (lanes != 1 && lanes != 2 && lanes != 5 && lanes != 25) || states <= 0 || perms <= 0)
+    return set_status(DPKEM_EINVAL);
   std::lock_guard<std::mutex> lock(c->mu);
   cudaSetDevice(c->device);
   cudaError_t e = cudaStreamWaitEvent(c->stream, c->last, 0);
@@ -754,7 +756,8 @@ int dpkem_set_tuning(const char *key, int value) {
   const std::string k(key);
   const bool zero_ok = k == "pipe_priority" || k == "saber_pair_max" || k == "saber_five_max" ||
                        k == "saber_finish_five_max" || k == "frodo_five_max" || k == "frodo_ss_five_max" ||
-                       k == "saber_tc_ctas_per_sm";
+                       k == "saber_tc_ctas_per_sm" || k == "saber_warp_max" || k == "saber_finish_warp_max" ||
+                       k == "frodo_warp_max" || k == "frodo_ss_warp_max";
   if (value == 0 && !zero_ok) return set_status(DPKEM_EINVAL);
   if (k == "thread_block") {
     if (value % 32 || value > 256) return set_status(DPKEM_EINVAL);
@@ -779,6 +782,14 @@ int dpkem_set_tuning(const char *key, int value) {
     t.frodo_five_max = value;
   } else if (k == "frodo_ss_five_max") {
     t.frodo_ss_five_max = value;
+  } else if (k == "saber_warp_max") {
+    t.saber_warp_max = value;
+  } else if (k == "saber_finish_warp_max") {
+    t.saber_finish_warp_max = value;
+  } else if (k == "frodo_warp_max") {
+    t.frodo_warp_max = value;
+  } else if (k == "frodo_ss_warp_max") {
+    t.frodo_ss_warp_max = value;
   } else if (k == "saber_tc_ctas_per_sm") {
     t.saber_tc_ctas_per_sm = std::min(value, 8);
   } else {

@@ -46,8 +46,12 @@ struct Tuning {
   int pipe_chunks = 4;          // chunks (one stream each) of a pipelined host-mode batch, <= 8
   int pipe_priority = 1;        // 1: chunk streams get descending priorities (earlier chunks finish first)
   int saber_pair_max = 6144;    // largest Saber batch whose prologue runs GenMatrix on lane pairs (0: never)
+  int saber_warp_max = 0;       // largest Saber batch whose prologue sponges run on a warp per state (0: never)
+  int saber_finish_warp_max = 0;  // the same for the encaps / keypair finish
   int saber_five_max = 0;       // largest Saber batch whose prologue sponges run on five lanes per state (0: never)
   int saber_finish_five_max = 0;  // the same for the encaps / keypair finish
+  int frodo_warp_max = 0;       // largest Frodo batch whose prologues run on a warp per state (0: never)
+  int frodo_ss_warp_max = 0;    // the same for H(pk) and the final hash
   int frodo_five_max = 0;       // largest Frodo batch whose prologues run on five lanes per state (0: never)
   int frodo_ss_five_max = 0;    // the same for H(pk) and the final hash
   int saber_tc_ctas_per_sm = 0; // persistent Saber tensor-core product CTAs per SM (0: a CTA per instance)

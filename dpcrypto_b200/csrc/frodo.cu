@@ -36,35 +36,39 @@ __global__ void __launch_bounds__(64) dec_prologue_kernel(FrodoBatch b) {
   else fdev::ct_absorb_inst(inst_of(b, i, OP_DEC));
 }
 
-// Five lanes per state (keccak5.cuh): 32 threads = 6 instances per warp.  STAGE selects the
-// stage body: 0 keypair prologue, 1 H(pk), 2 encaps prologue, 3 encaps final hash,
-// 4 decaps final hash; the decaps prologue below has its own kernel.
-template <int STAGE>
-__global__ void __launch_bounds__(32) stage5_kernel(FrodoBatch b) {
-  __shared__ __align__(16) uint8_t xbuf[k5::kSmemPerWarp];
-  const k5::Lanes k = k5::make_lanes(xbuf);
-  const int g = threadIdx.x / 5, i = blockIdx.x * 6 + g;
-  const bool live = g < 6 && i < b.n;
+// Several lanes per state (msponge.cuh; NS = 5: five lanes, six instances per warp; NS = 1:
+// a warp per instance), one warp per block.  STAGE selects the stage body: 0 keypair
+// prologue, 1 H(pk), 2 encaps prologue, 3 encaps final hash, 4 decaps final hash; the
+// decaps prologue below has its own kernel.
+template <int STAGE, int NS>
+__global__ void __launch_bounds__(32) stage_multi_kernel(FrodoBatch b) {
+  using S = msp::Multi<NS>;
+  __shared__ __align__(16) uint8_t xbuf[S::SMEM_PER_WARP > 0 ? S::SMEM_PER_WARP : 16];
+  const S s(xbuf);
+  const int g = s.state(), i = blockIdx.x * S::STATES_PER_WARP + g;
+  const bool live = g < S::STATES_PER_WARP && i < b.n;
   constexpr int op = STAGE <= 1 ? OP_KEYPAIR : STAGE <= 3 ? OP_ENC : OP_DEC;
   const fdev::Inst v = inst_of(b, live ? i : b.n - 1, op);
-  if constexpr (STAGE == 0) fdev::kp_prologue5(v, k, live);
-  else if constexpr (STAGE == 1) fdev::pk_hash5(v, k, live);
-  else if constexpr (STAGE == 2) fdev::prologue5<OP_ENC>(v, k, live);
-  else if constexpr (STAGE == 3) fdev::ss5<OP_ENC>(v, k, live);
-  else fdev::ss5<OP_DEC>(v, k, live);
+  if constexpr (STAGE == 0) fdev::kp_prologue_multi<S>(v, s, live);
+  else if constexpr (STAGE == 1) fdev::pk_hash_multi<S>(v, s, live);
+  else if constexpr (STAGE == 2) fdev::prologue_multi<S, OP_ENC>(v, s, live);
+  else if constexpr (STAGE == 3) fdev::ss_multi<S, OP_ENC>(v, s, live);
+  else fdev::ss_multi<S, OP_DEC>(v, s, live);
 }
 
-// Decaps prologue on five lanes: 64 threads = 6 instances, warp 0 the sampling chain,
-// warp 1 the ciphertext pre-absorb of the final hash.
-__global__ void __launch_bounds__(64) dec_prologue5_kernel(FrodoBatch b) {
-  __shared__ __align__(16) uint8_t xbuf[2 * k5::kSmemPerWarp];
+// Decaps prologue on several lanes per state: 64 threads, warp 0 the sampling chain, warp 1
+// the ciphertext pre-absorb of the final hash, for the same instances.
+template <int NS>
+__global__ void __launch_bounds__(64) dec_prologue_multi_kernel(FrodoBatch b) {
+  using S = msp::Multi<NS>;
+  __shared__ __align__(16) uint8_t xbuf[2 * (S::SMEM_PER_WARP > 0 ? S::SMEM_PER_WARP : 16)];
   const int w = threadIdx.x >> 5;
-  const k5::Lanes k = k5::make_lanes(xbuf + w * k5::kSmemPerWarp);
-  const int g = (threadIdx.x & 31) / 5, i = blockIdx.x * 6 + g;
-  const bool live = g < 6 && i < b.n;
+  const S s(xbuf + w * S::SMEM_PER_WARP);
+  const int g = s.state(), i = blockIdx.x * S::STATES_PER_WARP + g;
+  const bool live = g < S::STATES_PER_WARP && i < b.n;
   const fdev::Inst v = inst_of(b, live ? i : b.n - 1, OP_DEC);
-  if (w == 0) fdev::prologue5<OP_DEC>(v, k, live);
-  else fdev::ct_absorb5(v, k, live);
+  if (w == 0) fdev::prologue_multi<S, OP_DEC>(v, s, live);
+  else fdev::ct_absorb_multi<S>(v, s, live);
 }
 
 template <int MODE>
@@ -135,13 +139,20 @@ __global__ void __launch_bounds__(256, 2) kp_as_tc_kernel(FrodoBatch b) {
 
 inline int blocks_for(int n, int t) { return (n + t - 1) / t; }
 
-// Lanes per state of a thread-level sponge stage: five up to the stage's threshold
-// (frodo_five_max for the prologues, frodo_ss_five_max for the hashes), else one.
+// Lanes per state of a thread-level sponge stage: a warp per state up to warp_max, five lanes
+// up to five_max (frodo_warp_max / frodo_five_max for the prologues, frodo_ss_warp_max /
+// frodo_ss_five_max for the hashes), else one (false: the caller launches that).
 template <int STAGE>
-bool launch5(const FrodoBatch &b, int five_max, cudaStream_t st) {
-  if (b.n > five_max) return false;
-  stage5_kernel<STAGE><<<blocks_for(b.n, 6), 32, 0, st>>>(b);
-  return true;
+bool launch_multi(const FrodoBatch &b, int warp_max, int five_max, cudaStream_t st) {
+  if (b.n <= warp_max) {
+    stage_multi_kernel<STAGE, 1><<<b.n, 32, 0, st>>>(b);
+    return true;
+  }
+  if (b.n <= five_max) {
+    stage_multi_kernel<STAGE, 5><<<blocks_for(b.n, 6), 32, 0, st>>>(b);
+    return true;
+  }
+  return false;
 }
 
 template <typename K>
@@ -210,14 +221,14 @@ cudaError_t frodo_keypair(const FrodoBatch &b, int form, cudaStream_t st) {
   if (b.n <= 0) return cudaSuccess;
   const int tb = tuning().thread_block;
   mark(b, st);
-  if (!launch5<0>(b, tuning().frodo_five_max, st))
+  if (!launch_multi<0>(b, tuning().frodo_warp_max, tuning().frodo_five_max, st))
     kp_prologue_kernel<OP_KEYPAIR><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);
   const cudaError_t e = b.aes ? launch_kp_as<fdev::AesRowsFull, 1>(b, form, st)
                              : launch_kp_as<fdev::ShakeRows, fdev::KPT_NST>(b, form, st);
   if (e != cudaSuccess) return e;
   mark(b, st);
-  if (!launch5<1>(b, tuning().frodo_ss_five_max, st)) pk_hash_kernel<OP_KEYPAIR><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
+  if (!launch_multi<1>(b, tuning().frodo_ss_warp_max, tuning().frodo_ss_five_max, st)) pk_hash_kernel<OP_KEYPAIR><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);
   return cudaGetLastError();
 }
@@ -226,12 +237,12 @@ cudaError_t frodo_enc(const FrodoBatch &b, int form, cudaStream_t st) {
   if (b.n <= 0) return cudaSuccess;
   const int tb = tuning().thread_block;
   mark(b, st);
-  if (!launch5<2>(b, tuning().frodo_five_max, st)) prologue_kernel<OP_ENC><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
+  if (!launch_multi<2>(b, tuning().frodo_warp_max, tuning().frodo_five_max, st)) prologue_kernel<OP_ENC><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);
   cudaError_t e = launch_sa<OP_ENC>(b, form, st);
   if (e != cudaSuccess) return e;
   mark(b, st);
-  if (!launch5<3>(b, tuning().frodo_ss_five_max, st)) ss_kernel<OP_ENC><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
+  if (!launch_multi<3>(b, tuning().frodo_ss_warp_max, tuning().frodo_ss_five_max, st)) ss_kernel<OP_ENC><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);
   return cudaGetLastError();
 }
@@ -242,13 +253,14 @@ cudaError_t frodo_dec(const FrodoBatch &b, int form, cudaStream_t st) {
   mark(b, st);
   dec_w_kernel<<<b.n, 256, fdev::DEC_W_SMEM, st>>>(b);
   mark(b, st);
-  if (b.n <= tuning().frodo_five_max) dec_prologue5_kernel<<<blocks_for(b.n, 6), 64, 0, st>>>(b);
+  if (b.n <= tuning().frodo_warp_max) dec_prologue_multi_kernel<1><<<b.n, 64, 0, st>>>(b);
+  else if (b.n <= tuning().frodo_five_max) dec_prologue_multi_kernel<5><<<blocks_for(b.n, 6), 64, 0, st>>>(b);
   else dec_prologue_kernel<<<blocks_for(b.n, 32), 64, 0, st>>>(b);
   mark(b, st);
   cudaError_t e = launch_sa<OP_DEC>(b, form, st);
   if (e != cudaSuccess) return e;
   mark(b, st);
-  if (!launch5<4>(b, tuning().frodo_ss_five_max, st)) ss_kernel<OP_DEC><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
+  if (!launch_multi<4>(b, tuning().frodo_ss_warp_max, tuning().frodo_ss_five_max, st)) ss_kernel<OP_DEC><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
   mark(b, st);
   return cudaGetLastError();
 }

@@ -17,7 +17,7 @@
 #pragma once
 #include "common.cuh"
 #include "keccak.cuh"
-#include "keccak5.cuh"
+#include "msponge.cuh"
 #include "tc.cuh"
 
 namespace dpkem {
@@ -232,36 +232,47 @@ __device__ __forceinline__ void ss_inst(const Inst &v) {
   for (int q = 0; q < 3; q++) *reinterpret_cast<uint2 *>(v.ss + 8 * q) = a[q];
 }
 
-// ---------------------------------------------------------------- five lanes per state
-// The thread-level stages above with each sponge spread over a group of five lanes
-// (keccak5.cuh); they write the same bytes.  live = false keeps a group without an instance
-// in step (its reads stay in bounds, its writes are skipped).
+// ---------------------------------------------------------------- several lanes per state
+// The thread-level stages above with each sponge spread over several lanes (msponge.cuh:
+// S = msp::Multi<5>, five lanes per state, or msp::Multi<1>, a warp per state); they write
+// the same bytes.  live = false keeps a state without an instance in step (its reads stay
+// in bounds, its writes are skipped).
 
 __device__ __forceinline__ uint64_t u64_of(uint2 v) { return ((uint64_t)v.y << 32) | v.x; }
 __device__ __forceinline__ uint2 uint2_of(uint64_t v) { return make_uint2((uint32_t)v, (uint32_t)(v >> 32)); }
 
-// dom || seed (25 bytes) absorbed and finished, the seed in lanes 0..2 of g (threads 0..2,
-// slot 0): message lane j = (seed lane j-1 >> 56) | (seed lane j << 8), lane 0 with dom.
-__device__ __forceinline__ void seed_stream_init5(uint2 (&a)[5], const k5::Lanes &k, uint32_t dom,
-                                                  const uint2 (&g)[5]) {
-  const uint2 prev = k5::shfl(g[0], k.left);
-  const uint64_t x = k.t <= 2 ? u64_of(g[0]) : 0ull, xp = (k.t >= 1 && k.t <= 3) ? u64_of(prev) : 0ull;
-  const uint64_t l = (k.t == 0 ? (uint64_t)dom : (xp >> 56)) | (x << 8);
-  k5::zero(a);
-  if (k.t <= 3) a[0] = uint2_of(l);
-  k5::absorb_finish<136>(a, k, 25, 0x1Fu);
+// dom || seed (25 bytes) absorbed and finished, the 24-byte seed in lanes 0..2 of g:
+// message lane j = (seed lane j-1 >> 56) | (seed lane j << 8), lane 0 with dom.
+template <class S>
+__device__ __forceinline__ void seed_stream_init_multi(uint2 (&a)[S::NS], const S &s, uint32_t dom,
+                                                       const uint2 (&g)[S::NS]) {
+  const uint64_t x0 = u64_of(s.template get<0>(g)), x1 = u64_of(s.template get<1>(g)),
+                 x2 = u64_of(s.template get<2>(g));
+  msp::zero<S>(a);
+#pragma unroll
+  for (int y = 0; y < S::NS; y++) {
+    const int q = s.lane(y);
+    const uint64_t l = q == 0 ? (uint64_t)dom | (x0 << 8)
+                     : q == 1 ? (x0 >> 56) | (x1 << 8)
+                     : q == 2 ? (x1 >> 56) | (x2 << 8)
+                     : q == 3 ? (x2 >> 56)
+                              : 0ull;
+    a[y] = uint2_of(l);
+  }
+  msp::absorb_finish<S, 136>(a, s, 25, 0x1Fu);
 }
 
-// sample_stream on five lanes: each thread samples and stores the rate lanes it owns.
-__device__ __forceinline__ void sample_stream5(uint2 (&a)[5], const k5::Lanes &k, uint16_t *dst, int words,
-                                               uint8_t *dst_le, int le_words, bool live) {
+// sample_stream on several lanes: each thread samples and stores the rate lanes it owns.
+template <class S>
+__device__ __forceinline__ void sample_stream_multi(uint2 (&a)[S::NS], const S &s, uint16_t *dst, int words,
+                                                    uint8_t *dst_le, int le_words, bool live) {
   const int nblk = (words + 67) / 68;
   for (int blk = 0; blk < nblk; blk++) {
-    if (blk) k5::f1600(a, k);
+    if (blk) s.perm(a);
 #pragma unroll
-    for (int y = 0; y < 4; y++) {
-      const int q = k.t + 5 * y, w = blk * 68 + 4 * q;
-      if (q < 17 && w < words && live) {
+    for (int y = 0; y < S::NS; y++) {
+      const int q = s.lane(y), w = blk * 68 + 4 * q;
+      if (q < 17 && w < words && live && s.writer()) {
         const uint2 v = sample_lane(a[y]);
         *reinterpret_cast<uint2 *>(dst + w) = v;
         if (dst_le && w < le_words) *reinterpret_cast<uint2 *>(dst_le + 2 * w) = v;
@@ -270,105 +281,101 @@ __device__ __forceinline__ void sample_stream5(uint2 (&a)[5], const k5::Lanes &k
   }
 }
 
-// Store lanes 0 .. nw-1 (nw <= 10) of a state to dst.
-__device__ __forceinline__ void store_lanes5(const uint2 (&a)[5], const k5::Lanes &k, uint8_t *dst, int nw,
-                                             bool live) {
-#pragma unroll
-  for (int y = 0; y < 2; y++) {
-    const int q = k.t + 5 * y;
-    if (q < nw && live) *reinterpret_cast<uint2 *>(dst + 8 * q) = a[y];
-  }
-}
-
-__device__ __forceinline__ void kp_prologue5(const Inst &v, const k5::Lanes &k, bool live) {
-  uint2 a[5], g[5];
+template <class S>
+__device__ __forceinline__ void kp_prologue_multi(const Inst &v, const S &s, bool live) {
+  uint2 a[S::NS], g[S::NS];
   // seedA = SHAKE256(z, 16)
-  k5::zero(a);
-  k5::absorb_aligned<136>(a, k, 0, v.coins + 48, 16, live);
-  k5::absorb_finish<136>(a, k, 16, 0x1Fu);
-  store_lanes5(a, k, v.pk, 2, live);
-  store_lanes5(a, k, v.sk + LENS, 2, live);
-  if (live && k.t < 3) *reinterpret_cast<uint2 *>(v.sk + 8 * k.t) = ld_lane(v.coins + 8 * k.t);
+  msp::zero<S>(a);
+  msp::absorb_aligned<S, 136>(a, s, 0, v.coins + 48, 16, live);
+  msp::absorb_finish<S, 136>(a, s, 16, 0x1Fu);
+  msp::store<S>(a, s, v.pk, 2, live);
+  msp::store<S>(a, s, v.sk + LENS, 2, live);
+  const int q = s.lane(0);
+  if (live && s.writer() && q < 3) *reinterpret_cast<uint2 *>(v.sk + 8 * q) = ld_lane(v.coins + 8 * q);
   // S^T || E = sample(SHAKE256(0x5F || seedSE))
-  k5::zero(g);
-  k5::absorb_aligned<136>(g, k, 0, v.coins + 24, 24, live);
-  seed_stream_init5(a, k, 0x5Fu, g);
-  sample_stream5(a, k, v.rw, 2 * N * NBAR, v.sk + SK_S, N * NBAR, live);
+  msp::zero<S>(g);
+  msp::absorb_aligned<S, 136>(g, s, 0, v.coins + 24, 24, live);
+  seed_stream_init_multi<S>(a, s, 0x5Fu, g);
+  sample_stream_multi<S>(a, s, v.rw, 2 * N * NBAR, v.sk + SK_S, N * NBAR, live);
 }
 
-__device__ __forceinline__ void pk_hash5(const Inst &v, const k5::Lanes &k, bool live) {
-  uint2 a[5];
-  k5::zero(a);
-  const int pos = k5::absorb_aligned<136>(a, k, 0, v.pk, PK, live);
-  k5::absorb_finish<136>(a, k, pos, 0x1Fu);
-  store_lanes5(a, k, v.sk + SK_PKH, 3, live);
+template <class S>
+__device__ __forceinline__ void pk_hash_multi(const Inst &v, const S &s, bool live) {
+  uint2 a[S::NS];
+  msp::zero<S>(a);
+  const int pos = msp::absorb_aligned<S, 136>(a, s, 0, v.pk, PK, live);
+  msp::absorb_finish<S, 136>(a, s, pos, 0x1Fu);
+  msp::store<S>(a, s, v.sk + SK_PKH, 3, live);
 }
 
-template <int MODE>
-__device__ __forceinline__ void prologue5(const Inst &v, const k5::Lanes &k, bool live) {
-  uint2 a[5], g[5];
-  k5::zero(g);
+template <class S, int MODE>
+__device__ __forceinline__ void prologue_multi(const Inst &v, const S &s, bool live) {
+  uint2 a[S::NS], g[S::NS];
+  msp::zero<S>(g);
   if (MODE == OP_ENC) {
-    k5::zero(a);
-    const int pos = k5::absorb_aligned<136>(a, k, 0, v.pk, PK, live);
-    k5::absorb_finish<136>(a, k, pos, 0x1Fu);
-    if (k.t <= 2) g[0] = a[0];  // pkh = lanes 0..2
-    k5::absorb_aligned<136>(g, k, 24, v.coins, 24, live);
+    msp::zero<S>(a);
+    const int pos = msp::absorb_aligned<S, 136>(a, s, 0, v.pk, PK, live);
+    msp::absorb_finish<S, 136>(a, s, pos, 0x1Fu);
+#pragma unroll
+    for (int y = 0; y < S::NS; y++)
+      if (s.lane(y) < 3) g[y] = a[y];  // pkh = lanes 0..2
+    msp::absorb_aligned<S, 136>(g, s, 24, v.coins, 24, live);
   } else {
-    k5::absorb_aligned<136>(g, k, 0, v.sk + SK_PKH, 24, live);
-    k5::absorb_aligned<136>(g, k, 24, v.mu, 24, live);
+    msp::absorb_aligned<S, 136>(g, s, 0, v.sk + SK_PKH, 24, live);
+    msp::absorb_aligned<S, 136>(g, s, 24, v.mu, 24, live);
   }
   // G2 = SHAKE256(pkh || mu, 48) = seedSE (lanes 0..2) || k (lanes 3..5)
-  k5::absorb_finish<136>(g, k, 48, 0x1Fu);
+  msp::absorb_finish<S, 136>(g, s, 48, 0x1Fu);
 #pragma unroll
-  for (int y = 0; y < 2; y++) {
-    const int q = k.t + 5 * y;
-    if (q >= 3 && q < 6 && live) *reinterpret_cast<uint2 *>(v.kk + 8 * (q - 3)) = g[y];
+  for (int y = 0; y < S::NS; y++) {
+    const int q = s.lane(y);
+    if (q >= 3 && q < 6 && live && s.writer()) *reinterpret_cast<uint2 *>(v.kk + 8 * (q - 3)) = g[y];
   }
-  seed_stream_init5(a, k, 0x96u, g);
-  sample_stream5(a, k, v.rw, RW, nullptr, 0, live);
+  seed_stream_init_multi<S>(a, s, 0x96u, g);
+  sample_stream_multi<S>(a, s, v.rw, RW, nullptr, 0, live);
 }
 
-__device__ __forceinline__ void ct_absorb5(const Inst &v, const k5::Lanes &k, bool live) {
-  uint2 a[5];
-  k5::zero(a);
-  k5::absorb_aligned<136>(a, k, 0, v.ct, CT_FULL, live);
+template <class S>
+__device__ __forceinline__ void ct_absorb_multi(const Inst &v, const S &s, bool live) {
+  uint2 a[S::NS];
+  msp::zero<S>(a);
+  msp::absorb_aligned<S, 136>(a, s, 0, v.ct, CT_FULL, live);
 #pragma unroll
-  for (int y = 0; y < 5; y++)
-    if (live) v.hs[k.t + 5 * y] = a[y];
+  for (int y = 0; y < S::NS; y++)
+    if (live && s.writer()) v.hs[s.lane(y)] = a[y];
 }
 
-template <int MODE>
-__device__ __forceinline__ void ss5(const Inst &v, const k5::Lanes &k, bool live) {
-  uint2 a[5];
+template <class S, int MODE>
+__device__ __forceinline__ void ss_multi(const Inst &v, const S &s, bool live) {
+  uint2 a[S::NS];
   int pos;
   if (MODE == OP_DEC) {
 #pragma unroll
-    for (int y = 0; y < 5; y++) a[y] = live ? v.hs[k.t + 5 * y] : make_uint2(0u, 0u);
-    pos = k5::absorb_aligned<136>(a, k, 0, v.ct + CT_FULL, CT - CT_FULL, live);
+    for (int y = 0; y < S::NS; y++) a[y] = live ? v.hs[s.lane(y)] : make_uint2(0u, 0u);
+    pos = msp::absorb_aligned<S, 136>(a, s, 0, v.ct + CT_FULL, CT - CT_FULL, live);
   } else {
-    k5::zero(a);
-    pos = k5::absorb_aligned<136>(a, k, 0, v.ct, CT, live);
+    msp::zero<S>(a);
+    pos = msp::absorb_aligned<S, 136>(a, s, 0, v.ct, CT, live);
   }
   // k (encaps) or k' / s selected in constant time (decaps), in lanes pos/8 .. pos/8 + 2
   static_assert(CT % 136 % 8 == 0 && CT % 136 + 24 < 136, "k-hat fits after ct in the last rate block");
   const uint32_t m = (MODE == OP_DEC && live) ? 0u - (uint32_t)(*v.fail != 0u) : 0u;
   const int q0 = pos / 8;
 #pragma unroll
-  for (int y = 0; y < 5; y++) {
-    const int q = k.t + 5 * y;
+  for (int y = 0; y < S::NS; y++) {
+    const int q = s.lane(y);
     if (q >= q0 && q < q0 + 3 && live) {
       uint2 x = ld_lane(v.kk + 8 * (q - q0));
       if (MODE == OP_DEC) {
-        const uint2 s = ld_lane(v.sk + 8 * (q - q0));
-        x = make_uint2((x.x & ~m) | (s.x & m), (x.y & ~m) | (s.y & m));
+        const uint2 sv = ld_lane(v.sk + 8 * (q - q0));
+        x = make_uint2((x.x & ~m) | (sv.x & m), (x.y & ~m) | (sv.y & m));
       }
       a[y].x ^= x.x;
       a[y].y ^= x.y;
     }
   }
-  k5::absorb_finish<136>(a, k, pos + 24, 0x1Fu);
-  store_lanes5(a, k, v.ss, 3, live);
+  msp::absorb_finish<S, 136>(a, s, pos + 24, 0x1Fu);
+  msp::store<S>(a, s, v.ss, 3, live);
 }
 
 // ---------------------------------------------------------------- CTA-level stages (256 threads)

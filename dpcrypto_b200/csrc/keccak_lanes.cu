@@ -1,11 +1,12 @@
 // Keccak-f[1600] in each lanes-per-state layout, on independent states in device memory:
-// one lane per state (keccak.cuh), a lane pair in bit-interleaved form (keccak_pair.cuh) and
-// five lanes per state (keccak5.cuh).  Used to check the layouts against each other and the
+// one lane per state (keccak.cuh), a lane pair in bit-interleaved form (keccak_pair.cuh),
+// five lanes per state (keccak5.cuh) and a warp per state (keccak25.cuh).  Used to check the layouts against each other and the
 // oracle (dpkem_keccak_f1600_lanes) and to measure the latency of a dependent permutation
 // chain per layout and batch size (dpkem_probe_keccak_chain), which is what picks the layout
 // of each latency-bound sponge stage.
 #include "common.cuh"
 #include "keccak.cuh"
+#include "keccak25.cuh"
 #include "keccak5.cuh"
 #include "keccak_pair.cuh"
 
@@ -38,6 +39,12 @@ __global__ void __launch_bounds__(32) lanes_kernel(const uint2 *in, uint2 *out, 
       const uint32_t h = kpair::from_slice(a[q], p);
       if (live) reinterpret_cast<uint32_t *>(out + (size_t)s * 25 + q)[p] = h;
     }
+  } else if constexpr (LANES == 25) {
+    const k25::Lane k = k25::make_lane();
+    const int s = blockIdx.x;
+    uint2 v = in[(size_t)s * 25 + k.i];
+    for (int r = 0; r < perms; r++) k25::f1600(v, k);
+    if (lane < 25) out[(size_t)s * 25 + k.i] = v;
   } else {
     __shared__ __align__(16) uint8_t xbuf[k5::kSmemPerWarp];
     const k5::Lanes k = k5::make_lanes(xbuf);
@@ -56,7 +63,7 @@ __global__ void __launch_bounds__(32) lanes_kernel(const uint2 *in, uint2 *out, 
 
 template <int LANES>
 constexpr int states_per_block() {
-  return LANES == 1 ? 32 : LANES == 2 ? 16 : 6;
+  return LANES == 1 ? 32 : LANES == 2 ? 16 : LANES == 25 ? 1 : 6;
 }
 
 template <int LANES>
@@ -70,6 +77,7 @@ cudaError_t run(int lanes, const uint2 *in, uint2 *out, int n, int perms, cudaSt
     case 1: launch<1>(in, out, n, perms, st); break;
     case 2: launch<2>(in, out, n, perms, st); break;
     case 5: launch<5>(in, out, n, perms, st); break;
+    case 25: launch<25>(in, out, n, perms, st); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

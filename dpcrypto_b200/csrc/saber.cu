@@ -13,9 +13,8 @@ using sdev::PL;
 using sdev::Scr;
 
 // One or two lanes per state: 32 instances per block.  Warp 0 = hash chain + GenSecret XOF
-// (a thread per instance);
-// GenMatrix XOF on warp 1 (a thread per instance, PAIR = false, blockDim 64) or on warps 1-2
-// (a lane pair per instance, PAIR = true, blockDim 96).  Pairs shorten the longest chain
+// (a thread per instance); GenMatrix XOF on warp 1 (a thread per instance, PAIR = false,
+// blockDim 64) or on warps 1-2 (a lane pair per instance, PAIR = true, blockDim 96).  Pairs shorten the longest chain
 // while the batch leaves SM sub-partitions idle, and cost more issue slots per state once
 // it does not (tuning knob saber_pair_max).
 template <int L, int OP, bool PAIR>
@@ -30,24 +29,34 @@ __global__ void __launch_bounds__(96) prologue_kernel(SaberBatch b) {
   sdev::matrix_pair<L, OP>(inst_of<L>(b, live ? i : b.n - 1, OP), t & 1, live);
 }
 
-// Five lanes per state (keccak5.cuh): 64 threads = 6 instances, warp 0 the hash chain and
-// GenSecret, warp 1 GenMatrix; each warp keeps its 1.4 KB transpose buffer in shared memory.
-template <int L, int OP>
-__global__ void __launch_bounds__(64) prologue5_kernel(SaberBatch b) {
-  __shared__ __align__(16) uint8_t xbuf[2 * k5::kSmemPerWarp];
+// Several lanes per state (msponge.cuh; NS = 5: five lanes, six instances per warp; NS = 1:
+// a warp per instance).  Two warps per block: warp 0 the hash chain and GenSecret, warp 1
+// GenMatrix, for the same instances.
+template <int L, int OP, int NS>
+__global__ void __launch_bounds__(64) prologue_multi_kernel(SaberBatch b) {
+  using S = msp::Multi<NS>;
+  __shared__ __align__(16) uint8_t xbuf[2 * (S::SMEM_PER_WARP > 0 ? S::SMEM_PER_WARP : 16)];
   const int w = threadIdx.x >> 5;
-  const k5::Lanes k = k5::make_lanes(xbuf + w * k5::kSmemPerWarp);
-  const int g = (threadIdx.x & 31) / 5, i = blockIdx.x * 6 + g;
-  const bool live = g < 6 && i < b.n;
-  sdev::prologue5<L, OP>(inst_of<L>(b, live ? i : b.n - 1, OP), k, w, live);
+  const S s(xbuf + w * S::SMEM_PER_WARP);
+  const int g = s.state(), i = blockIdx.x * S::STATES_PER_WARP + g;
+  const bool live = g < S::STATES_PER_WARP && i < b.n;
+  sdev::prologue_multi<S, L, OP>(inst_of<L>(b, live ? i : b.n - 1, OP), s, w, live);
 }
 
-// Lanes per state of the prologue's sponges for a batch of n: five up to saber_five_max,
-// a pair (GenMatrix only) up to saber_pair_max, else one.
+template <int L, int OP, int NS>
+void launch_prologue_multi(const SaberBatch &b, cudaStream_t st) {
+  constexpr int spw = msp::Multi<NS>::STATES_PER_WARP;
+  prologue_multi_kernel<L, OP, NS><<<(b.n + spw - 1) / spw, 64, 0, st>>>(b);
+}
+
+// Lanes per state of the prologue's sponges for a batch of n: a warp per state up to
+// saber_warp_max, five lanes up to saber_five_max, a pair (GenMatrix only) up to
+// saber_pair_max, else one.
 template <int L, int OP>
 void launch_prologue(const SaberBatch &b, cudaStream_t st) {
   const int pb = (b.n + 31) / 32;
-  if (b.n <= tuning().saber_five_max) prologue5_kernel<L, OP><<<(b.n + 5) / 6, 64, 0, st>>>(b);
+  if (b.n <= tuning().saber_warp_max) launch_prologue_multi<L, OP, 1>(b, st);
+  else if (b.n <= tuning().saber_five_max) launch_prologue_multi<L, OP, 5>(b, st);
   else if (b.n <= tuning().saber_pair_max) prologue_kernel<L, OP, true><<<pb, 96, 0, st>>>(b);
   else prologue_kernel<L, OP, false><<<pb, 64, 0, st>>>(b);
 }
@@ -60,16 +69,32 @@ __global__ void __launch_bounds__(64) finish_enc_pair_kernel(SaberBatch b) {
   sdev::finish_enc_pair<L>(inst_of<L>(b, live ? i : b.n - 1, OP_ENC), t & 1, live);
 }
 
-// Encaps / keypair finish on five lanes per state, 32 threads = 6 instances.
-template <int L, int OP>
-__global__ void __launch_bounds__(32) finish5_kernel(SaberBatch b) {
-  __shared__ __align__(16) uint8_t xbuf[k5::kSmemPerWarp];
-  const k5::Lanes k = k5::make_lanes(xbuf);
-  const int g = threadIdx.x / 5, i = blockIdx.x * 6 + g;
-  const bool live = g < 6 && i < b.n;
+// Encaps / keypair finish on several lanes per state, one warp per block.
+template <int L, int OP, int NS>
+__global__ void __launch_bounds__(32) finish_multi_kernel(SaberBatch b) {
+  using S = msp::Multi<NS>;
+  __shared__ __align__(16) uint8_t xbuf[S::SMEM_PER_WARP > 0 ? S::SMEM_PER_WARP : 16];
+  const S s(xbuf);
+  const int g = s.state(), i = blockIdx.x * S::STATES_PER_WARP + g;
+  const bool live = g < S::STATES_PER_WARP && i < b.n;
   const sdev::Inst v = inst_of<L>(b, live ? i : b.n - 1, OP);
-  if (OP == OP_ENC) sdev::finish_enc5<L>(v, k, live);
-  else sdev::finish_kp5<L>(v, k, live);
+  if (OP == OP_ENC) sdev::finish_enc_multi<S, L>(v, s, live);
+  else sdev::finish_kp_multi<S, L>(v, s, live);
+}
+
+// The finish on a warp per state or five lanes per state when n is within the thresholds;
+// false otherwise.
+template <int L, int OP>
+bool launch_finish_multi(const SaberBatch &b, cudaStream_t st) {
+  if (b.n <= tuning().saber_finish_warp_max) {
+    finish_multi_kernel<L, OP, 1><<<b.n, 32, 0, st>>>(b);
+    return true;
+  }
+  if (b.n <= tuning().saber_finish_five_max) {
+    finish_multi_kernel<L, OP, 5><<<(b.n + 5) / 6, 32, 0, st>>>(b);
+    return true;
+  }
+  return false;
 }
 
 template <int L, int OP>
@@ -216,17 +241,17 @@ cudaError_t run(const SaberBatch &b, int op, int form, cudaStream_t st) {
       mark(b, st);
       if ((e = launch_product<L, sdev::PM_KEYPAIR>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
-      if (b.n <= tuning().saber_finish_five_max) finish5_kernel<L, OP_KEYPAIR><<<(b.n + 5) / 6, 32, 0, st>>>(b);
-      else finish_kernel<L, OP_KEYPAIR><<<fb, tb, 0, st>>>(b);
+      if (!launch_finish_multi<L, OP_KEYPAIR>(b, st)) finish_kernel<L, OP_KEYPAIR><<<fb, tb, 0, st>>>(b);
       break;
     case OP_ENC:
       launch_prologue<L, OP_ENC>(b, st);
       mark(b, st);
       if ((e = launch_product<L, sdev::PM_ENC>(b, form, st)) != cudaSuccess) return e;
       mark(b, st);
-      if (b.n <= tuning().saber_finish_five_max) finish5_kernel<L, OP_ENC><<<(b.n + 5) / 6, 32, 0, st>>>(b);
-      else if (b.n <= tuning().saber_pair_max) finish_enc_pair_kernel<L><<<(b.n + 31) / 32, 64, 0, st>>>(b);
-      else finish_kernel<L, OP_ENC><<<fb, tb, 0, st>>>(b);
+      if (!launch_finish_multi<L, OP_ENC>(b, st)) {
+        if (b.n <= tuning().saber_pair_max) finish_enc_pair_kernel<L><<<(b.n + 31) / 32, 64, 0, st>>>(b);
+        else finish_kernel<L, OP_ENC><<<fb, tb, 0, st>>>(b);
+      }
       break;
     default:
       if ((e = launch_product<L, sdev::PM_DEC_INNER>(b, form, st)) != cudaSuccess) return e;

@@ -30,8 +30,8 @@
 #pragma once
 #include "common.cuh"
 #include "keccak.cuh"
-#include "keccak5.cuh"
 #include "keccak_pair.cuh"
+#include "msponge.cuh"
 #include "tc.cuh"
 
 namespace dpkem {
@@ -278,126 +278,103 @@ __device__ __forceinline__ void finish_enc_pair(const Inst &v, int p, bool live)
   }
 }
 
-// ---------------------------------------------------------------- five lanes per state
-// The same prologue roles and encaps finish with each sponge spread over a group of five
-// lanes (keccak5.cuh): the bytes written are those of prologue_inst / finish_inst.  live =
-// false keeps a group without an instance in step (reads stay in bounds, writes skipped).
-
-// Lanes 0..3 of `src` (a finished state) moved to lanes D..D+3 of `dst`.
-template <int D>
-__device__ __forceinline__ void k5_move4(uint2 (&dst)[5], const uint2 (&src)[5], const k5::Lanes &k) {
-  k5::xor_lane<D + 0>(dst, k, k5::get<0>(src, k));
-  k5::xor_lane<D + 1>(dst, k, k5::get<1>(src, k));
-  k5::xor_lane<D + 2>(dst, k, k5::get<2>(src, k));
-  k5::xor_lane<D + 3>(dst, k, k5::get<3>(src, k));
-}
-
-// Store lanes 0 .. nw-1 of a state (8 bytes each) to dst.
-__device__ __forceinline__ void k5_store(const uint2 (&a)[5], const k5::Lanes &k, uint8_t *dst, int nw, bool live) {
-#pragma unroll
-  for (int y = 0; y < 2; y++) {
-    const int q = k.t + 5 * y;
-    if (q < nw && live) *reinterpret_cast<uint2 *>(dst + 8 * q) = a[y];
-  }
-}
-
-template <int L, int OP>
-__device__ __forceinline__ void prologue5(const Inst &v, const k5::Lanes &k, int role, bool live) {
+// ---------------------------------------------------------------- several lanes per state
+// The same prologue roles and encaps / keypair finish with each sponge spread over several
+// lanes (msponge.cuh: S = msp::Multi<5>, five lanes per state, or msp::Multi<1>, a warp per
+// state): the bytes written are those of prologue_inst / finish_inst.  live = false keeps a
+// state without an instance in step (reads stay in bounds, writes are skipped).
+template <class S, int L, int OP>
+__device__ __forceinline__ void prologue_multi(const Inst &v, const S &s, int role, bool live) {
   using P = SP<L>;
-  using S = Scr<L>;
+  using Q = Scr<L>;
   uint8_t *scr = v.scr;
-  uint2 a[5];
-  k5::zero(a);
+  uint2 a[S::NS];
+  msp::zero<S>(a);
   if (role == 1) {  // GenMatrix
     if (OP == OP_KEYPAIR) {  // seed_A = SHAKE128(coins[0:32], 32), published in pk
-      k5::absorb_aligned<168>(a, k, 0, v.coins, 32, live);
-      k5::absorb_finish<168>(a, k, 32, 0x1Fu);
-      k5_store(a, k, v.pk + P::POLYVECCOMP, 4, live);
-      if (k.t == 4) a[0] = make_uint2(0u, 0u);  // keep lanes 0..3 (the seed), clear the rest
-#pragma unroll
-      for (int y = 1; y < 5; y++) a[y] = make_uint2(0u, 0u);
+      msp::absorb_aligned<S, 168>(a, s, 0, v.coins, 32, live);
+      msp::absorb_finish<S, 168>(a, s, 32, 0x1Fu);
+      msp::store<S>(a, s, v.pk + P::POLYVECCOMP, 4, live);
+      msp::keep<S>(a, s, 4);
     } else {
       const uint8_t *src = OP == OP_ENC ? v.pk + P::POLYVECCOMP : v.sk + P::POLYVEC + P::POLYVECCOMP;
-      k5::absorb_aligned<168>(a, k, 0, src, 32, live);
+      msp::absorb_aligned<S, 168>(a, s, 0, src, 32, live);
     }
-    k5::absorb_finish<168>(a, k, 32, 0x1Fu);
-    k5::squeeze<168>(a, k, scr + S::ARAW, P::ARAW, live);
+    msp::absorb_finish<S, 168>(a, s, 32, 0x1Fu);
+    msp::squeeze<S, 168>(a, s, scr + Q::ARAW, P::ARAW, live);
     return;
   }
   if (OP == OP_KEYPAIR) {
-    k5::absorb_aligned<168>(a, k, 0, v.coins + 32, 32, live);
+    msp::absorb_aligned<S, 168>(a, s, 0, v.coins + 32, 32, live);
   } else {
-    uint2 kr[5];
-    k5::zero(kr);
+    uint2 kr[S::NS];
+    msp::zero<S>(kr);
     if (OP == OP_ENC) {
       // m = SHA3-256(coins), H(pk), kr = SHA3-512(m || H(pk))  (cuda_kernel.cu:68-70)
-      k5::absorb_aligned<136>(a, k, 0, v.coins, 32, live);
-      k5::absorb_finish<136>(a, k, 32, 0x06u);
-      k5_store(a, k, scr + S::MTXT, 4, live);
-      uint2 h[5];
-      k5::zero(h);
-      const int pos = k5::absorb_aligned<136>(h, k, 0, v.pk, P::PK, live);
-      k5::absorb_finish<136>(h, k, pos, 0x06u);
-      if (k.t == 4) a[0] = make_uint2(0u, 0u);  // lanes 0..3 = m
-#pragma unroll
-      for (int y = 1; y < 5; y++) a[y] = make_uint2(0u, 0u);
-      k5_move4<4>(a, h, k);
-#pragma unroll
-      for (int y = 0; y < 5; y++) kr[y] = a[y];
+      msp::absorb_aligned<S, 136>(kr, s, 0, v.coins, 32, live);
+      msp::absorb_finish<S, 136>(kr, s, 32, 0x06u);
+      msp::store<S>(kr, s, scr + Q::MTXT, 4, live);
+      msp::keep<S>(kr, s, 4);  // lanes 0..3 = m
+      const int pos = msp::absorb_aligned<S, 136>(a, s, 0, v.pk, P::PK, live);
+      msp::absorb_finish<S, 136>(a, s, pos, 0x06u);
+      msp::move4<S, 4>(kr, a, s);  // lanes 4..7 = H(pk)
     } else {
       // m' from the inner-product pass, H(pk) stored in sk (cuda_kernel.cu:231-232)
-      int pos = k5::absorb_aligned<72>(kr, k, 0, scr + S::MTXT, 32, live);
-      pos = k5::absorb_aligned<72>(kr, k, pos, v.sk + P::SK - 64, 32, live);
+      const int pos = msp::absorb_aligned<S, 72>(kr, s, 0, scr + Q::MTXT, 32, live);
+      msp::absorb_aligned<S, 72>(kr, s, pos, v.sk + P::SK - 64, 32, live);
     }
-    k5::absorb_finish<72>(kr, k, 64, 0x06u);
-    k5_store(kr, k, scr + S::KR, 8, live);
+    msp::absorb_finish<S, 72>(kr, s, 64, 0x06u);
+    msp::store<S>(kr, s, scr + Q::KR, 8, live);
     // GenSecret seed = kr[32:64] = lanes 4..7 -> lanes 0..3
-    k5::zero(a);
-    k5::xor_lane<0>(a, k, k5::get<4>(kr, k));
-    k5::xor_lane<1>(a, k, k5::get<5>(kr, k));
-    k5::xor_lane<2>(a, k, k5::get<6>(kr, k));
-    k5::xor_lane<3>(a, k, k5::get<7>(kr, k));
+    msp::zero<S>(a);
+    msp::xor_lane<S, 0>(a, s, s.template get<4>(kr));
+    msp::xor_lane<S, 1>(a, s, s.template get<5>(kr));
+    msp::xor_lane<S, 2>(a, s, s.template get<6>(kr));
+    msp::xor_lane<S, 3>(a, s, s.template get<7>(kr));
   }
-  k5::absorb_finish<168>(a, k, 32, 0x1Fu);
-  k5::squeeze<168>(a, k, scr + S::SRAW, P::SRAW, live);
+  msp::absorb_finish<S, 168>(a, s, 32, 0x1Fu);
+  msp::squeeze<S, 168>(a, s, scr + Q::SRAW, P::SRAW, live);
   if (OP == OP_DEC) {  // H(c) of the input ciphertext (see prologue_inst)
-    k5::zero(a);
-    const int pos = k5::absorb_aligned<136>(a, k, 0, v.ct, P::CT, live);
-    k5::absorb_finish<136>(a, k, pos, 0x06u);
-    k5_store(a, k, scr + S::HC, 4, live);
+    msp::zero<S>(a);
+    const int pos = msp::absorb_aligned<S, 136>(a, s, 0, v.ct, P::CT, live);
+    msp::absorb_finish<S, 136>(a, s, pos, 0x06u);
+    msp::store<S>(a, s, scr + Q::HC, 4, live);
   }
 }
 
 // Encaps finish: k = SHA3-256(kr[0:32] || SHA3-256(c)).
-template <int L>
-__device__ __forceinline__ void finish_enc5(const Inst &v, const k5::Lanes &k, bool live) {
+template <class S, int L>
+__device__ __forceinline__ void finish_enc_multi(const Inst &v, const S &s, bool live) {
   using P = SP<L>;
-  using S = Scr<L>;
-  uint2 h[5], a[5];
-  k5::zero(h);
-  const int pos = k5::absorb_aligned<136>(h, k, 0, v.ct, P::CT, live);
-  k5::absorb_finish<136>(h, k, pos, 0x06u);
-  k5::zero(a);
-  k5::absorb_aligned<136>(a, k, 0, v.scr + S::KR, 32, live);
-  k5_move4<4>(a, h, k);
-  k5::absorb_finish<136>(a, k, 64, 0x06u);
-  k5_store(a, k, v.ss, 4, live);
+  using Q = Scr<L>;
+  uint2 h[S::NS], a[S::NS];
+  msp::zero<S>(h);
+  const int pos = msp::absorb_aligned<S, 136>(h, s, 0, v.ct, P::CT, live);
+  msp::absorb_finish<S, 136>(h, s, pos, 0x06u);
+  msp::zero<S>(a);
+  msp::absorb_aligned<S, 136>(a, s, 0, v.scr + Q::KR, 32, live);
+  msp::move4<S, 4>(a, h, s);
+  msp::absorb_finish<S, 136>(a, s, 64, 0x06u);
+  msp::store<S>(a, s, v.ss, 4, live);
 }
 
 // Keypair finish: sk = s || pk || H(pk) || z (the secret part was written by the product).
-template <int L>
-__device__ __forceinline__ void finish_kp5(const Inst &v, const k5::Lanes &k, bool live) {
+template <class S, int L>
+__device__ __forceinline__ void finish_kp_multi(const Inst &v, const S &s, bool live) {
   using P = SP<L>;
-  if (live)
-    for (int off = 8 * k.t; off < P::PK; off += 40)
-      *reinterpret_cast<uint2 *>(v.sk + P::POLYVEC + off) = ld_lane(v.pk + off);
-  uint2 a[5];
-  k5::zero(a);
-  const int pos = k5::absorb_aligned<136>(a, k, 0, v.pk, P::PK, live);
-  k5::absorb_finish<136>(a, k, pos, 0x06u);
-  k5_store(a, k, v.sk + P::SK - 64, 4, live);
-  if (live && k.t < 4)
-    *reinterpret_cast<uint2 *>(v.sk + P::SK - 32 + 8 * k.t) = ld_lane(v.coins + 64 + 8 * k.t);
+  if (live && s.writer()) {
+    const int t = s.lane(0) % 5;  // five threads share the copy (a warp per state: lanes 0..4)
+    if (s.lane(0) < 5)
+      for (int off = 8 * t; off < P::PK; off += 40)
+        *reinterpret_cast<uint2 *>(v.sk + P::POLYVEC + off) = ld_lane(v.pk + off);
+  }
+  uint2 a[S::NS];
+  msp::zero<S>(a);
+  const int pos = msp::absorb_aligned<S, 136>(a, s, 0, v.pk, P::PK, live);
+  msp::absorb_finish<S, 136>(a, s, pos, 0x06u);
+  msp::store<S>(a, s, v.sk + P::SK - 64, 4, live);
+  const int q = s.lane(0);
+  if (live && s.writer() && q < 4) *reinterpret_cast<uint2 *>(v.sk + P::SK - 32 + 8 * q) = ld_lane(v.coins + 64 + 8 * q);
 }
 
 // ---------------------------------------------------------------- finish

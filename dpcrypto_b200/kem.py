@@ -137,7 +137,8 @@ def load() -> ctypes.CDLL:
 TUNING_PATH = os.path.join(HERE, "tuning.json")
 RUNTIME_KNOBS = ("thread_block", "mixed_frodo_task", "mixed_pair_task", "mixed_thread_task", "pipe_chunks",
                  "pipe_priority", "saber_pair_max", "saber_five_max", "saber_finish_five_max", "frodo_five_max",
-                 "frodo_ss_five_max", "saber_tc_ctas_per_sm")
+                 "frodo_ss_five_max", "saber_tc_ctas_per_sm", "saber_warp_max", "saber_finish_warp_max",
+                 "frodo_warp_max", "frodo_ss_warp_max")
 
 
 _tuning: dict = {}
@@ -321,7 +322,7 @@ class Engine:
 
     def keccak_lanes(self, lanes: int, states, perms: int = 1):
         """`perms` Keccak-f[1600] permutations of each row of `states` (an n x 25 torch CUDA
-        tensor of 64-bit lanes) in the given lanes-per-state layout (1, 2 or 5); returns a new
+        tensor of 64-bit lanes) in the given lanes-per-state layout (1, 2, 5 or 25); returns a new
         tensor.  The calling torch stream's pending work is synchronised first."""
         import torch
 

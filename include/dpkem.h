@@ -155,7 +155,7 @@ int dpkem_probe_int_peaks(dpkem_ctx *ctx, double *int_ops_per_s, double *keccak_
 int dpkem_probe_i8_mma_peak(dpkem_ctx *ctx, double *macs_per_s);
 
 /* Keccak-f[1600] in each lanes-per-state layout the sponge stages use (1: a thread per state,
- * 2: a bit-interleaved lane pair, 5: five lanes of a warp per state): `perms` permutations
+ * 2: a bit-interleaved lane pair, 5: five lanes of a warp, 25: a warp per state): `perms` permutations
  * applied to each of n states (25 little-endian 64-bit lanes each, device pointers, 8-byte
  * aligned); returns when done.  No counterpart in the reference (its permutation is
  * KeccakF1600_StatePermute, FrodoKEM976-GPU/src/shake.cu:66-331, one thread per state). */

@@ -57,13 +57,15 @@ def test_frodo_forms_agree_at_scale(engine, oracle):
 
 
 @pytest.mark.parametrize("form", [d.FORM_TC, d.FORM_DP4A])
-def test_frodo_sponges_on_five_lanes(engine, oracle, form):
+@pytest.mark.parametrize("layout", ["five", "warp"])
+def test_frodo_sponges_on_several_lanes(engine, oracle, form, layout):
     """Every thread-level sponge stage (keypair prologue, H(pk), both prologues, the
-    ciphertext pre-absorb and both final hashes) on five lanes per state, against the oracle;
-    n = 7 leaves a partial group of lanes, and tampered ciphertexts take the reject path."""
+    ciphertext pre-absorb and both final hashes) on five lanes per state or a warp per state,
+    against the oracle; n = 7 leaves a partial group of lanes, and tampered ciphertexts take
+    the reject path."""
     from dpcrypto_b200 import kem
 
-    knobs = ("frodo_five_max", "frodo_ss_five_max")
+    knobs = ("frodo_five_max", "frodo_ss_five_max") if layout == "five" else ("frodo_warp_max", "frodo_ss_warp_max")
     before = {k: kem.get_tuning().get(k, 0) for k in knobs}
     for k in knobs:
         kem.set_tuning(k, 1 << 30)

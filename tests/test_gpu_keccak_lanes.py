@@ -1,5 +1,5 @@
 """Keccak-f[1600] in every lanes-per-state layout the sponge stages use (one thread, a
-bit-interleaved lane pair, five lanes of a warp) against the CPU oracle's permutation, on
+bit-interleaved lane pair, five lanes of a warp, a warp per state) against the CPU oracle's permutation, on
 random and edge states, with batch sizes that leave partial warps and partial groups."""
 import numpy as np
 import pytest
@@ -8,7 +8,7 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("lanes", [1, 2, 5])
+@pytest.mark.parametrize("lanes", [1, 2, 5, 25])
 @pytest.mark.parametrize("n,perms", [(1, 1), (7, 1), (33, 3), (601, 2)])
 def test_keccak_lanes_match_oracle(engine, oracle, lanes, n, perms):
     rng = np.random.default_rng(n * 10 + lanes)

@@ -137,16 +137,19 @@ def test_saber_malformed_secret_key(engine, oracle, level, form):
 
 
 @pytest.mark.parametrize("level", LEVELS)
-@pytest.mark.parametrize("five", [0, 1 << 30])
-def test_saber_sponges_on_five_lanes(engine, oracle, level, five):
-    """The prologue and finish sponges on five lanes per state (saber_five_max /
-    saber_finish_five_max) or not, against the oracle, with batch sizes that leave partial
-    groups and partial warps (n = 1, 7, 45)."""
+@pytest.mark.parametrize("layout", ["one/pair", "five", "warp"])
+def test_saber_sponges_on_several_lanes(engine, oracle, level, layout):
+    """The prologue and finish sponges on one lane or a pair (the defaults), five lanes per
+    state (saber_five_max / saber_finish_five_max) or a warp per state (saber_warp_max /
+    saber_finish_warp_max), against the oracle, with batch sizes that leave partial groups and
+    partial warps (n = 1, 7, 45)."""
     from dpcrypto_b200 import kem
 
-    before = {k: kem.get_tuning().get(k, 0) for k in ("saber_five_max", "saber_finish_five_max")}
-    for k in before:
-        kem.set_tuning(k, five)
+    knobs = {"five": ("saber_five_max", "saber_finish_five_max"),
+             "warp": ("saber_warp_max", "saber_finish_warp_max")}.get(layout, ())
+    before = {k: kem.get_tuning().get(k, 0) for k in knobs}
+    for k in knobs:
+        kem.set_tuning(k, 1 << 30)
     try:
         for n in (1, 7, 45):
             kc, ec = oracle.coins(n, 96, "kp", first=91), oracle.coins(n, 32, "enc", first=91)
