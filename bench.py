@@ -470,6 +470,44 @@ def main():
             ares[name + "_roundtrip_ok"] = bool(torch.equal(ss, ss2))
         ares["tc_over_shake_tc"] = ares["tc"] / value
         line["frodo976aes_batch8192"] = dict(ares, unit=UNIT, note="AES blocks = 976 rows x 126 (12 x 10.5 per row)")
+        # The same batch under one key pair (a server decapsulating under its own key, clients
+        # encapsulating to it): A expanded once and read from memory by every instance's S'A
+        # stage, so that stage is the product alone in each form (the reference's own product
+        # stage, DoDP4Av5s, also reads A from memory) and the ratio of its times is the
+        # product-only tensor-core speed-up.
+        pk1, sk1 = pk[0].contiguous(), sk[0].contiguous()
+        amat = eng.expand_a(FS, pk1)
+        shared = {}
+        for name, f in (("tc", d.FORM_TC), ("dp4a", d.FORM_DP4A), ("int32", d.FORM_INT32)):
+            for _ in range(2):
+                c1, s1 = eng.enc_shared(FS, pk1, ec, f, amat)
+                eng.dec_shared(FS, c1, sk1, f, amat)
+            eng.profile(True)
+            c1, s1 = eng.enc_shared(FS, pk1, ec, f, amat)
+            es = eng.stage_times()
+            s2 = eng.dec_shared(FS, c1, sk1, f, amat)
+            ds = eng.stage_times()
+            eng.profile(False)
+            barrier()
+            shared[name + "_roundtrip_ok"] = bool(torch.equal(s1, s2))
+            reps = max(3, args.steps // 2)
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for _ in range(reps):
+                c1, s1 = eng.enc_shared(FS, pk1, ec, f, amat)
+                eng.dec_shared(FS, c1, sk1, f, amat)
+            t1.record(stream)
+            barrier()
+            shared[name] = world * B * reps / (t0.elapsed_time(t1) * 1e-3)
+            shared[name + "_stage_ms"] = {"enc": es, "dec": ds}
+            shared[name + "_product_ms"] = (es[1] + ds[2]) / 2
+        shared["tc_over_dp4a"] = shared["tc"] / shared["dp4a"]
+        shared["product_only_tc_over_dp4a"] = shared["dp4a_product_ms"] / shared["tc_product_ms"]
+        shared["product_only_tc_over_int32"] = shared["int32_product_ms"] / shared["tc_product_ms"]
+        shared["note"] = ("encaps to one pk and decaps with one sk, A expanded once (dpkem_frodo_expand_a); "
+                          "product_ms = the S'A stage reading A from memory, per 8192-instance launch")
+        line["frodo976_shared_key_batch8192"] = dict(shared, unit=UNIT)
+        line["forms"]["product_only_tc_over_dp4a"] = shared["product_only_tc_over_dp4a"]
 
         # Saber l=3, batch 4096 (configs' second workload)
         SB = 4096

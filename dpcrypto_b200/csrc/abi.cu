@@ -352,6 +352,68 @@ int run_op(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *
   return DPKEM_OK;
 }
 
+// Shared-key FrodoKEM batches (device pointers): op = OP_ENC runs n encapsulations to the
+// one public key `key` (coins = in0, ct = out0, ss = out1), op = OP_DEC n decapsulations with
+// the one secret key `key` (ct = in0, ss = out0).  amat: the key's A from
+// dpkem_frodo_expand_a, or null (then every instance still generates its rows).  Encaps
+// hashes pk once (H(pk) in the arena) instead of once per instance.
+int run_shared(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8_t *in0, const uint8_t *key,
+               const uint16_t *amat, uint8_t *out0, uint8_t *out1, void *stream) {
+  if (!c || (scheme != DPKEM_FRODO976 && scheme != DPKEM_FRODO976AES)) return DPKEM_EINVAL;
+  if (form != DPKEM_FORM_DP4A && form != DPKEM_FORM_TC && form != DPKEM_FORM_INT32) return DPKEM_EINVAL;
+  if (n == 0) return DPKEM_OK;
+  if (n > (size_t)INT32_MAX || !in0 || !key || !out0 || (op == OP_ENC && !out1)) return DPKEM_EINVAL;
+  if (!op_aligned(op, in0, key, out0, out1) || (amat && !aligned16(amat))) return DPKEM_EINVAL;
+  std::lock_guard<std::mutex> lock(c->mu);
+  if (cudaSetDevice(c->device) != cudaSuccess) return cuda_status(cudaErrorInvalidDevice);
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  const size_t chunk = std::min(n, chunk_for(c, scheme, op, false));
+  int rc = ensure_arena(c, arena_need(scheme, op, chunk, false) + kAlign);
+  if (rc) return rc;
+  cudaError_t e = cudaStreamWaitEvent(st, c->last, 0);
+  if (e != cudaSuccess) return cuda_status(e);
+  Carver cv{c->arena};
+  FrodoBatch fb{};
+  fb.rw = cv.take<uint16_t>(chunk * frodo::RW * 2);
+  fb.kk = cv.take<uint8_t>(chunk * 24);
+  fb.mu = cv.take<uint8_t>(chunk * 24);
+  fb.fail = cv.take<uint32_t>(chunk * 4);
+  fb.hs = cv.take<uint2>(chunk * 200);
+  uint8_t *pkh = cv.take<uint8_t>(kAlign);
+  fb.aes = scheme == DPKEM_FRODO976AES;
+  fb.err = c->d_err;
+  fb.shared = 1;
+  fb.amat = amat;
+  if (c->profile) {
+    c->timer.n = 0;
+    fb.timer = &c->timer;
+  }
+  if (op == OP_ENC) {
+    if ((e = frodo_pk_digest(key, pkh, st)) != cudaSuccess) return cuda_status(e);
+    fb.pkh = pkh;
+    fb.pk = const_cast<uint8_t *>(key);
+  } else {
+    fb.sk = const_cast<uint8_t *>(key);
+  }
+  for (size_t first = 0; first < n; first += chunk) {
+    fb.n = (int)std::min(chunk, n - first);
+    if (op == OP_ENC) {
+      fb.coins = in0 + first * frodo::ENC_COINS;
+      fb.ct = out0 + first * frodo::CT;
+      fb.ss = out1 + first * frodo::SS;
+      e = frodo_enc(fb, form, st);
+    } else {
+      fb.ct = const_cast<uint8_t *>(in0) + first * frodo::CT;
+      fb.ss = out0 + first * frodo::SS;
+      e = frodo_dec(fb, form, st);
+    }
+    if (e != cudaSuccess) return cuda_status(e);
+    if (fb.timer) c->timer_stages = fb.timer->n - 1;
+  }
+  if ((e = cudaEventRecord(c->last, st)) != cudaSuccess) return cuda_status(e);
+  return DPKEM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -711,6 +773,26 @@ int dpkem_probe_int_peaks(dpkem_ctx *c, double *int_ops_per_s, double *keccak_pe
   return set_status(cuda_status(probe_int_peaks(c->stream, int_ops_per_s, keccak_per_s)));
 }
 
+int dpkem_frodo_expand_a(dpkem_ctx *c, int scheme, const uint8_t *pk, uint16_t *amat, void *stream) {
+  if (!c || !pk || !amat || (scheme != DPKEM_FRODO976 && scheme != DPKEM_FRODO976AES) || !aligned16(pk) ||
+      !aligned16(amat))
+    return set_status(DPKEM_EINVAL);
+  std::lock_guard<std::mutex> lock(c->mu);
+  if (cudaSetDevice(c->device) != cudaSuccess) return set_status(cuda_status(cudaErrorInvalidDevice));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  return set_status(cuda_status(frodo_expand_a(scheme == DPKEM_FRODO976AES, pk, amat, st)));
+}
+
+int dpkem_frodo_enc_shared(dpkem_ctx *c, int scheme, int form, size_t n, const uint8_t *coins, const uint8_t *pk,
+                           const uint16_t *amat, uint8_t *ct, uint8_t *ss, void *stream) {
+  return set_status(run_shared(c, scheme, form, OP_ENC, n, coins, pk, amat, ct, ss, stream));
+}
+
+int dpkem_frodo_dec_shared(dpkem_ctx *c, int scheme, int form, size_t n, const uint8_t *ct, const uint8_t *sk,
+                           const uint16_t *amat, uint8_t *ss, void *stream) {
+  return set_status(run_shared(c, scheme, form, OP_DEC, n, ct, sk, amat, ss, nullptr, stream));
+}
+
 int dpkem_keccak_f1600_lanes(dpkem_ctx *c, int lanes, size_t n, const uint64_t *in, uint64_t *out, int perms) {
   if (!c || (lanes != 1 && lanes != 2 && lanes != 5 && lanes != 25) || perms < 0 || n > (size_t)INT32_MAX)
     return set_status(DPKEM_EINVAL);
@@ -796,6 +878,29 @@ int dpkem_set_tuning(const char *key, int value) {
     return set_status(DPKEM_EINVAL);
   }
   return set_status(DPKEM_OK);
+}
+
+int dpkem_get_tuning(const char *key, int *value) {
+  if (!key || !value) return set_status(DPKEM_EINVAL);
+  const Tuning &t = tuning();
+  const std::string k(key);
+  const struct {
+    const char *name;
+    int v;
+  } knobs[] = {{"thread_block", t.thread_block}, {"mixed_frodo_task", t.mixed_frodo_task},
+               {"mixed_pair_task", t.mixed_pair_task}, {"mixed_thread_task", t.mixed_thread_task},
+               {"pipe_chunks", t.pipe_chunks}, {"pipe_priority", t.pipe_priority},
+               {"saber_pair_max", t.saber_pair_max}, {"saber_warp_max", t.saber_warp_max},
+               {"saber_finish_warp_max", t.saber_finish_warp_max}, {"saber_five_max", t.saber_five_max},
+               {"saber_finish_five_max", t.saber_finish_five_max}, {"frodo_warp_max", t.frodo_warp_max},
+               {"frodo_ss_warp_max", t.frodo_ss_warp_max}, {"frodo_five_max", t.frodo_five_max},
+               {"frodo_ss_five_max", t.frodo_ss_five_max}, {"saber_tc_ctas_per_sm", t.saber_tc_ctas_per_sm}};
+  for (const auto &kn : knobs)
+    if (k == kn.name) {
+      *value = kn.v;
+      return set_status(DPKEM_OK);
+    }
+  return set_status(DPKEM_EINVAL);
 }
 
 const char *dpkem_strerror(int s) {

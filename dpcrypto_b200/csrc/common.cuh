@@ -46,12 +46,12 @@ struct Tuning {
   int pipe_chunks = 4;          // chunks (one stream each) of a pipelined host-mode batch, <= 8
   int pipe_priority = 1;        // 1: chunk streams get descending priorities (earlier chunks finish first)
   int saber_pair_max = 6144;    // largest Saber batch whose prologue runs GenMatrix on lane pairs (0: never)
-  int saber_warp_max = 0;       // largest Saber batch whose prologue sponges run on a warp per state (0: never)
-  int saber_finish_warp_max = 0;  // the same for the encaps / keypair finish
+  int saber_warp_max = 512;     // largest Saber batch whose prologue sponges run on a warp per state (0: never)
+  int saber_finish_warp_max = 1024;  // the same for the encaps / keypair finish
   int saber_five_max = 0;       // largest Saber batch whose prologue sponges run on five lanes per state (0: never)
   int saber_finish_five_max = 0;  // the same for the encaps / keypair finish
-  int frodo_warp_max = 0;       // largest Frodo batch whose prologues run on a warp per state (0: never)
-  int frodo_ss_warp_max = 0;    // the same for H(pk) and the final hash
+  int frodo_warp_max = 1024;    // largest Frodo batch whose prologues run on a warp per state (0: never)
+  int frodo_ss_warp_max = 1024; // the same for H(pk) and the final hash
   int frodo_five_max = 0;       // largest Frodo batch whose prologues run on five lanes per state (0: never)
   int frodo_ss_five_max = 0;    // the same for H(pk) and the final hash
   int saber_tc_ctas_per_sm = 0; // persistent Saber tensor-core product CTAs per SM (0: a CTA per instance)
@@ -85,6 +85,12 @@ struct FrodoBatch {
   uint2 *hs;             // scratch [n][25]: SHAKE256 state after absorbing ct's full blocks (dec)
   uint32_t *err;         // device error word (DEV_ERR_*)
   StageTimer *timer;     // optional
+  // One key for the whole batch (enc: one pk, dec: one sk): pk / sk are not strided, A may
+  // come expanded from memory (amat, 976 x 976 LE u16, rows of 1952 bytes) instead of being
+  // regenerated by every instance, and encaps reads H(pk) from pkh (24 bytes) when given.
+  int shared;
+  const uint16_t *amat;
+  const uint8_t *pkh;
 };
 
 struct SaberBatch {
@@ -109,6 +115,10 @@ struct CoinsBatch {
 cudaError_t frodo_keypair(const FrodoBatch &b, int form, cudaStream_t st);
 cudaError_t frodo_enc(const FrodoBatch &b, int form, cudaStream_t st);
 cudaError_t frodo_dec(const FrodoBatch &b, int form, cudaStream_t st);
+// Shared-key helpers: A of one public key (aes: the AES-128 variant) into amat (976 x 976
+// LE u16), and H(pk) = SHAKE256(pk, 24) of one public key into out.
+cudaError_t frodo_expand_a(int aes, const uint8_t *pk, uint16_t *amat, cudaStream_t st);
+cudaError_t frodo_pk_digest(const uint8_t *pk, uint8_t *out, cudaStream_t st);
 
 cudaError_t saber_keypair(const SaberBatch &b, int form, cudaStream_t st);
 cudaError_t saber_enc(const SaberBatch &b, int form, cudaStream_t st);

@@ -187,8 +187,41 @@ cudaError_t launch_sa_g(const FrodoBatch &b, int form, cudaStream_t st) {
 
 template <int MODE>
 cudaError_t launch_sa(const FrodoBatch &b, int form, cudaStream_t st) {
+  if (b.amat) return launch_sa_g<MODE, fdev::MemRows, fdev::MemRows, kTcStages>(b, form, st);
   if (b.aes) return launch_sa_g<MODE, fdev::AesRowsFull, fdev::AesRowsHalf, 1>(b, form, st);
   return launch_sa_g<MODE, fdev::ShakeRows, fdev::ShakeRows, kTcStages>(b, form, st);
+}
+
+// A (976 x 976 LE u16, row-major) of the public key pk, one row per thread, with the same
+// row generators as the S'A stages (SHAKE128 or AES-128 rows).
+template <class G>
+__global__ void __launch_bounds__(256) expand_a_kernel(const uint8_t *pk, uint16_t *amat) {
+  extern __shared__ __align__(16) uint8_t gmem[];
+  G gen;
+  gen.setup(pk, gmem);
+  __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  uint2 a[25];
+  gen.start(a, j);
+  uint2 *row = reinterpret_cast<uint2 *>(amat + (size_t)j * N);
+  for (int blk = 0; blk < 12; blk++) {
+    gen.next(a);
+#pragma unroll
+    for (int q = 0; q < 21; q++)
+      if (84 * blk + 4 * q < N) row[21 * blk + q] = a[q];
+  }
+}
+
+// H(pk) = SHAKE256(pk, 24) of one public key, on a warp (a warp per state).
+__global__ void __launch_bounds__(32) pk_digest_kernel(const uint8_t *pk, uint8_t *out) {
+  using S = msp::Multi<1>;
+  const S s(nullptr);
+  uint2 a[1];
+  msp::zero<S>(a);
+  const int pos = msp::absorb_aligned<S, 136>(a, s, 0, pk, PK, true);
+  msp::absorb_finish<S, 136>(a, s, pos, 0x1Fu);
+  msp::store<S>(a, s, out, 3, true);
 }
 
 template <class G, int NST>
@@ -216,6 +249,22 @@ inline void mark(const FrodoBatch &b, cudaStream_t st) {
 }
 
 }  // namespace
+
+cudaError_t frodo_expand_a(int aes, const uint8_t *pk, uint16_t *amat, cudaStream_t st) {
+  cudaError_t e;
+  if (aes) {
+    if ((e = set_smem(expand_a_kernel<fdev::AesRowsFull>, fdev::AesRowsFull::SMEM)) != cudaSuccess) return e;
+    expand_a_kernel<fdev::AesRowsFull><<<blocks_for(N, 256), 256, fdev::AesRowsFull::SMEM, st>>>(pk, amat);
+  } else {
+    expand_a_kernel<fdev::ShakeRows><<<blocks_for(N, 256), 256, 0, st>>>(pk, amat);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t frodo_pk_digest(const uint8_t *pk, uint8_t *out, cudaStream_t st) {
+  pk_digest_kernel<<<1, 32, 0, st>>>(pk, out);
+  return cudaGetLastError();
+}
 
 cudaError_t frodo_keypair(const FrodoBatch &b, int form, cudaStream_t st) {
   if (b.n <= 0) return cudaSuccess;

@@ -33,13 +33,16 @@ struct Inst {
   uint8_t *kk, *mu;      // 24 B each
   uint32_t *fail;
   uint2 *hs;             // 25 lanes: SHAKE256 state after ct's full blocks (decaps)
+  const uint16_t *amat;  // A expanded in memory (shared-key batches), or null
+  const uint8_t *pkh;    // H(pk) precomputed (shared-key encaps), or null
 };
 
 __device__ __forceinline__ Inst inst_of(const FrodoBatch &b, int i, int op) {
   Inst v;
   v.coins = b.coins ? b.coins + (size_t)i * (op == OP_KEYPAIR ? KP_COINS : ENC_COINS) : nullptr;
-  v.pk = b.pk ? b.pk + (size_t)i * PK : nullptr;
-  v.sk = b.sk ? b.sk + (size_t)i * SK : nullptr;
+  const size_t ik = b.shared ? 0 : (size_t)i;  // shared-key batches: one pk / sk for all
+  v.pk = b.pk ? b.pk + ik * PK : nullptr;
+  v.sk = b.sk ? b.sk + ik * SK : nullptr;
   v.ct = b.ct ? b.ct + (size_t)i * CT : nullptr;
   v.ss = b.ss ? b.ss + (size_t)i * SS : nullptr;
   v.rw = b.rw + (size_t)i * RW;
@@ -47,6 +50,8 @@ __device__ __forceinline__ Inst inst_of(const FrodoBatch &b, int i, int op) {
   v.mu = b.mu + (size_t)i * LENMU;
   v.fail = b.fail + i;
   v.hs = b.hs ? b.hs + (size_t)i * 25 : nullptr;
+  v.amat = b.amat;
+  v.pkh = b.pkh;
   return v;
 }
 
@@ -158,9 +163,14 @@ template <int MODE>
 __device__ __forceinline__ void prologue_inst(const Inst &v) {
   uint2 a[25], pkh[3], mu[3];
   if (MODE == OP_ENC) {
-    keccak_zero(a);
-    const int pos = absorb_aligned<136>(a, 0, v.pk, PK);
-    absorb_finish<136>(a, pos, 0x1Fu);
+    if (v.pkh) {  // shared-key batch: H(pk) hashed once
+#pragma unroll
+      for (int q = 0; q < 3; q++) a[q] = ld_lane(v.pkh + 8 * q);
+    } else {
+      keccak_zero(a);
+      const int pos = absorb_aligned<136>(a, 0, v.pk, PK);
+      absorb_finish<136>(a, pos, 0x1Fu);
+    }
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       pkh[q] = a[q];
@@ -313,12 +323,16 @@ __device__ __forceinline__ void prologue_multi(const Inst &v, const S &s, bool l
   uint2 a[S::NS], g[S::NS];
   msp::zero<S>(g);
   if (MODE == OP_ENC) {
-    msp::zero<S>(a);
-    const int pos = msp::absorb_aligned<S, 136>(a, s, 0, v.pk, PK, live);
-    msp::absorb_finish<S, 136>(a, s, pos, 0x1Fu);
+    if (v.pkh) {  // shared-key batch: H(pk) hashed once
+      msp::absorb_aligned<S, 136>(g, s, 0, v.pkh, 24, live);
+    } else {
+      msp::zero<S>(a);
+      const int pos = msp::absorb_aligned<S, 136>(a, s, 0, v.pk, PK, live);
+      msp::absorb_finish<S, 136>(a, s, pos, 0x1Fu);
 #pragma unroll
-    for (int y = 0; y < S::NS; y++)
-      if (s.lane(y) < 3) g[y] = a[y];  // pkh = lanes 0..2
+      for (int y = 0; y < S::NS; y++)
+        if (s.lane(y) < 3) g[y] = a[y];  // pkh = lanes 0..2
+    }
     msp::absorb_aligned<S, 136>(g, s, 24, v.coins, 24, live);
   } else {
     msp::absorb_aligned<S, 136>(g, s, 0, v.sk + SK_PKH, 24, live);
@@ -445,6 +459,26 @@ struct ShakeRows {
   }
   __device__ __forceinline__ void start(uint2 (&a)[25], uint32_t j) { row_init(a, j, sa0, sa1); }
   __device__ __forceinline__ void next(uint2 (&a)[25]) { keccak_f1600(a); }
+};
+
+// MemRows: rows of an A expanded once in memory (976 x 976 LE u16, row-major; shared-key
+// batches, where every instance's A is the same).  setup() receives A's address in place of
+// the seed.  Entries past column 975 of the last block are zero; padding rows (j >= 976)
+// read row 975, and their secret words are zero, so they add nothing.
+struct MemRows {
+  static constexpr int SMEM = 0;
+  const uint2 *base, *row;
+  int col;
+  __device__ __forceinline__ void setup(const uint8_t *amat, uint8_t *) { base = reinterpret_cast<const uint2 *>(amat); }
+  __device__ __forceinline__ void start(uint2 (&)[25], uint32_t j) {
+    row = base + (size_t)(j < (uint32_t)N ? j : N - 1) * (N / 4);
+    col = 0;
+  }
+  __device__ __forceinline__ void next(uint2 (&a)[25]) {
+#pragma unroll
+    for (int q = 0; q < 21; q++) a[q] = col + 4 * q < N ? row[col / 4 + q] : make_uint2(0u, 0u);
+    col += 84;
+  }
 };
 
 // AES-128 (FIPS 197) tables, evaluated at compile time from the definitions: the S-box is
@@ -666,7 +700,7 @@ __device__ __forceinline__ void sa_dp4a_cta(const Inst &v, uint8_t *smem) {
   uint32_t(*red)[64] = reinterpret_cast<uint32_t(*)[64]>(smem + 83200);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint16_t *rw = v.rw;
-  const uint8_t *seed = MODE == OP_ENC ? v.pk : v.sk + LENS;
+  const uint8_t *seed = v.amat ? reinterpret_cast<const uint8_t *>(v.amat) : MODE == OP_ENC ? v.pk : v.sk + LENS;
   for (int q = tid; q < N * NBAR; q += 256) acc[q] = 0;
   for (int q = tid; q < (ROWS_PAD / 4) * NBAR; q += 256) {
     const int qd = q >> 3, k = q & 7;
@@ -785,7 +819,7 @@ __device__ __forceinline__ bool sa_tc_cta(const Inst &v, uint8_t *smem, uint32_t
   uint32_t(*red)[64] = reinterpret_cast<uint32_t(*)[64]>(smem + L::red);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint16_t *rw = v.rw;
-  const uint8_t *seed = MODE == OP_ENC ? v.pk : v.sk + LENS;
+  const uint8_t *seed = v.amat ? reinterpret_cast<const uint8_t *>(v.amat) : MODE == OP_ENC ? v.pk : v.sk + LENS;
 
   for (int q = tid; q < 62 * NBAR; q += 256) {
     const int g = q >> 3, k = q & 7;

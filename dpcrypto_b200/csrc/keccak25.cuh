@@ -7,11 +7,11 @@
 //   theta  the other four lanes of column x by four shuffles, C[x] by XOR; C[x-1], C[x+1]
 //          from the threads of the same row by two more
 //   rho    its lane rotated by rho(x, y) (a per-thread offset: keccak5.cuh's rotv)
-//   pi     one shuffle: thread (x, y) takes the lane that pi moves to (x, y), from thread
-//          (x + 3y mod 5) + 5x
-//   chi    the row neighbours (x+1, y), (x+2, y) by two shuffles
+//   pi+chi one level of three shuffles: thread (x, y) takes the lanes that pi moves to
+//          (x, y), (x+1, y) and (x+2, y) straight from their threads (the lane pi moves to
+//          (x', y) comes from thread (x' + 3y mod 5) + 5x'), then chi is local
 //   iota   on thread 0
-// Four dependent shuffle levels (a shuffle is 26 cycles on B200, measured) and about 16
+// Three dependent shuffle levels (a shuffle is 26 cycles on B200, measured) and about 16
 // integer instructions per thread and round, against 180 on one thread.  A warp holds one
 // state instead of 32, so the layout pays only while the batch leaves warps' issue slots
 // free; lanes per state is a tuning knob of each stage.
@@ -31,8 +31,7 @@ struct Lane {
   int i;                 // lane index x + 5y this thread holds (threads 25..31: a copy of i - 25)
   int col[4];            // threads holding (x, y+1 .. y+4)
   int left, right;       // (x-1, y), (x+1, y)
-  int pisrc;             // the thread whose lane pi moves to (x, y)
-  int chi1, chi2;        // (x+1, y), (x+2, y)
+  int pi[3];             // the threads whose lanes pi moves to (x, y), (x+1, y), (x+2, y)
   uint32_t rot, swap;    // rho(x, y) mod 32, all-ones when rho >= 32
   uint32_t iota;         // all-ones on thread 0
 };
@@ -46,9 +45,11 @@ __device__ __forceinline__ Lane make_lane() {
   for (int d = 1; d < 5; d++) k.col[d - 1] = x + 5 * ((y + d) % 5);
   k.left = (x + 4) % 5 + 5 * y;
   k.right = (x + 1) % 5 + 5 * y;
-  k.pisrc = (x + 3 * y) % 5 + 5 * x;
-  k.chi1 = (x + 1) % 5 + 5 * y;
-  k.chi2 = (x + 2) % 5 + 5 * y;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const int xp = (x + d) % 5;
+    k.pi[d] = (xp + 3 * y) % 5 + 5 * xp;
+  }
   int r = 0;
 #pragma unroll
   for (int j = 0; j < 25; j++)
@@ -66,15 +67,14 @@ __device__ __forceinline__ void round25(uint2 &v, const Lane &k, uint2 rcv) {
   const uint2 cl = k5::shfl(c, k.left), cr = rotl64<1>(k5::shfl(c, k.right));
   v = xor3(v, cl, cr);
   v = k5::rotv(v, k.rot, k.swap);
-  const uint2 b = k5::shfl(v, k.pisrc);
-  const uint2 b1 = k5::shfl(b, k.chi1), b2 = k5::shfl(b, k.chi2);
+  const uint2 b = k5::shfl(v, k.pi[0]), b1 = k5::shfl(v, k.pi[1]), b2 = k5::shfl(v, k.pi[2]);
   v = chi(b, b1, b2);
   v.x ^= rcv.x & k.iota;
   v.y ^= rcv.y & k.iota;
 }
 
 __device__ __forceinline__ void f1600(uint2 &v, const Lane &k) {
-#pragma unroll 1
+#pragma unroll 4
   for (int r = 0; r < 24; r++) round25(v, k, c_keccak_rc[r]);
 }
 

@@ -69,6 +69,14 @@ EXPORTS = {
     "dpkem_probe_int_peaks": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_double)]),
     "dpkem_probe_i8_mma_peak": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    "dpkem_frodo_expand_a": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p]),
+    "dpkem_frodo_enc_shared": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_size_t,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_void_p]),
+    "dpkem_frodo_dec_shared": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_size_t,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_void_p]),
     "dpkem_keccak_f1600_lanes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p,
                                                 ctypes.c_void_p, ctypes.c_int]),
     "dpkem_probe_keccak_chain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -77,6 +85,7 @@ EXPORTS = {
                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_void_p]),
     "dpkem_set_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
+    "dpkem_get_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
     "dpkem_strerror": (ctypes.c_char_p, [ctypes.c_int]),
     "dpkem_last_status": (ctypes.c_int, []),
     "dpkem_set_compat_batch": (None, [ctypes.c_size_t]),
@@ -165,6 +174,32 @@ def apply_tuning(path: str = TUNING_PATH) -> dict:
                 raise DpkemError(rc, f"tuning {k}={chosen[k]}")
             _tuning[k] = int(chosen[k])
     return chosen
+
+
+def tuning_value(key: str) -> int:
+    """The library's current value of a knob (its compiled default unless set)."""
+    v = ctypes.c_int()
+    rc = load().dpkem_get_tuning(key.encode(), ctypes.byref(v))
+    if rc != OK:
+        raise DpkemError(rc, f"get_tuning({key})")
+    return v.value
+
+
+class knobs:
+    """Context manager: set knobs for a block, restore their previous values after."""
+
+    def __init__(self, **values):
+        self.values = values
+
+    def __enter__(self):
+        self.saved = {k: tuning_value(k) for k in self.values}
+        for k, v in self.values.items():
+            set_tuning(k, v)
+        return self
+
+    def __exit__(self, *exc):
+        for k, v in self.saved.items():
+            set_tuning(k, v)
 
 
 def set_tuning(key: str, value: int) -> None:
@@ -299,6 +334,39 @@ class Engine:
         flags, st = self._mode(out)
         self._check(self._lib.dpkem_coins(self._h, n, length, first, tag.encode(), _ptr(out), flags, st), "coins")
         return out
+
+    # -- FrodoKEM batches under one key (torch CUDA tensors, current torch stream) -------
+    def expand_a(self, scheme: int, pk):
+        """A of one public key pk (a 1-D uint8 CUDA tensor) as a 976 x 976 int16 tensor."""
+        import torch
+
+        amat = torch.empty((976, 976), dtype=torch.int16, device=pk.device)
+        flags, st = self._mode(pk)
+        self._check(self._lib.dpkem_frodo_expand_a(self._h, scheme, _ptr(pk), ctypes.c_void_p(amat.data_ptr()), st),
+                    "frodo_expand_a")
+        return amat
+
+    def enc_shared(self, scheme: int, pk, coins, form: int = FORM_TC, amat=None):
+        """n encapsulations to the one public key pk (1-D); coins (n, 24); returns (ct, ss)."""
+        z = sizes(scheme)
+        n = self._rows(coins, z["enc_coins"], "coins")
+        ct, ss = self._alloc(coins, n, z["ct"]), self._alloc(coins, n, z["ss"])
+        flags, st = self._mode(coins, pk, ct, ss)
+        a = ctypes.c_void_p(amat.data_ptr()) if amat is not None else None
+        self._check(self._lib.dpkem_frodo_enc_shared(self._h, scheme, form, n, _ptr(coins), _ptr(pk), a, _ptr(ct),
+                                                    _ptr(ss), st), "frodo_enc_shared")
+        return ct, ss
+
+    def dec_shared(self, scheme: int, ct, sk, form: int = FORM_TC, amat=None):
+        """n decapsulations with the one secret key sk (1-D); ct (n, 15744); returns ss."""
+        z = sizes(scheme)
+        n = self._rows(ct, z["ct"], "ct")
+        ss = self._alloc(ct, n, z["ss"])
+        flags, st = self._mode(ct, sk, ss)
+        a = ctypes.c_void_p(amat.data_ptr()) if amat is not None else None
+        self._check(self._lib.dpkem_frodo_dec_shared(self._h, scheme, form, n, _ptr(ct), _ptr(sk), a, _ptr(ss), st),
+                    "frodo_dec_shared")
+        return ss
 
     def sync(self, stream=None):
         self._check(self._lib.dpkem_sync(self._h, stream), "sync")

@@ -154,6 +154,22 @@ int dpkem_probe_int_peaks(dpkem_ctx *ctx, double *int_ops_per_s, double *keccak_
  * tcgen05.mma kind::i8 (u8 x s8, s32 accumulators in TMEM); int8 multiply-adds per second. */
 int dpkem_probe_i8_mma_peak(dpkem_ctx *ctx, double *macs_per_s);
 
+/* ---- FrodoKEM batches under one key (device pointers, enqueued on `stream`) ----
+ * Many encapsulations to one public key, or many decapsulations with one secret key (a
+ * server decapsulating under its own key): the n instances share the key's matrix A, so it
+ * can be expanded once (dpkem_frodo_expand_a: A as 976 x 976 little-endian u16, row-major,
+ * 1,905,152 bytes, 16-byte aligned) and read by every instance's S'A stage instead of being
+ * regenerated by each (amat NULL keeps the generation).  Encaps also hashes pk once.  Byte
+ * layouts are the batched calls'; results equal dpkem_enc_batch / dpkem_dec_batch with the
+ * key repeated n times.  dpkem_sync() reports device-side errors.  No counterpart in the
+ * reference, whose instances all regenerate A (FrodoKEM976-GPU/src/cuda_kernel.cu:172-173,
+ * :302-303). */
+int dpkem_frodo_expand_a(dpkem_ctx *ctx, int scheme, const uint8_t *pk, uint16_t *amat, void *stream);
+int dpkem_frodo_enc_shared(dpkem_ctx *ctx, int scheme, int form, size_t n, const uint8_t *coins, const uint8_t *pk,
+                           const uint16_t *amat, uint8_t *ct, uint8_t *ss, void *stream);
+int dpkem_frodo_dec_shared(dpkem_ctx *ctx, int scheme, int form, size_t n, const uint8_t *ct, const uint8_t *sk,
+                           const uint16_t *amat, uint8_t *ss, void *stream);
+
 /* Keccak-f[1600] in each lanes-per-state layout the sponge stages use (1: a thread per state,
  * 2: a bit-interleaved lane pair, 5: five lanes of a warp, 25: a warp per state): `perms` permutations
  * applied to each of n states (25 little-endian 64-bit lanes each, device pointers, 8-byte
@@ -190,6 +206,8 @@ int dpkem_saber_enc_batch_static(int scheme, int form, size_t n, const uint8_t *
  * instances run GenMatrix on two lanes per state, larger ones on one; 0 = never).  Chosen by
  * dpcrypto_b200/autotune.py and stored in dpcrypto_b200/tuning.json. */
 int dpkem_set_tuning(const char *key, int value);
+/* Current value of a knob (DPKEM_EINVAL for an unknown key). */
+int dpkem_get_tuning(const char *key, int *value);
 
 const char *dpkem_strerror(int status);
 /* Status of the last call made by this thread (the compatibility shims return void). */

@@ -71,6 +71,7 @@ def test_tuning_knobs():
     try:
         for k in kem.RUNTIME_KNOBS:
             assert lib.dpkem_set_tuning(k.encode(), 32 if k == "thread_block" else 1) == kem.OK, k
+            assert kem.tuning_value(k) == (32 if k == "thread_block" else 1), k
         for k in ("saber_pair_max", "saber_five_max", "saber_finish_five_max", "frodo_five_max", "frodo_ss_five_max",
                   "saber_tc_ctas_per_sm", "saber_warp_max", "saber_finish_warp_max", "frodo_warp_max",
                   "frodo_ss_warp_max"):
@@ -84,7 +85,7 @@ def test_tuning_knobs():
         defaults = {"thread_block": 64, "mixed_frodo_task": 256, "mixed_pair_task": 128, "mixed_thread_task": 256,
                     "pipe_chunks": 4, "pipe_priority": 1, "saber_pair_max": 6144, "saber_five_max": 0,
                     "saber_finish_five_max": 0, "frodo_five_max": 0, "frodo_ss_five_max": 0,
-                    "saber_tc_ctas_per_sm": 0, "saber_warp_max": 0, "saber_finish_warp_max": 0,
-                    "frodo_warp_max": 0, "frodo_ss_warp_max": 0}
+                    "saber_tc_ctas_per_sm": 0, "saber_warp_max": 512, "saber_finish_warp_max": 1024,
+                    "frodo_warp_max": 1024, "frodo_ss_warp_max": 1024}
         for k in kem.RUNTIME_KNOBS:
             lib.dpkem_set_tuning(k.encode(), saved.get(k, defaults[k]))

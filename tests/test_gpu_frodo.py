@@ -57,19 +57,19 @@ def test_frodo_forms_agree_at_scale(engine, oracle):
 
 
 @pytest.mark.parametrize("form", [d.FORM_TC, d.FORM_DP4A])
-@pytest.mark.parametrize("layout", ["five", "warp"])
+@pytest.mark.parametrize("layout", ["one", "five", "warp"])
 def test_frodo_sponges_on_several_lanes(engine, oracle, form, layout):
     """Every thread-level sponge stage (keypair prologue, H(pk), both prologues, the
-    ciphertext pre-absorb and both final hashes) on five lanes per state or a warp per state,
-    against the oracle; n = 7 leaves a partial group of lanes, and tampered ciphertexts take
-    the reject path."""
+    ciphertext pre-absorb and both final hashes) on one lane, five lanes per state or a warp
+    per state, against the oracle; n = 7 leaves a partial group of lanes, and tampered
+    ciphertexts take the reject path."""
     from dpcrypto_b200 import kem
 
-    knobs = ("frodo_five_max", "frodo_ss_five_max") if layout == "five" else ("frodo_warp_max", "frodo_ss_warp_max")
-    before = {k: kem.get_tuning().get(k, 0) for k in knobs}
-    for k in knobs:
-        kem.set_tuning(k, 1 << 30)
-    try:
+    big = 1 << 30
+    sel = {"one": dict(frodo_warp_max=0, frodo_ss_warp_max=0, frodo_five_max=0, frodo_ss_five_max=0),
+           "five": dict(frodo_warp_max=0, frodo_ss_warp_max=0, frodo_five_max=big, frodo_ss_five_max=big),
+           "warp": dict(frodo_warp_max=big, frodo_ss_warp_max=big)}[layout]
+    with kem.knobs(**sel):
         n = 7
         kc, ec = oracle.coins(n, 64, "kp", first=61), oracle.coins(n, 24, "enc", first=61)
         pk_o, sk_o = oracle.keypair(0, kc, threads=8)
@@ -81,6 +81,3 @@ def test_frodo_sponges_on_several_lanes(engine, oracle, form, layout):
         assert (engine.dec(d.FRODO976, ct_o, sk_o, form) == ss_o).all()
         bad = _tamper(ct_o)
         assert (engine.dec(d.FRODO976, bad, sk_o, form) == oracle.dec(0, bad, sk_o, threads=8)).all()
-    finally:
-        for k, v in before.items():
-            kem.set_tuning(k, v)

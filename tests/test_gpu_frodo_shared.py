@@ -1,0 +1,52 @@
+"""FrodoKEM batches under one key: A expanded once (dpkem_frodo_expand_a) against the oracle's
+rows, and n encapsulations to one public key / n decapsulations with one secret key, with A
+from memory or regenerated, in every product form, byte for byte against the oracle."""
+import numpy as np
+import pytest
+import torch
+
+import dpcrypto_b200 as d
+
+pytestmark = pytest.mark.gpu
+FORMS = [d.FORM_TC, d.FORM_DP4A, d.FORM_INT32]
+
+
+def _tamper(ct):
+    bad = ct.copy()
+    for i in range(bad.shape[0]):
+        bad[i, (i * 7919) % bad.shape[1]] ^= 1 << (i % 8)
+    return bad
+
+
+@pytest.mark.parametrize("scheme", [d.FRODO976, d.FRODO976AES])
+def test_expand_a_matches_oracle_rows(engine, oracle, scheme):
+    kc = oracle.coins(1, 64, "kp", first=314)
+    pk, _ = oracle.keypair(scheme, kc)
+    amat = engine.expand_a(scheme, torch.from_numpy(pk[0].copy()).cuda()).cpu().numpy().view(np.uint16)
+    gen = oracle.frodo_gen_row if scheme == d.FRODO976 else oracle.frodo_gen_row_aes
+    for i in (0, 1, 255, 256, 511, 974, 975):
+        assert (amat[i] == gen(pk[0, :16].tobytes(), i)).all(), i
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("scheme", [d.FRODO976, d.FRODO976AES])
+@pytest.mark.parametrize("with_a", [True, False])
+def test_shared_key_enc_dec_match_oracle(engine, oracle, scheme, form, with_a):
+    n = 9
+    kc = oracle.coins(1, 64, "kp", first=271)
+    pk, sk = oracle.keypair(scheme, kc)
+    ec = oracle.coins(n, 24, "enc", first=271)
+    pk_n, sk_n = np.repeat(pk, n, axis=0), np.repeat(sk, n, axis=0)
+    ct_o, ss_o = oracle.enc(scheme, pk_n, ec, threads=8)
+    bad = _tamper(ct_o)
+    ssb_o = oracle.dec(scheme, bad, sk_n, threads=8)
+    dpk, dsk = torch.from_numpy(pk[0].copy()).cuda(), torch.from_numpy(sk[0].copy()).cuda()
+    amat = engine.expand_a(scheme, dpk) if with_a else None
+    ct, ss = engine.enc_shared(scheme, dpk, torch.from_numpy(ec).cuda(), form, amat)
+    torch.cuda.synchronize()
+    assert (ct.cpu().numpy() == ct_o).all() and (ss.cpu().numpy() == ss_o).all()
+    ss2 = engine.dec_shared(scheme, torch.from_numpy(ct_o).cuda(), dsk, form, amat)
+    ss3 = engine.dec_shared(scheme, torch.from_numpy(bad).cuda(), dsk, form, amat)
+    torch.cuda.synchronize()
+    assert (ss2.cpu().numpy() == ss_o).all()
+    assert (ss3.cpu().numpy() == ssb_o).all()

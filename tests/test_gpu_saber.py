@@ -47,13 +47,13 @@ def test_saber_reference_fixture(engine, oracle, saber_tv, form):
 @pytest.mark.parametrize("level", LEVELS)
 @pytest.mark.parametrize("pair_max", [0, 1 << 30])
 def test_saber_prologue_lanes_per_state(engine, oracle, level, pair_max):
-    """GenMatrix on one lane per state and on a lane pair (the saber_pair_max knob) give the
-    oracle's bytes, a partial last warp included."""
+    """GenMatrix on one lane per state and on a lane pair (the saber_pair_max knob, with the
+    five-lane and warp-per-state thresholds off) give the oracle's bytes, a partial last warp
+    included."""
     from dpcrypto_b200 import kem
 
-    before = kem.get_tuning().get("saber_pair_max", 6144)
-    kem.set_tuning("saber_pair_max", pair_max)
-    try:
+    with kem.knobs(saber_pair_max=pair_max, saber_warp_max=0, saber_five_max=0, saber_finish_warp_max=0,
+                   saber_finish_five_max=0):
         n = 45
         kc, ec = oracle.coins(n, 96, "kp", first=77), oracle.coins(n, 32, "enc", first=77)
         pk_o, sk_o = oracle.keypair(level, kc, threads=8)
@@ -63,8 +63,6 @@ def test_saber_prologue_lanes_per_state(engine, oracle, level, pair_max):
         ct, ss = engine.enc(level, pk_o, ec, d.FORM_TC)
         assert (ct == ct_o).all() and (ss == ss_o).all()
         assert (engine.dec(level, ct_o, sk_o, d.FORM_TC) == ss_o).all()
-    finally:
-        kem.set_tuning("saber_pair_max", before)
 
 
 def _unpack13(b):
@@ -139,18 +137,17 @@ def test_saber_malformed_secret_key(engine, oracle, level, form):
 @pytest.mark.parametrize("level", LEVELS)
 @pytest.mark.parametrize("layout", ["one/pair", "five", "warp"])
 def test_saber_sponges_on_several_lanes(engine, oracle, level, layout):
-    """The prologue and finish sponges on one lane or a pair (the defaults), five lanes per
-    state (saber_five_max / saber_finish_five_max) or a warp per state (saber_warp_max /
+    """The prologue and finish sponges on one lane or a pair, five lanes per state
+    (saber_five_max / saber_finish_five_max) or a warp per state (saber_warp_max /
     saber_finish_warp_max), against the oracle, with batch sizes that leave partial groups and
     partial warps (n = 1, 7, 45)."""
     from dpcrypto_b200 import kem
 
-    knobs = {"five": ("saber_five_max", "saber_finish_five_max"),
-             "warp": ("saber_warp_max", "saber_finish_warp_max")}.get(layout, ())
-    before = {k: kem.get_tuning().get(k, 0) for k in knobs}
-    for k in knobs:
-        kem.set_tuning(k, 1 << 30)
-    try:
+    big = 1 << 30
+    sel = {"one/pair": dict(saber_warp_max=0, saber_finish_warp_max=0, saber_five_max=0, saber_finish_five_max=0),
+           "five": dict(saber_warp_max=0, saber_finish_warp_max=0, saber_five_max=big, saber_finish_five_max=big),
+           "warp": dict(saber_warp_max=big, saber_finish_warp_max=big)}[layout]
+    with kem.knobs(**sel):
         for n in (1, 7, 45):
             kc, ec = oracle.coins(n, 96, "kp", first=91), oracle.coins(n, 32, "enc", first=91)
             pk_o, sk_o = oracle.keypair(level, kc, threads=8)
@@ -163,9 +160,6 @@ def test_saber_sponges_on_several_lanes(engine, oracle, level, layout):
                 assert (engine.dec(level, ct_o, sk_o, form) == ss_o).all()
                 bad = _tamper(ct_o)
                 assert (engine.dec(level, bad, sk_o, form) == oracle.dec(level, bad, sk_o, threads=8)).all()
-    finally:
-        for k, v in before.items():
-            kem.set_tuning(k, v)
 
 
 @pytest.mark.parametrize("level", LEVELS)
@@ -176,9 +170,7 @@ def test_saber_tc_product_persistent(engine, oracle, level, per_sm):
     gives every CTA two or three instances), against the oracle, reject path included."""
     from dpcrypto_b200 import kem
 
-    before = kem.get_tuning().get("saber_tc_ctas_per_sm", 0)
-    kem.set_tuning("saber_tc_ctas_per_sm", per_sm)
-    try:
+    with kem.knobs(saber_tc_ctas_per_sm=per_sm):
         n = 333
         kc, ec = oracle.coins(n, 96, "kp", first=123), oracle.coins(n, 32, "enc", first=123)
         pk_o, sk_o = oracle.keypair(level, kc, threads=8)
@@ -190,5 +182,3 @@ def test_saber_tc_product_persistent(engine, oracle, level, per_sm):
         assert (engine.dec(level, ct_o, sk_o, d.FORM_TC) == ss_o).all()
         bad = _tamper(ct_o)
         assert (engine.dec(level, bad, sk_o, d.FORM_TC) == oracle.dec(level, bad, sk_o, threads=8)).all()
-    finally:
-        kem.set_tuning("saber_tc_ctas_per_sm", before)
