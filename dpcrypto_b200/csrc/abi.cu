@@ -839,7 +839,7 @@ int dpkem_set_tuning(const char *key, int value) {
   const bool zero_ok = k == "pipe_priority" || k == "saber_pair_max" || k == "saber_five_max" ||
                        k == "saber_finish_five_max" || k == "frodo_five_max" || k == "frodo_ss_five_max" ||
                        k == "saber_tc_ctas_per_sm" || k == "saber_warp_max" || k == "saber_finish_warp_max" ||
-                       k == "frodo_warp_max" || k == "frodo_ss_warp_max";
+                       k == "frodo_warp_max" || k == "frodo_ss_warp_max" || k == "mixed_warp_max";
   if (value == 0 && !zero_ok) return set_status(DPKEM_EINVAL);
   if (k == "thread_block") {
     if (value % 32 || value > 256) return set_status(DPKEM_EINVAL);
@@ -864,6 +864,8 @@ int dpkem_set_tuning(const char *key, int value) {
     t.frodo_five_max = value;
   } else if (k == "frodo_ss_five_max") {
     t.frodo_ss_five_max = value;
+  } else if (k == "mixed_warp_max") {
+    t.mixed_warp_max = value;
   } else if (k == "saber_warp_max") {
     t.saber_warp_max = value;
   } else if (k == "saber_finish_warp_max") {
@@ -889,6 +891,7 @@ int dpkem_get_tuning(const char *key, int *value) {
     int v;
   } knobs[] = {{"thread_block", t.thread_block}, {"mixed_frodo_task", t.mixed_frodo_task},
                {"mixed_pair_task", t.mixed_pair_task}, {"mixed_thread_task", t.mixed_thread_task},
+               {"mixed_warp_max", t.mixed_warp_max},
                {"pipe_chunks", t.pipe_chunks}, {"pipe_priority", t.pipe_priority},
                {"saber_pair_max", t.saber_pair_max}, {"saber_warp_max", t.saber_warp_max},
                {"saber_finish_warp_max", t.saber_finish_warp_max}, {"saber_five_max", t.saber_five_max},

@@ -47,6 +47,12 @@ __host__ __device__ constexpr int form_of(int code) { return code & 3; }
 // ciphertext pre-absorb), 1 = CTA (one instance per task).
 enum Kind : int { K_THREAD = 0, K_CTA = 1, K_THREAD2 = 2 };
 
+// Task code flag: a thread-level stage run on a warp per instance (and role): the Keccak
+// sponges spread over the warp's lanes (keccak25.cuh), 8 instances per task (4 for two-role
+// stages).  The planner uses it for groups small enough that one thread per instance would
+// leave the GPU idle (knob mixed_warp_max).
+constexpr int kWarpTask = 1 << 10;
+
 __host__ __device__ constexpr int nstages(int scheme, int op) { return op == OP_DEC ? 4 : 3; }
 
 __host__ __device__ constexpr int kind_of(int scheme, int op, int stage) {
@@ -200,6 +206,60 @@ __device__ __forceinline__ void saber_thread(const Plan &p, int op, int stage, c
   }
 }
 
+// The same stages on a warp per instance (a warp-wide call: every lane runs it).
+template <int L>
+__device__ __forceinline__ void saber_warp(const Plan &p, int op, int stage, const DevReq &r, int role) {
+  using S = msp::Multi<1>;
+  const S s(nullptr);
+  sdev::Inst v = saber_view<L>(r);
+  if (r.gen && stage == 0 && op != OP_DEC) {
+    uint8_t *slot = const_cast<uint8_t *>(r.in0) + (role ? 96 : 0);
+    if ((role == 0 || op == OP_KEYPAIR) && (threadIdx.x & 31) == 0) draw_coins(p, r, slot);
+    __syncwarp();
+    v.coins = slot;
+  }
+  if (op == OP_KEYPAIR) {
+    if (stage == 0) sdev::prologue_multi<S, L, OP_KEYPAIR>(v, s, role, true);
+    else sdev::finish_kp_multi<S, L>(v, s, true);
+  } else if (op == OP_ENC) {
+    if (stage == 0) sdev::prologue_multi<S, L, OP_ENC>(v, s, role, true);
+    else sdev::finish_enc_multi<S, L>(v, s, true);
+  } else {
+    if (stage == 1) sdev::prologue_multi<S, L, OP_DEC>(v, s, role, true);
+    else if ((threadIdx.x & 31) == 0) sdev::finish_inst<L, OP_DEC>(v);  // one permutation
+  }
+}
+
+__device__ __forceinline__ void warp_stage(const Plan &p, int code, const DevReq &r, int role) {
+  using S = msp::Multi<1>;
+  const int scheme = scheme_of(code), op = op_of(code), stage = stage_of(code);
+  if (scheme <= 1) {
+    if (r.gen && stage == 0 && op != OP_DEC) {
+      if ((threadIdx.x & 31) == 0) draw_coins(p, r, const_cast<uint8_t *>(r.in0));
+      __syncwarp();
+    }
+    const S s(nullptr);
+    const fdev::Inst v = frodo_view(r);
+    if (op == OP_KEYPAIR) {
+      if (stage == 0) fdev::kp_prologue_multi<S>(v, s, true);
+      else fdev::pk_hash_multi<S>(v, s, true);
+    } else if (op == OP_ENC) {
+      if (stage == 0) fdev::prologue_multi<S, OP_ENC>(v, s, true);
+      else fdev::ss_multi<S, OP_ENC>(v, s, true);
+    } else {
+      if (stage == 1 && role == 0) fdev::prologue_multi<S, OP_DEC>(v, s, true);
+      else if (stage == 1) fdev::ct_absorb_multi<S>(v, s, true);
+      else fdev::ss_multi<S, OP_DEC>(v, s, true);
+    }
+  } else if (scheme == 2) {
+    saber_warp<2>(p, op, stage, r, role);
+  } else if (scheme == 3) {
+    saber_warp<3>(p, op, stage, r, role);
+  } else {
+    saber_warp<4>(p, op, stage, r, role);
+  }
+}
+
 __device__ __forceinline__ void thread_stage(const Plan &p, int code, const DevReq &r, int role) {
   const int scheme = scheme_of(code), op = op_of(code), stage = stage_of(code);
   if (scheme <= 1) {
@@ -321,6 +381,19 @@ __global__ void __launch_bounds__(256, 2) mixed_kernel(Plan p) {
       if (s_ready) cta_stage(code, p.req[r], smem, tbase, p.err);  // skipped after an error: the batch drains
       __syncthreads();
       if (tid == 0) mark_done(p, r);
+    } else if (code & kWarpTask) {
+      const int warp = tid >> 5, lane = tid & 31;
+      const int slot = kind == K_THREAD2 ? warp >> 1 : warp, role = kind == K_THREAD2 ? warp & 1 : 0;
+      if (slot < tk.count) {  // warp-uniform: every lane of the warp runs the stage
+        const uint32_t r = p.idx[tk.first + slot];
+        int ok = 0;
+        if (lane == 0) ok = wait_done(p, r, need) ? 1 : 0;
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (ok) warp_stage(p, code, p.req[r], role);
+        __threadfence();  // every lane's writes, before the count that publishes them
+        __syncwarp();
+        if (lane == 0) atomicAdd(p.done + r, 1u);
+      }
     } else {
       const int per = kind == K_THREAD2 ? 128 : 256;
       const int slot = tid % per, role = tid / per;
@@ -375,6 +448,15 @@ int task_size(int scheme, int kind) {
   return std::max(1, std::min(v, cap));
 }
 
+// Whether a thread-level stage of a group of `count` requests runs as warp tasks (a warp
+// per instance), and the instances per task either way.
+bool warp_tasks(int kind, size_t count) { return kind != K_CTA && count <= (size_t)tuning().mixed_warp_max; }
+int task_per(int scheme, int kind, size_t count) {
+  if (kind == K_CTA) return 1;
+  if (warp_tasks(kind, count)) return kind == K_THREAD2 ? 4 : 8;
+  return task_size(scheme, kind);
+}
+
 // Bytes of device memory a plan for these requests needs (tables + scratch records).
 size_t plan_bytes(const Req *reqs, size_t n, size_t *ntasks_out) {
   size_t scr = 0, ntasks = 0, nidx = 0;
@@ -389,7 +471,7 @@ size_t plan_bytes(const Req *reqs, size_t n, size_t *ntasks_out) {
       if (!c) continue;
       for (int st = 0; st < nstages(s, op); st++) {
         const int kind = kind_of(s, op, st);
-        const size_t per = kind == K_CTA ? 1 : (size_t)task_size(s, kind);
+        const size_t per = (size_t)task_per(s, kind, c);
         ntasks += (c + per - 1) / per;
         nidx += c;
       }
@@ -463,7 +545,8 @@ cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *
     owner.assign(R.size(), -1);
     for (int stg = 0; stg < nstages(scheme, op); stg++) {
       const int kind = kind_of(scheme, op, stg);
-      const int per = kind == K_CTA ? 1 : task_size(scheme, kind);
+      const int per = task_per(scheme, kind, R.size());
+      const bool warp = warp_tasks(kind, R.size());
       const uint32_t base = (uint32_t)nid;
       std::memcpy(idx + nid, R.data(), R.size() * 4);
       nid += R.size();
@@ -471,9 +554,11 @@ cudaError_t plan_build(const Req *reqs, size_t n, int form, int slots, uint8_t *
         const int cnt = (int)std::min<size_t>(per, R.size() - a);
         const int id = (int)ht.size();
         const int lo = owner_prev[a], hi = owner_prev[a + cnt - 1];
-        const double dur = est_us(scheme, op, stg, cnt);
+        // a warp per instance runs a sponge chain in about half the time of one thread
+        const double dur = est_us(scheme, op, stg, cnt) * (warp ? 0.45 : 1.0);
         const int prio = kind == K_CTA ? (dur > 500 ? 2 : 1) : 0;  // latency-bound thread stages first
-        ht.push_back(HostTask{Task{(uint16_t)code_of(scheme, op, stg, form), (uint16_t)cnt, base + (uint32_t)a}, dur,
+        const int code = code_of(scheme, op, stg, form) | (warp ? kWarpTask : 0);
+        ht.push_back(HostTask{Task{(uint16_t)code, (uint16_t)cnt, base + (uint32_t)a}, dur,
                               0.0, lo >= 0 ? hi - lo + 1 : 0, INT32_MAX, -1, prio});
         for (int k = 0; k < cnt; k++) owner[a + k] = id;
         for (int d = lo; lo >= 0 && d <= hi; d++) {

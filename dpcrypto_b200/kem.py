@@ -147,7 +147,7 @@ TUNING_PATH = os.path.join(HERE, "tuning.json")
 RUNTIME_KNOBS = ("thread_block", "mixed_frodo_task", "mixed_pair_task", "mixed_thread_task", "pipe_chunks",
                  "pipe_priority", "saber_pair_max", "saber_five_max", "saber_finish_five_max", "frodo_five_max",
                  "frodo_ss_five_max", "saber_tc_ctas_per_sm", "saber_warp_max", "saber_finish_warp_max",
-                 "frodo_warp_max", "frodo_ss_warp_max")
+                 "frodo_warp_max", "frodo_ss_warp_max", "mixed_warp_max")
 
 
 _tuning: dict = {}

@@ -74,7 +74,7 @@ def test_tuning_knobs():
             assert kem.tuning_value(k) == (32 if k == "thread_block" else 1), k
         for k in ("saber_pair_max", "saber_five_max", "saber_finish_five_max", "frodo_five_max", "frodo_ss_five_max",
                   "saber_tc_ctas_per_sm", "saber_warp_max", "saber_finish_warp_max", "frodo_warp_max",
-                  "frodo_ss_warp_max"):
+                  "frodo_ss_warp_max", "mixed_warp_max"):
             assert lib.dpkem_set_tuning(k.encode(), 0) == kem.OK  # 0 = never on lane pairs / five lanes
         assert lib.dpkem_set_tuning(b"pipe_priority", 0) == kem.OK
         assert lib.dpkem_set_tuning(b"thread_block", 0) == kem.EINVAL
@@ -86,6 +86,6 @@ def test_tuning_knobs():
                     "pipe_chunks": 4, "pipe_priority": 1, "saber_pair_max": 6144, "saber_five_max": 0,
                     "saber_finish_five_max": 0, "frodo_five_max": 0, "frodo_ss_five_max": 0,
                     "saber_tc_ctas_per_sm": 0, "saber_warp_max": 512, "saber_finish_warp_max": 1024,
-                    "frodo_warp_max": 1024, "frodo_ss_warp_max": 1024}
+                    "frodo_warp_max": 1024, "frodo_ss_warp_max": 1024, "mixed_warp_max": 512}
         for k in kem.RUNTIME_KNOBS:
             lib.dpkem_set_tuning(k.encode(), saved.get(k, defaults[k]))

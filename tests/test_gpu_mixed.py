@@ -127,3 +127,49 @@ def test_mixed_null_inputs_rejected(engine):
     with pytest.raises(d.DpkemError) as e:  # decaps needs its ciphertext even with a key
         engine.mixed([(d.SABER, 2, None, sk, oss, None)], d.FORM_TC, coin_key=bytes(32))
     assert e.value.status == d.kem.EINVAL
+
+
+@pytest.mark.parametrize("warp", [0, 1 << 20])
+@pytest.mark.parametrize("form", [d.FORM_TC, d.FORM_DP4A])
+def test_mixed_warp_tasks(engine, oracle_check_items, warp, form):
+    """The sponge stages of a mixed batch as thread tasks (a thread per instance) or as warp
+    tasks (a warp per instance and role; mixed_warp_max), every scheme and op, tampered
+    decaps included: equal to the batched calls and, on every fifth request, to the oracle."""
+    from dpcrypto_b200 import kem
+
+    with kem.knobs(mixed_warp_max=warp):
+        items, expect = _mixed_case(engine, 7, 5, form)
+        engine.mixed(items, form)
+        engine.sync()
+        torch.cuda.synchronize()
+    for pairs in expect:
+        for got, ref in pairs:
+            assert torch.equal(got, ref)
+    assert oracle_check_items(items, stride=5) >= 20
+
+
+@pytest.mark.parametrize("warp", [0, 1 << 20])
+def test_mixed_warp_tasks_device_coins(engine, oracle, warp):
+    """Keypair requests without coins draw them inside the kernel; with warp tasks one lane
+    draws them for its warp.  With key 00..1F the stream is the oracle's coins(i, "kp"), so the
+    key pairs must equal the oracle's for those coins."""
+    from dpcrypto_b200 import kem
+
+    key = bytes(range(32))
+    with kem.knobs(mixed_warp_max=warp):
+        items, outs = [], []
+        for scheme in (d.FRODO976, d.SABER):
+            z = d.sizes(scheme)
+            for i in range(3):
+                opk = torch.empty(z["pk"], dtype=torch.uint8, device="cuda")
+                osk = torch.empty(z["sk"], dtype=torch.uint8, device="cuda")
+                items.append((scheme, 0, None, None, opk, osk))
+                outs.append((scheme, len(items) - 1, opk, osk))
+        engine.mixed(items, d.FORM_TC, coin_key=key, coin_first=40)
+        engine.sync()
+        torch.cuda.synchronize()
+    for scheme, pos, opk, osk in outs:
+        z = d.sizes(scheme)
+        kc = oracle.coins(1, z["kp_coins"], "kp", first=40 + pos)
+        pk_o, sk_o = oracle.keypair(scheme, kc)
+        assert (opk.cpu().numpy() == pk_o[0]).all() and (osk.cpu().numpy() == sk_o[0]).all()
