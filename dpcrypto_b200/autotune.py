@@ -8,15 +8,21 @@ Knobs:
   mixed_thread_task  instances per other thread-level task
   pipe_chunks        chunks (one stream each) of a pipelined host-buffer batch
   pipe_priority      chunk streams with descending priorities (earlier chunks finish first)
-  saber_pair_max     Keccak lanes per state in the Saber prologue: batches of up to this many
-                     instances run GenMatrix on lane pairs (shorter chain while SM
-                     sub-partitions idle), larger ones on one lane (fewer issue slots per
-                     state); the sweep times both at 2k-16k instances and keeps the crossover
+  lanes per state    per sponge stage (Saber prologue, Saber encaps finish, Frodo prologue,
+                     Frodo shared-secret hash) and batch size: a warp per state
+                     (*_warp_max), five lanes (*_five_max), a lane pair (saber_pair_max,
+                     Saber only) or one lane.  Each layout is forced in turn at 64-16k
+                     instances and timed with the stage timer; a layout covers batches up
+                     to the largest swept size at which it was the fastest
+  saber_tc_ctas_per_sm  persistent Saber tensor-core product (CTAs per SM) or a CTA per
+                     instance (0)
+  mixed_warp_max     groups of up to this many instances run their sponge stages as warp
+                     tasks in the persistent mixed kernel
 Not knobs, with the measured reason recorded in the output: the MMA tile shape (the int8
 MMAs are <1 % of the tensor pipe: M = 128 is the smallest tile that keeps one TMEM lane per
-output row) and Keccak lanes per state in the throughput-bound kernels (the fused S'A
-stages and the persistent mixed kernel keep one state per thread: a pair costs more issue
-slots per state on an integer pipe those kernels already saturate).
+output row) and Keccak lanes per state in the fused S'A stages (their row generators keep
+one state per thread: those kernels already saturate the integer pipe, where a split state
+costs more issue slots per state).
 
     python -m dpcrypto_b200.autotune --build          # build variants (CPU, nvcc)
     python -m dpcrypto_b200.autotune --measure        # on a B200: sweep, write tuning.json
@@ -146,33 +152,156 @@ def _child(u: int) -> dict:
                 eng.dec(d.FRODO976, h_ct, h_sk, d.FORM_TC, out=h_ss2)
             psweep[f"{pc}/{prio}"] = (time.perf_counter() - t0) / 3 * 1e3
     res["pipe_chunks_priority_ms"] = psweep
-    # Keccak lanes per state in the Saber l=3 prologue, by batch size: encaps + decaps, device buffers
-    def saber_time(n: int) -> float:
-        kc = torch.empty((n, 96), dtype=torch.uint8, device="cuda")
-        sc = torch.empty((n, 32), dtype=torch.uint8, device="cuda")
-        eng.coins(n, 96, "tune-kp", out=kc)
-        eng.coins(n, 32, "tune-enc", out=sc)
-        spk, ssk = eng.keypair(d.SABER, kc, d.FORM_TC)
-        sct = torch.empty((n, 1088), dtype=torch.uint8, device="cuda")
-        sss = torch.empty((n, 32), dtype=torch.uint8, device="cuda")
-        for _ in range(2):
-            eng.enc(d.SABER, spk, sc, d.FORM_TC, out=(sct, sss))
-            eng.dec(d.SABER, sct, ssk, d.FORM_TC)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(10):
-            eng.enc(d.SABER, spk, sc, d.FORM_TC, out=(sct, sss))
-            eng.dec(d.SABER, sct, ssk, d.FORM_TC)
-        torch.cuda.synchronize()
-        return (time.perf_counter() - t0) / 10 * 1e3
-
-    lsweep = {}
-    for n in (2048, 4096, 8192, 16384):
-        for name, val in (("one", 0), ("pair", 1 << 30)):
-            kem.set_tuning("saber_pair_max", val)
-            lsweep[f"{n}/{name}"] = saber_time(n)
-    res["saber_lanes_ms"] = lsweep
+    res.update(_lanes_sweep(eng, d, kem))
     return res
+
+# Lanes per state of each sponge stage, by batch size.  Every layout is forced in turn with
+# the thresholds of the stage (a warp per state first, then five lanes, then the pair, else
+# one lane); the stage's device time comes from the stage timer of an encaps + decaps.
+BIG = 1 << 30
+SABER_SIZES = (64, 256, 512, 1024, 2048, 4096, 8192, 16384)
+FRODO_SIZES = (64, 256, 512, 1024, 2048, 4096)
+LAYOUTS = {
+    # stage: {layout: knob values}, and the stage timer slots (encaps, decaps) it owns
+    "saber_prologue": ({"warp": dict(saber_warp_max=BIG),
+                        "five": dict(saber_warp_max=0, saber_five_max=BIG),
+                        "pair": dict(saber_warp_max=0, saber_five_max=0, saber_pair_max=BIG),
+                        "one": dict(saber_warp_max=0, saber_five_max=0, saber_pair_max=0)}, (0,), (1,)),
+    "saber_finish": ({"warp": dict(saber_finish_warp_max=BIG),
+                      "five": dict(saber_finish_warp_max=0, saber_finish_five_max=BIG),
+                      "pair": dict(saber_finish_warp_max=0, saber_finish_five_max=0, saber_pair_max=BIG),
+                      "one": dict(saber_finish_warp_max=0, saber_finish_five_max=0, saber_pair_max=0)}, (2,), ()),
+    "frodo_prologue": ({"warp": dict(frodo_warp_max=BIG),
+                        "five": dict(frodo_warp_max=0, frodo_five_max=BIG),
+                        "one": dict(frodo_warp_max=0, frodo_five_max=0)}, (0,), (1,)),
+    "frodo_ss": ({"warp": dict(frodo_ss_warp_max=BIG),
+                  "five": dict(frodo_ss_warp_max=0, frodo_ss_five_max=BIG),
+                  "one": dict(frodo_ss_warp_max=0, frodo_ss_five_max=0)}, (2,), (3,)),
+}
+
+
+def _lanes_sweep(eng, d, kem) -> dict:
+    import numpy as np
+    import torch
+
+    def keys(scheme, n):
+        z = kem.sizes(scheme)
+        kc = torch.empty((n, z["kp_coins"]), dtype=torch.uint8, device="cuda")
+        ec = torch.empty((n, z["enc_coins"]), dtype=torch.uint8, device="cuda")
+        eng.coins(n, z["kp_coins"], "tune-kp", out=kc)
+        eng.coins(n, z["enc_coins"], "tune-enc", out=ec)
+        pk, sk = eng.keypair(scheme, kc, d.FORM_TC)
+        ct = torch.empty((n, z["ct"]), dtype=torch.uint8, device="cuda")
+        ss = torch.empty((n, z["ss"]), dtype=torch.uint8, device="cuda")
+        return pk, sk, ec, ct, ss
+
+    def stage_ms(scheme, inputs, enc_slots, dec_slots, reps=5):
+        pk, sk, ec, ct, ss = inputs
+        eng.enc(scheme, pk, ec, d.FORM_TC, out=(ct, ss))
+        eng.dec(scheme, ct, sk, d.FORM_TC)
+        torch.cuda.synchronize()
+        eng.profile(True)
+        ts = []
+        for _ in range(reps):
+            eng.enc(scheme, pk, ec, d.FORM_TC, out=(ct, ss))
+            e = eng.stage_times()
+            eng.dec(scheme, ct, sk, d.FORM_TC)
+            x = eng.stage_times()
+            ts.append(sum(e[k] for k in enc_slots) + sum(x[k] for k in dec_slots))
+        eng.profile(False)
+        return float(np.median(ts))
+
+    out = {}
+    for stage, (layouts, es, ds) in LAYOUTS.items():
+        scheme = d.SABER if stage.startswith("saber") else d.FRODO976
+        sweep = {}
+        for n in SABER_SIZES if scheme == d.SABER else FRODO_SIZES:
+            inputs = keys(scheme, n)
+            for name, kv in layouts.items():
+                with kem.knobs(**kv):
+                    sweep[f"{n}/{name}"] = stage_ms(scheme, inputs, es, ds)
+            del inputs
+        out[f"lanes_{stage}_ms"] = sweep
+    # persistent Saber tensor-core product (CTAs per SM, 0 = a CTA per instance), l=3 product stages
+    psweep = {}
+    for n in (1024, 4096, 16384):
+        inputs = keys(d.SABER, n)
+        for per_sm in (0, 1, 2, 4):
+            with kem.knobs(saber_tc_ctas_per_sm=per_sm):
+                psweep[f"{n}/{per_sm}"] = stage_ms(d.SABER, inputs, (1,), (0, 2))
+        del inputs
+    out["saber_tc_ctas_per_sm_ms"] = psweep
+    # sponge stages of small groups as warp tasks in the persistent mixed kernel
+    from dpcrypto_b200.workloads import MixedBatch
+
+    wsweep = {}
+    for n in (512, 4096):
+        mb = MixedBatch(eng, n, seed=11)
+        for wm in (0, 128, 512, 2048):
+            with kem.knobs(mixed_warp_max=wm):
+                eng.mixed(mb.items, d.FORM_TC)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                for _ in range(3):
+                    eng.mixed(mb.items, d.FORM_TC)
+                torch.cuda.synchronize()
+                wsweep[f"{n}/{wm}"] = (time.perf_counter() - t0) / 3 * 1e3
+            eng.sync()
+            ok = mb.check()
+            mb.clear()
+            if not ok:
+                raise RuntimeError("mixed batch mismatch while tuning warp tasks")
+        del mb
+    out["mixed_warp_max_ms"] = wsweep
+    return out
+
+
+def _winners(sweep: dict) -> dict:
+    """{n: fastest layout} of a {"n/layout": ms} sweep."""
+    best = {}
+    for k, v in sweep.items():
+        n, name = k.split("/")
+        if int(n) not in best or v < sweep[f"{n}/{best[int(n)]}"]:
+            best[int(n)] = name
+    return best
+
+
+def _max_where(win: dict, name: str, above: int = 0) -> int:
+    """Largest swept batch whose fastest layout is `name` (0 if none, or if it is not above
+    the threshold checked before it, which would shadow it)."""
+    m = max([n for n, w in win.items() if w == name], default=0)
+    return m if m > above else 0
+
+
+def lanes_choice(best: dict) -> dict:
+    """Per-stage thresholds from the lanes sweep: a layout covers batches up to the largest
+    swept size at which it was the fastest."""
+    ch = {}
+    w = _winners(best["lanes_saber_prologue_ms"])
+    ch["saber_warp_max"] = _max_where(w, "warp")
+    ch["saber_five_max"] = _max_where(w, "five", ch["saber_warp_max"])
+    w = _winners(best["lanes_saber_finish_ms"])
+    ch["saber_finish_warp_max"] = _max_where(w, "warp")
+    ch["saber_finish_five_max"] = _max_where(w, "five", ch["saber_finish_warp_max"])
+    # saber_pair_max gates the pair in both the prologue and the encaps finish: pair against one
+    # lane on the sum of the two stages
+    p, f = best["lanes_saber_prologue_ms"], best["lanes_saber_finish_ms"]
+    ns = sorted({int(k.split("/")[0]) for k in p})
+    ch["saber_pair_max"] = max([n for n in ns if p[f"{n}/pair"] + f[f"{n}/pair"] < p[f"{n}/one"] + f[f"{n}/one"]],
+                               default=0)
+    for stage, key in (("frodo_prologue", "frodo"), ("frodo_ss", "frodo_ss")):
+        w = _winners(best[f"lanes_{stage}_ms"])
+        ch[f"{key}_warp_max"] = _max_where(w, "warp")
+        ch[f"{key}_five_max"] = _max_where(w, "five", ch[f"{key}_warp_max"])
+    ps = best["saber_tc_ctas_per_sm_ms"]
+    per = sorted({int(k.split("/")[1]) for k in ps})
+    ns = sorted({int(k.split("/")[0]) for k in ps})
+    ch["saber_tc_ctas_per_sm"] = min(per, key=lambda c: sum(ps[f"{n}/{c}"] / min(ps[f"{n}/{x}"] for x in per) for n in ns))
+    ws = best["mixed_warp_max_ms"]
+    wm = sorted({int(k.split("/")[1]) for k in ws})
+    ns = sorted({int(k.split("/")[0]) for k in ws})
+    ch["mixed_warp_max"] = min(wm, key=lambda c: sum(ws[f"{n}/{c}"] / min(ws[f"{n}/{x}"] for x in wm) for n in ns))
+    return ch
 
 
 def measure() -> dict:
@@ -194,18 +323,16 @@ def measure() -> dict:
     mk = min(best["mixed_task_ms"], key=best["mixed_task_ms"].get)
     pc, prio = (int(x) for x in min(best["pipe_chunks_priority_ms"], key=best["pipe_chunks_priority_ms"].get).split("/"))
     ft, stt, tt = (int(x) for x in mk.split("/"))
-    ls = best["saber_lanes_ms"]
-    pair_max = max([int(k.split("/")[0]) for k in ls if k.endswith("/pair") and ls[k] < ls[k.replace("/pair", "/one")]],
-                   default=0)
+    lanes = lanes_choice(best)
     import torch
 
     out = {
         "device": torch.cuda.get_device_name(0),
         "chosen": {"keccak_unroll": best["keccak_unroll"], "thread_block": int(tb), "mixed_frodo_task": ft,
                    "mixed_pair_task": stt, "mixed_thread_task": tt, "pipe_chunks": pc,
-                   "pipe_priority": prio, "saber_pair_max": pair_max},
+                   "pipe_priority": prio, **lanes},
         "fixed": {"mma_tile": "M=128 (N=8 Frodo, N=8/16 Saber), K=32: int8 MMA <1% of the tensor pipe",
-                  "keccak_lanes_per_state_throughput_kernels": 1},
+                  "keccak_lanes_per_state_fused_sa_stages": 1},
         "measurements": results,
         "command": "python -m dpcrypto_b200.autotune --measure",
         "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),

@@ -47,11 +47,13 @@ __host__ __device__ constexpr int form_of(int code) { return code & 3; }
 // ciphertext pre-absorb), 1 = CTA (one instance per task).
 enum Kind : int { K_THREAD = 0, K_CTA = 1, K_THREAD2 = 2 };
 
-// Task code flag: a thread-level stage run on a warp per instance (and role): the Keccak
+// Task code flag (above the stage code's 10 bits, masked off before decoding): a
+// thread-level stage run on a warp per instance (and role): the Keccak
 // sponges spread over the warp's lanes (keccak25.cuh), 8 instances per task (4 for two-role
 // stages).  The planner uses it for groups small enough that one thread per instance would
 // leave the GPU idle (knob mixed_warp_max).
 constexpr int kWarpTask = 1 << 10;
+static_assert(code_of(4, 3, 7, 3) < kWarpTask, "stage codes must stay below the warp-task flag");
 
 __host__ __device__ constexpr int nstages(int scheme, int op) { return op == OP_DEC ? 4 : 3; }
 
@@ -371,7 +373,7 @@ __global__ void __launch_bounds__(256, 2) mixed_kernel(Plan p) {
     __syncthreads();
     if (t >= p.ntasks) break;
     const Task tk = p.tasks[t];
-    const int code = tk.code, scheme = scheme_of(code), op = op_of(code), stage = stage_of(code);
+    const int code = tk.code & (kWarpTask - 1), scheme = scheme_of(code), op = op_of(code), stage = stage_of(code);
     const int kind = kind_of(scheme, op, stage);
     const uint32_t need = threshold(scheme, op, stage);
     if (kind == K_CTA) {
@@ -381,7 +383,7 @@ __global__ void __launch_bounds__(256, 2) mixed_kernel(Plan p) {
       if (s_ready) cta_stage(code, p.req[r], smem, tbase, p.err);  // skipped after an error: the batch drains
       __syncthreads();
       if (tid == 0) mark_done(p, r);
-    } else if (code & kWarpTask) {
+    } else if (tk.code & kWarpTask) {
       const int warp = tid >> 5, lane = tid & 31;
       const int slot = kind == K_THREAD2 ? warp >> 1 : warp, role = kind == K_THREAD2 ? warp & 1 : 0;
       if (slot < tk.count) {  // warp-uniform: every lane of the warp runs the stage

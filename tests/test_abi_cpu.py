@@ -89,3 +89,37 @@ def test_tuning_knobs():
                     "frodo_warp_max": 1024, "frodo_ss_warp_max": 1024, "mixed_warp_max": 512}
         for k in kem.RUNTIME_KNOBS:
             lib.dpkem_set_tuning(k.encode(), saved.get(k, defaults[k]))
+
+
+def test_autotune_lanes_choice():
+    """Per-stage lanes-per-state thresholds from a synthetic sweep: each layout covers the
+    batches up to the largest size at which it was fastest; a five-lane range shadowed by the
+    warp range is dropped; the pair threshold compares pair and one lane on prologue + finish."""
+    from dpcrypto_b200 import autotune as at
+
+    def sweep(win: dict, layouts):
+        return {f"{n}/{l}": (1.0 if l == w else 2.0) for n, w in win.items() for l in layouts}
+
+    sab = ("warp", "five", "pair", "one")
+    fro = ("warp", "five", "one")
+    best = {
+        "lanes_saber_prologue_ms": sweep({64: "warp", 512: "warp", 1024: "five", 4096: "pair", 16384: "one"}, sab),
+        "lanes_saber_finish_ms": sweep({64: "warp", 512: "five", 1024: "warp", 4096: "pair", 16384: "one"}, sab),
+        "lanes_frodo_prologue_ms": sweep({64: "warp", 1024: "warp", 4096: "one"}, fro),
+        "lanes_frodo_ss_ms": sweep({64: "five", 1024: "one", 4096: "one"}, fro),
+        "saber_tc_ctas_per_sm_ms": {"1024/0": 1.0, "1024/1": 1.2, "4096/0": 2.0, "4096/1": 1.9},
+        "mixed_warp_max_ms": {"512/0": 3.0, "512/512": 2.0, "4096/0": 5.0, "4096/512": 5.1},
+    }
+    ch = at.lanes_choice(best)
+    assert ch["saber_warp_max"] == 512 and ch["saber_five_max"] == 1024
+    assert ch["saber_finish_warp_max"] == 1024 and ch["saber_finish_five_max"] == 0  # shadowed
+    # pair against one lane on prologue + finish: 1 + 1 < 2 + 2 at 4096; 2 + 2 > 1 + 1 at 16384;
+    # a tie where neither is fastest
+    assert ch["saber_pair_max"] == 4096
+    assert ch["frodo_warp_max"] == 1024 and ch["frodo_five_max"] == 0
+    assert ch["frodo_ss_warp_max"] == 0 and ch["frodo_ss_five_max"] == 64
+    assert ch["saber_tc_ctas_per_sm"] == 0
+    assert ch["mixed_warp_max"] == 512
+    from dpcrypto_b200 import kem
+
+    assert set(ch) <= set(kem.RUNTIME_KNOBS)
