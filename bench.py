@@ -639,6 +639,30 @@ def main():
                     serving[key] = {"peak_ops_per_s": peak, "levels": levels, "bit_exact": pool.check()}
                 finally:
                     srv.close()
+        # admission inside the running kernel: one long-lived service launch, each request
+        # submitted as it arrives (no host batching window), 32 CTAs for Saber work only
+        from dpcrypto_b200.serving import ServiceServer
+
+        serving["service"] = {"note": "dpkem_service_*: requests admitted by the running persistent kernel into "
+                                      "per-stage ready queues; 32 of its CTAs take only Saber work"}
+        for name, f in (("tc", d.FORM_TC), ("dp4a", d.FORM_DP4A)):
+            srv = ServiceServer(form=f, saber_ctas=32)
+            try:
+                srv.run(pool, np.zeros(2048))  # warm-up
+                peak = max(srv.run(pool, np.zeros(pool.n))["ops_per_s"] for _ in range(2))
+                levels = []
+                for frac in (0.1, 0.25, 0.5, 0.75, 1.0):
+                    if frac == 1.0:
+                        pool.clear()  # the last level's outputs are checked against the batched calls
+                    r = srv.run(pool, poisson_arrivals(pool.n, rate=frac * peak, seed=int(frac * 100) + 7))
+                    levels.append({"load": frac, "offered_per_s": frac * peak, "ops_per_s": r["ops_per_s"],
+                                   "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "frodo_p50_ms": r["frodo_p50_ms"],
+                                   "frodo_p99_ms": r["frodo_p99_ms"], "saber_p50_ms": r["saber_p50_ms"],
+                                   "saber_p99_ms": r["saber_p99_ms"], "mean_submit": r["mean_submit"]})
+                torch.cuda.synchronize()
+                serving["service"][name] = {"peak_ops_per_s": peak, "levels": levels, "bit_exact": pool.check()}
+            finally:
+                srv.close()
         line["serving"] = serving
 
     # ---- wire format: 16384 mixed request frames from pinned host memory, then the same

@@ -5,6 +5,6 @@ include/dpkem.h); this package only binds it (kem.py) and builds it (build.py).
 """
 from .kem import (  # noqa: F401
     EXPORTS, FIRESABER, FLAG_DEVICE_PTRS, FORM_DP4A, FORM_INT32, FORM_TC, FRODO976, FRODO976AES, LIGHTSABER, SABER, SCHEMES,
-    DpkemError, Engine, MixedGraph, Request, frodoKEMDecap, frodoKEMEncap, frodoKEMKeypair, load, saber_dec, saber_enc, set_compat,
+    DpkemError, Engine, MixedGraph, Request, Service, ServiceConfig, frodoKEMDecap, frodoKEMEncap, frodoKEMKeypair, load, saber_dec, saber_enc, set_compat,
     sizes,
 )

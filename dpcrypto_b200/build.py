@@ -18,10 +18,10 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdpkem.so")
 SOURCES = ["frodo.cu", "saber.cu", "coins.cu", "peak.cu", "keccak_lanes.cu", "abi.cu", "noalloc.cu", "mixed.cu",
-           "frames.cu"]
-# The persistent mixed-batch kernel reads data other CTAs wrote in the same launch: its
-# global loads bypass the (non-coherent) L1.
-EXTRA = {"mixed.cu": ["-Xptxas", "-dlcm=cg"]}
+           "frames.cu", "serve.cu"]
+# The persistent mixed-batch and service kernels read data other CTAs (and the host's
+# copies) wrote during the launch: their global loads bypass the (non-coherent) L1.
+EXTRA = {"mixed.cu": ["-Xptxas", "-dlcm=cg"], "serve.cu": ["-Xptxas", "-dlcm=cg"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "-Xptxas", "-warn-spills"]

@@ -416,6 +416,28 @@ int run_shared(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8
 
 }  // namespace
 
+namespace dpkem {
+namespace abi {
+
+// device_coins: keypair / encaps requests may leave in0 (coins) null.
+int check_requests(size_t n, const dpkem_request *reqs, bool device_coins) {
+  if (!reqs || n == 0 || n > (size_t)INT32_MAX) return DPKEM_EINVAL;
+  alignas(16) static const uint8_t kAligned[16] = {};
+  for (size_t i = 0; i < n; i++) {
+    const dpkem_request &r = reqs[i];
+    Sizes z;
+    if (!scheme_sizes(r.scheme, &z) || r.op < 0 || r.op > 2) return DPKEM_EINVAL;
+    const bool two_out = r.op != OP_DEC;
+    const bool coins_ok = r.in0 || (device_coins && r.op != OP_DEC);
+    if (!coins_ok || !r.out0 || (r.op != OP_KEYPAIR && !r.in1) || (two_out && !r.out1)) return DPKEM_EINVAL;
+    if (!op_aligned(r.op, r.in0 ? r.in0 : kAligned, r.in1, r.out0, r.out1)) return DPKEM_EINVAL;
+  }
+  return DPKEM_OK;
+}
+
+}  // namespace abi
+}  // namespace dpkem
+
 extern "C" {
 
 int dpkem_ctx_create(dpkem_ctx **out, int device, size_t hbm_budget_bytes) {
@@ -560,21 +582,6 @@ int dpkem_dec_batch(dpkem_ctx *c, int scheme, int form, size_t n, const uint8_t 
 
 static_assert(sizeof(dpkem_request) == sizeof(mixed::Req), "request layout");
 
-// device_coins: keypair / encaps requests may leave in0 (coins) null.
-static int check_requests(size_t n, const dpkem_request *reqs, bool device_coins = false) {
-  if (!reqs || n == 0 || n > (size_t)INT32_MAX) return DPKEM_EINVAL;
-  alignas(16) static const uint8_t kAligned[16] = {};
-  for (size_t i = 0; i < n; i++) {
-    const dpkem_request &r = reqs[i];
-    Sizes z;
-    if (!scheme_sizes(r.scheme, &z) || r.op < 0 || r.op > 2) return DPKEM_EINVAL;
-    const bool two_out = r.op != OP_DEC;
-    const bool coins_ok = r.in0 || (device_coins && r.op != OP_DEC);
-    if (!coins_ok || !r.out0 || (r.op != OP_KEYPAIR && !r.in1) || (two_out && !r.out1)) return DPKEM_EINVAL;
-    if (!op_aligned(r.op, r.in0 ? r.in0 : kAligned, r.in1, r.out0, r.out1)) return DPKEM_EINVAL;
-  }
-  return DPKEM_OK;
-}
 
 static int mixed_batch(dpkem_ctx *c, int form, size_t n, const dpkem_request *reqs, const uint8_t *key,
                        uint64_t first, void *stream);

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <mutex>
 
+#include "../../include/dpkem.h"
 #include "common.cuh"
 
 struct dpkem_ctx {
@@ -53,6 +54,9 @@ cudaError_t persistent_grid(const dpkem_ctx *c, int *grid);
 // upload just enqueued on st.
 uint8_t *stage_for(dpkem_ctx *c, int j, size_t bytes);
 void stage_used(dpkem_ctx *c, int j, cudaStream_t st);
+// DPKEM_OK when every request names a known scheme and operation with the buffers it needs,
+// aligned as the mixed entry points require (device_coins: keypair / encaps may omit coins).
+int check_requests(size_t n, const dpkem_request *reqs, bool device_coins = false);
 
 }  // namespace abi
 }  // namespace dpkem

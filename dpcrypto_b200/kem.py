@@ -35,6 +35,13 @@ class Request(ctypes.Structure):
                 ("in1", ctypes.c_void_p), ("out0", ctypes.c_void_p), ("out1", ctypes.c_void_p)]
 
 
+class ServiceConfig(ctypes.Structure):
+    """dpkem_service_config (include/dpkem.h)."""
+
+    _fields_ = [("max_inflight", ctypes.c_uint32), ("idle_ms", ctypes.c_uint32), ("saber_ctas", ctypes.c_uint32),
+                ("warp_max", ctypes.c_uint32), ("scratch_bytes", ctypes.c_uint64), ("coin_key", ctypes.c_void_p)]
+
+
 EXPORTS = {
     "dpkem_ctx_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_size_t]),
     "dpkem_ctx_destroy": (ctypes.c_int, [ctypes.c_void_p]),
@@ -96,6 +103,18 @@ EXPORTS = {
     "frodoKEMDecap": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "saber_enc": (None, [ctypes.c_uint8, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "saber_dec": (None, [ctypes.c_uint8, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    # KEM service: one long-lived launch that admits requests while it runs
+    "dpkem_service_default_config": (ctypes.c_int, [ctypes.c_void_p]),
+    "dpkem_service_open": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.POINTER(ctypes.c_void_p)]),
+    "dpkem_service_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                            ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_uint64)]),
+    "dpkem_service_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                          ctypes.POINTER(ctypes.c_size_t)]),
+    "dpkem_service_drain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
+    "dpkem_service_stats": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_uint64)] * 3
+                            + [ctypes.POINTER(ctypes.c_int)]),
+    "dpkem_service_close": (ctypes.c_int, [ctypes.c_void_p]),
     # wire format and shared-memory ring (include/dpkem_wire.h)
     "dpkem_frame_bytes": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t),
                                          ctypes.POINTER(ctypes.c_size_t)]),
@@ -475,6 +494,95 @@ class MixedGraph:
         if getattr(self, "_h", None):
             self._lib.dpkem_mixed_graph_destroy(self._h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Service:
+    """A KEM service on an engine's device: one long-lived persistent launch that admits
+    requests while it runs (dpkem_service_*).  submit() takes a prefix of the requests (device
+    buffers, the mixed batches' layout) and returns (accepted, first_ticket); poll() returns
+    the tickets completed since the previous poll as a numpy array."""
+
+    def __init__(self, engine: Engine, form: int = FORM_TC, max_inflight: int | None = None,
+                 idle_ms: int | None = None, saber_ctas: int | None = None, warp_max: int | None = None,
+                 scratch_bytes: int | None = None, coin_key: bytes | None = None):
+        self._lib = engine._lib
+        self._engine = engine
+        cfg = ServiceConfig()
+        rc = self._lib.dpkem_service_default_config(ctypes.byref(cfg))
+        if rc != OK:
+            raise DpkemError(rc, "service_default_config")
+        for k, v in (("max_inflight", max_inflight), ("idle_ms", idle_ms), ("saber_ctas", saber_ctas),
+                     ("warp_max", warp_max), ("scratch_bytes", scratch_bytes)):
+            if v is not None:
+                setattr(cfg, k, int(v))
+        self._key = None
+        if coin_key is not None:
+            if len(coin_key) != 32:
+                raise ValueError("coin_key must be 32 bytes")
+            self._key = ctypes.create_string_buffer(bytes(coin_key), 32)
+            cfg.coin_key = ctypes.cast(self._key, ctypes.c_void_p)
+        h = ctypes.c_void_p()
+        rc = self._lib.dpkem_service_open(engine._h, form, ctypes.byref(cfg), ctypes.byref(h))
+        if rc != OK:
+            raise DpkemError(rc, "service_open")
+        self._h = h
+        self._buf = np.zeros(1 << 16, np.uint64)
+
+    def submit(self, items) -> tuple:
+        """items: (scheme, op, in0, in1, out0, out1) tuples, an Engine.requests table, or a numpy
+        array with dpkem_request's layout.  Returns (accepted, first_ticket); EAGAIN counts as
+        nothing accepted."""
+        if isinstance(items, np.ndarray):
+            n, ptr = len(items), items.ctypes.data
+        else:
+            arr = items if isinstance(items, ctypes.Array) else Engine.requests(items)
+            n, ptr = len(arr), ctypes.cast(arr, ctypes.c_void_p).value
+        acc, first = ctypes.c_size_t(), ctypes.c_uint64()
+        rc = self._lib.dpkem_service_submit(self._h, n, ctypes.c_void_p(ptr), ctypes.byref(acc), ctypes.byref(first))
+        if rc not in (OK, EAGAIN):
+            raise DpkemError(rc, "service_submit")
+        return acc.value, first.value
+
+    def poll(self) -> np.ndarray:
+        """Tickets completed since the previous poll."""
+        got = ctypes.c_size_t()
+        rc = self._lib.dpkem_service_poll(self._h, ctypes.c_void_p(self._buf.ctypes.data), len(self._buf),
+                                          ctypes.byref(got))
+        if rc != OK:
+            raise DpkemError(rc, "service_poll")
+        return self._buf[:got.value].copy()
+
+    def drain(self, timeout_ms: int = 30000):
+        rc = self._lib.dpkem_service_drain(self._h, timeout_ms)
+        if rc != OK:
+            raise DpkemError(rc, "service_drain")
+
+    def stats(self) -> dict:
+        a, b, c, r = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int()
+        rc = self._lib.dpkem_service_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                           ctypes.byref(r))
+        if rc != OK:
+            raise DpkemError(rc, "service_stats")
+        return {"submitted": a.value, "completed": b.value, "launches": c.value, "running": bool(r.value)}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            rc = self._lib.dpkem_service_close(self._h)
+            self._h = None
+            if rc != OK:
+                raise DpkemError(rc, "service_close")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
     def __del__(self):
         try:

@@ -205,6 +205,61 @@ class Server:
         return out
 
 
+class ServiceServer:
+    """Serving through one KEM service (dpkem_service_*): each request is submitted to the
+    running kernel as soon as it arrives (admission inside the launch, no batching window on
+    the host), and its completion is the host time at which a poll first returns its
+    ticket.  saber_ctas CTAs take only Saber work, so a Saber request never waits behind
+    the multi-millisecond FrodoKEM stages."""
+
+    def __init__(self, device: int = 0, form: int = K.FORM_TC, saber_ctas: int = 32, warp_max: int | None = None,
+                 max_inflight: int = 16384, idle_ms: int = 200):
+        self.eng = K.Engine(device)
+        self.svc = K.Service(self.eng, form, max_inflight=max_inflight, idle_ms=idle_ms, saber_ctas=saber_ctas,
+                             warp_max=warp_max)
+
+    def close(self):
+        self.svc.close()
+        self.eng.close()
+
+    def run(self, pool: RequestPool, arrivals: np.ndarray) -> dict:
+        """Serve pool requests 0..len(arrivals)-1 arriving at the given times (seconds)."""
+        n = len(arrivals)
+        base = self.svc.stats()["submitted"]  # tickets of this run: base + request index
+        done_s = np.full(n, np.nan)
+        nxt, completed, polls, submits = 0, 0, 0, 0
+        host0 = time.perf_counter()
+        while completed < n:
+            now = time.perf_counter() - host0
+            arrived = int(np.searchsorted(arrivals, now, side="right"))
+            if arrived > nxt:
+                acc, first = self.svc.submit(pool.table[nxt:arrived])
+                if acc:
+                    assert first == base + nxt
+                    nxt += acc
+                    submits += 1
+            got = self.svc.poll()
+            polls += 1
+            if len(got):
+                done_s[got.astype(np.int64) - base] = time.perf_counter() - host0
+                completed += len(got)
+            elif nxt == arrived and nxt < n:
+                wait = arrivals[nxt] - (time.perf_counter() - host0)
+                if wait > 50e-6:
+                    time.sleep(min(wait, 200e-6) - 20e-6)
+        lat = (done_s - arrivals) * 1e3
+        span = np.nanmax(done_s) - arrivals[0]
+        out = {"requests": n, "ops_per_s": n / span, "p50_ms": float(np.nanpercentile(lat, 50)),
+               "p99_ms": float(np.nanpercentile(lat, 99)), "latency_ms": lat, "submits": submits,
+               "mean_submit": n / max(1, submits), "polls": polls}
+        saber = pool.kind[:n] // 3 >= 2
+        for m, name in ((~saber, "frodo"), (saber, "saber")):
+            if m.any():
+                out[name + "_p50_ms"] = float(np.nanpercentile(lat[m], 50))
+                out[name + "_p99_ms"] = float(np.nanpercentile(lat[m], 99))
+        return out
+
+
 def poisson_arrivals(n: int, rate: float, seed: int = 0) -> np.ndarray:
     rng = np.random.default_rng(seed)
     return np.cumsum(rng.exponential(1.0 / rate, size=n))

@@ -131,6 +131,54 @@ int dpkem_mixed_graph_create(dpkem_ctx *ctx, int form, size_t n, const dpkem_req
 int dpkem_mixed_graph_launch(dpkem_graph *g, void *stream);
 int dpkem_mixed_graph_destroy(dpkem_graph *g);
 
+/* ---- KEM service: one long-lived launch that admits requests while it runs ----
+ * Requests (dpkem_request, device buffers, the mixed batches' layout and alignment) are
+ * appended to a ring the running kernel reads: the kernel's CTAs admit them into
+ * per-(scheme, operation, stage) ready queues in device memory and pull stage work from
+ * those queues (thread-level stages gather whatever instances are ready, across
+ * submissions), so a request never waits for an earlier launch to drain.  Each accepted
+ * request gets a ticket (consecutive from 0); the last stage writes it into host-mapped
+ * memory and dpkem_service_poll() returns the tickets that have completed.  Results equal
+ * the batched calls on the same inputs.  Input buffers must hold their data when submitted
+ * and stay untouched, and outputs unread, until the request's ticket is returned.
+ * Admission is live: a request is accepted while a ring slot is free and the scratch
+ * records of the requests in flight leave room for its own (FrodoKEM 31,744 bytes, Saber
+ * 2,816 / 4,864 / 7,936 bytes for l = 2 / 3 / 4); the rest of a submission is left to the caller
+ * to resubmit.
+ * The kernel ends after idle_ms without work and is relaunched by the next submit, poll or
+ * drain.  Every device wait is bounded; an expired one makes poll / drain / close return
+ * DPKEM_ETIMEOUT.  While a service is open its launch holds the CTA slots it was given
+ * (dpkem_ctx_set_max_ctas caps them): other kernels on the device share what is left.
+ * No counterpart in the reference (FrodoKEM976-GPU/main.cu:13-34, SABER-GPU/main.cu:12-38
+ * run one fixed batch per program). */
+typedef struct dpkem_service dpkem_service;
+typedef struct {
+  uint32_t max_inflight;   /* ring slots: requests submitted and not yet completed (rounded up to a power of 2) */
+  uint32_t idle_ms;        /* the launch ends after this long without work (relaunched on demand) */
+  uint32_t saber_ctas;     /* CTAs that take only Saber work (0 = none): Saber latency never waits on FrodoKEM */
+  uint32_t warp_max;       /* a thread-level stage with at most this many ready instances runs a warp per instance */
+  uint64_t scratch_bytes;  /* device scratch for the records of requests in flight (0 = max_inflight FrodoKEM records) */
+  const uint8_t *coin_key; /* NULL, or 32 bytes: keypair / encaps requests with in0 NULL draw their coins on the device,
+                              SHAKE256(key || LE64(ticket) || "kp" / "enc") truncated to the scheme's coin length */
+} dpkem_service_config;
+/* Defaults: 16384 slots, idle 1000 ms, no Saber-only CTAs, warp_max 32, default scratch, no key. */
+int dpkem_service_default_config(dpkem_service_config *cfg);
+/* cfg NULL = the defaults.  Device memory (ring, queues, scratch) counts against the context's budget. */
+int dpkem_service_open(dpkem_ctx *ctx, int form, const dpkem_service_config *cfg, dpkem_service **out);
+/* Accepts a prefix of reqs: *accepted requests with tickets *first_ticket, *first_ticket + 1, ...
+ * DPKEM_EAGAIN when none fits yet (poll, then resubmit). */
+int dpkem_service_submit(dpkem_service *svc, size_t n, const dpkem_request *reqs, size_t *accepted,
+                         uint64_t *first_ticket);
+/* Up to max tickets completed since the previous poll, in the order they were seen. */
+int dpkem_service_poll(dpkem_service *svc, uint64_t *tickets, size_t max, size_t *n_done);
+/* Waits until every accepted request has completed (DPKEM_ETIMEOUT after timeout_ms). */
+int dpkem_service_drain(dpkem_service *svc, uint32_t timeout_ms);
+/* Counters: tickets issued, tickets completed in order, launches so far, launch running now. */
+int dpkem_service_stats(dpkem_service *svc, uint64_t *submitted, uint64_t *completed, uint64_t *launches,
+                        int *running);
+/* Drains (30 s at most), ends the launch and frees the service. */
+int dpkem_service_close(dpkem_service *svc);
+
 /* Seeded synthetic coins: out[i] = SHAKE256(00 01 .. 1F || LE64(first + i) || tag, len), len <= 136,
  * strlen(tag) <= 16.  Same flag semantics as the batched operations. */
 int dpkem_coins(dpkem_ctx *ctx, size_t n, size_t len, uint64_t first, const char *tag, uint8_t *out,

@@ -123,3 +123,26 @@ def test_autotune_lanes_choice():
     from dpcrypto_b200 import kem
 
     assert set(ch) <= set(kem.RUNTIME_KNOBS)
+
+
+def test_service_host_checks():
+    """Service entry points: documented defaults, and argument errors reported before any
+    device work (no GPU needed)."""
+    import ctypes as C
+
+    from dpcrypto_b200 import kem
+
+    lib = kem.load()
+    cfg = kem.ServiceConfig()
+    assert lib.dpkem_service_default_config(C.byref(cfg)) == kem.OK
+    assert (cfg.max_inflight, cfg.idle_ms, cfg.saber_ctas, cfg.warp_max, cfg.scratch_bytes) == (16384, 1000, 0, 32, 0)
+    assert not cfg.coin_key
+    assert lib.dpkem_service_default_config(None) == kem.EINVAL
+    out = C.c_void_p()
+    assert lib.dpkem_service_open(None, kem.FORM_TC, None, C.byref(out)) == kem.EINVAL
+    acc, first = C.c_size_t(7), C.c_uint64()
+    assert lib.dpkem_service_submit(None, 1, None, C.byref(acc), C.byref(first)) == kem.EINVAL
+    assert acc.value == 0
+    assert lib.dpkem_service_poll(None, None, 0, None) == kem.EINVAL
+    assert lib.dpkem_service_drain(None, 10) == kem.EINVAL
+    assert lib.dpkem_service_close(None) == kem.EINVAL

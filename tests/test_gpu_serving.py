@@ -41,3 +41,25 @@ def test_serving_split_classes(engine, oracle_check_items):
     assert oracle_check_items(pool.items(), stride=13, offset=5) >= 40
     assert np.isfinite(res["latency_ms"]).all()
     assert res["saber_p50_ms"] < res["frodo_p50_ms"]
+
+
+@pytest.mark.parametrize("form", [d.FORM_TC, d.FORM_DP4A])
+def test_service_server_results_equal_alone(engine, form, oracle_check_items):
+    """Admission inside the running kernel (dpkem_service_*): requests submitted one arrival
+    at a time, results equal the batched calls' and a stride sample the oracle's."""
+    from dpcrypto_b200.serving import ServiceServer
+
+    pool = RequestPool(engine, 700, seed=5)
+    srv = ServiceServer(form=form, saber_ctas=16)
+    try:
+        res = srv.run(pool, poisson_arrivals(pool.n, rate=20000.0, seed=3))
+        pool.clear()
+        res2 = srv.run(pool, np.zeros(pool.n))  # everything at once, on the same running service
+    finally:
+        srv.close()
+    torch.cuda.synchronize()
+    assert pool.check()
+    assert oracle_check_items(pool.items(), stride=11, offset=3) >= 60
+    for r in (res, res2):
+        assert np.isfinite(r["latency_ms"]).all() and (r["latency_ms"] > 0).all()
+    assert res["submits"] > 10
