@@ -640,13 +640,13 @@ def main():
                 finally:
                     srv.close()
         # admission inside the running kernel: one long-lived service launch, each request
-        # submitted as it arrives (no host batching window), 32 CTAs for Saber work only
+        # submitted as it arrives (no host batching window), 16 CTAs for Saber work only
         from dpcrypto_b200.serving import ServiceServer
 
         serving["service"] = {"note": "dpkem_service_*: requests admitted by the running persistent kernel into "
-                                      "per-stage ready queues; 32 of its CTAs take only Saber work"}
+                                      "per-stage ready queues; 16 of its CTAs take only Saber work"}
         for name, f in (("tc", d.FORM_TC), ("dp4a", d.FORM_DP4A)):
-            srv = ServiceServer(form=f, saber_ctas=32)
+            srv = ServiceServer(form=f, saber_ctas=16)
             try:
                 srv.run(pool, np.zeros(2048))  # warm-up
                 peak = max(srv.run(pool, np.zeros(pool.n))["ops_per_s"] for _ in range(2))

@@ -56,16 +56,18 @@ constexpr uint64_t kDepLimitNs = 2000000000ull;
 // true when request r has completed `need` stage roles; false on expiry (the error word is
 // set) or when an error is already recorded, in which case the caller skips its stage.
 __device__ __forceinline__ bool wait_done(const Plan &p, uint32_t r, uint32_t need) {
-  if (ld_acquire(p.done + r) >= need) return true;
-  const uint64_t t0 = globaltimer_ns();
-  while (ld_acquire(p.done + r) < need) {
-    if (ld_acquire(p.err) != 0) return false;
-    __nanosleep(200);
-    if (globaltimer_ns() - t0 > kDepLimitNs) {
-      atomicOr(p.err, DEV_ERR_TIMEOUT);
-      return false;
+  if (ld_relaxed(p.done + r) < need) {
+    const uint64_t t0 = globaltimer_ns();
+    while (ld_relaxed(p.done + r) < need) {
+      if (ld_relaxed(p.err) != 0) return false;
+      __nanosleep(200);
+      if (globaltimer_ns() - t0 > kDepLimitNs) {
+        atomicOr(p.err, DEV_ERR_TIMEOUT);
+        return false;
+      }
     }
   }
+  __threadfence();  // acquire side of mark_done's release
   return true;
 }
 

@@ -126,6 +126,16 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
   return v;
 }
 
+// Spin loads: a relaxed load reads L2 (these kernels bypass L1) without the L1 invalidation
+// an acquire load performs on every iteration, which would evict the register spills of the
+// CTA sharing the SM; a spin that succeeds then fences once (__threadfence), which orders
+// the loads after it behind the value it saw.
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 
 template <int L>
 __device__ __forceinline__ void saber_thread(const CoinKey &key, int op, int stage, const DevReq &r, int role) {

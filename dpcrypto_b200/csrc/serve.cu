@@ -70,8 +70,14 @@ struct Ctl {
   Word head[kQueues], tail[kQueues];
 };
 
+// Counters (device memory, zeroed at open): per queue claims, instances, claims run a warp
+// per instance, and thread 0's busy time from claim to hand-off (ns); then the CTAs' idle
+// time (ns), admissions, requests admitted and claims lost to another CTA.
+constexpr int kStats = kQueues * 4 + 4;
+
 struct Svc {
   Ctl *ctl;
+  unsigned long long *stats;  // [kStats]
   const DevReq *req;          // [slots], slot = ticket & qmask
   uint32_t *done;             // [slots] roles finished in the current two-role stage
   unsigned long long *ent;    // [kQueues][slots]
@@ -90,18 +96,13 @@ struct Svc {
 
 constexpr uint64_t kEntryWaitNs = 1000000000ull;
 
-__device__ __forceinline__ unsigned long long ld_acq64(const unsigned long long *p) {
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p) {
   unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
 __device__ __forceinline__ void st_rel64(unsigned long long *p, unsigned long long v) {
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t *p) {
-  uint32_t v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
 }
 
 __device__ __forceinline__ void fail(const Svc &p) {
@@ -113,39 +114,38 @@ __device__ __forceinline__ void fail(const Svc &p) {
 // Waits (bounded) until entry e carries sequence `seq`; its value in *v.
 __device__ __forceinline__ bool wait_seq(const Svc &p, const unsigned long long *e, uint32_t seq,
                                          unsigned long long *v) {
-  unsigned long long x = ld_acq64(e);
-  if ((uint32_t)(x >> 32) == seq) {
-    *v = x;
-    return true;
+  unsigned long long x = ld_relaxed64(e);
+  if ((uint32_t)(x >> 32) != seq) {
+    const uint64_t t0 = globaltimer_ns();
+    do {
+      __nanosleep(64);
+      x = ld_relaxed64(e);
+      if ((uint32_t)(x >> 32) != seq && globaltimer_ns() - t0 > kEntryWaitNs) {
+        fail(p);
+        return false;
+      }
+    } while ((uint32_t)(x >> 32) != seq);
   }
-  const uint64_t t0 = globaltimer_ns();
-  while (true) {
-    __nanosleep(64);
-    x = ld_acq64(e);
-    if ((uint32_t)(x >> 32) == seq) {
-      *v = x;
-      return true;
-    }
-    if (globaltimer_ns() - t0 > kEntryWaitNs) {
-      fail(p);
-      return false;
-    }
-  }
+  __threadfence();  // acquire side of the entry's release store
+  *v = x;
+  return true;
 }
 
 __device__ __forceinline__ unsigned long long *entry(const Svc &p, int q, uint32_t j) {
   return p.ent + (size_t)q * (p.qmask + 1) + (j & p.qmask);
 }
 
-// Appends request slot r to queue q (after this thread's stage writes).
+// Appends request slot r to queue q (after this thread's stage writes).  Idle CTAs learn of
+// it from the push counter, which the caller bumps once per batch of pushes (wake()).
 __device__ __forceinline__ void push(const Svc &p, int q, uint32_t r) {
   __threadfence();
   const uint32_t j = atomicAdd(&p.ctl->tail[q].v, 1u);
   unsigned long long *e = entry(p, q, j);
   unsigned long long x;
   if (wait_seq(p, e, j, &x)) st_rel64(e, ((unsigned long long)(j + 1) << 32) | r);
-  atomicAdd(&p.ctl->version.v, 1u);
 }
+
+__device__ __forceinline__ void wake(const Svc &p) { atomicAdd(&p.ctl->version.v, 1u); }
 
 // The request slot in claimed entry j of queue q (~0u if the entry never filled); the entry
 // is handed to its next lap.
@@ -177,12 +177,20 @@ __device__ __forceinline__ void role_done(const Svc &p, int scheme, int op, int 
   }
 }
 
+// CTA-level stages of a few microseconds (the Saber products, FrodoKEM decaps' W): a claim
+// may take several instances, run one after another, so that claiming does not cost as
+// much as the work.
+__host__ __device__ constexpr bool short_cta(int q) {
+  return q_scheme(q) >= 2 || (q_op(q) == OP_DEC && q_stage(q) == 0);
+}
+constexpr uint32_t kCtaBatch = 8;
+
 // Instances one claim takes from queue q with `backlog` ready, and whether they run a warp
 // per instance (small backlogs: the chain finishes sooner and the CTA is free again sooner).
 __device__ __forceinline__ uint32_t cap_of(const Svc &p, int q, uint32_t backlog, bool *warp) {
   const int kind = kind_of(q_scheme(q), q_op(q), q_stage(q));
   *warp = false;
-  if (kind == K_CTA) return 1;
+  if (kind == K_CTA) return short_cta(q) ? min(kCtaBatch, 1u + backlog / 32u) : 1u;
   *warp = backlog <= p.warp_max;
   if (kind == K_THREAD2) return *warp ? 4 : 128;
   return *warp ? 8 : 256;
@@ -199,9 +207,9 @@ __device__ int pick(const Svc &p, bool short_only, uint32_t *h, uint32_t *k, boo
   Ctl *c = p.ctl;
   uint32_t sub = 0, adm = 0, v = 0, quit = 0;
   if (lane == 0) {
-    v = ld_acquire(&c->version.v);
-    sub = ld_acquire(&c->sub_tail.v);
-    adm = ld_acquire(&c->admitted.v);
+    v = ld_relaxed(&c->version.v);
+    sub = ld_relaxed(&c->sub_tail.v);
+    adm = ld_relaxed(&c->admitted.v);
     quit = ld_relaxed(&c->quit.v);
   }
   *ver = __shfl_sync(0xffffffffu, v, 0);
@@ -215,37 +223,50 @@ __device__ int pick(const Svc &p, bool short_only, uint32_t *h, uint32_t *k, boo
     int got = 0;
     if (lane == 0) got = atomicCAS(&c->admitted.v, adm, sub) == adm;
     if (!__shfl_sync(0xffffffffu, got, 0)) return kRetry;
+    __threadfence();  // the records were copied before the count that published them
     *h = adm;
     *k = sub - adm;
     return kAdmit;
   }
   const uint8_t *order = short_only ? p.prio_short : p.prio;
   const int n = short_only ? (int)p.nshort : (int)p.nprio;
-  for (int base = 0; base < n; base += 32) {
-    const int j = base + lane;
-    uint32_t hh = 0, tt = 0;
-    int q = 0;
-    if (j < n) {
-      q = order[j];
-      hh = ld_relaxed(&c->head[q].v);
-      tt = ld_acquire(&c->tail[q].v);
+  // Two passes in priority order: first CTA-level work and thread-level queues whose backlog
+  // fills a thread-per-instance claim (more than warp_max), then any non-empty queue.  A
+  // device with work elsewhere lets a sponge stage's backlog build up into one claim of up
+  // to 256 instances instead of spending a CTA slot on every few instances the stages before
+  // it trickle in (a warp per instance holds a slot for 8 of them at about three times the
+  // issue slots per permutation); an otherwise idle CTA takes what there is at once.
+  for (int pass = 0; pass < 2; pass++) {
+    for (int base = 0; base < n; base += 32) {
+      const int j = base + lane;
+      uint32_t hh = 0, tt = 0;
+      int q = 0;
+      bool ok = false;
+      if (j < n) {
+        q = order[j];
+        hh = ld_relaxed(&c->head[q].v);
+        tt = ld_relaxed(&c->tail[q].v);
+        const int backlog = (int)(tt - hh);
+        const int kind = kind_of(q_scheme(q), q_op(q), q_stage(q));
+        ok = backlog > 0 && (pass == 1 || kind == K_CTA || (uint32_t)backlog > p.warp_max);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (!m) continue;
+      const int src = __ffs(m) - 1;
+      q = __shfl_sync(0xffffffffu, q, src);
+      hh = __shfl_sync(0xffffffffu, hh, src);
+      tt = __shfl_sync(0xffffffffu, tt, src);
+      bool w;
+      const uint32_t cap = cap_of(p, q, tt - hh, &w);
+      const uint32_t n_take = min(tt - hh, cap);
+      int got = 0;
+      if (lane == 0) got = atomicCAS(&c->head[q].v, hh, hh + n_take) == hh;
+      if (!__shfl_sync(0xffffffffu, got, 0)) return kRetry;
+      *h = hh;
+      *k = n_take;
+      *warp = w;
+      return q;
     }
-    const unsigned m = __ballot_sync(0xffffffffu, j < n && (int)(tt - hh) > 0);
-    if (!m) continue;
-    const int src = __ffs(m) - 1;
-    q = __shfl_sync(0xffffffffu, q, src);
-    hh = __shfl_sync(0xffffffffu, hh, src);
-    tt = __shfl_sync(0xffffffffu, tt, src);
-    bool w;
-    const uint32_t cap = cap_of(p, q, tt - hh, &w);
-    const uint32_t n_take = min(tt - hh, cap);
-    int got = 0;
-    if (lane == 0) got = atomicCAS(&c->head[q].v, hh, hh + n_take) == hh;
-    if (!__shfl_sync(0xffffffffu, got, 0)) return kRetry;
-    *h = hh;
-    *k = n_take;
-    *warp = w;
-    return q;
   }
   return kNone;
 }
@@ -258,13 +279,13 @@ __device__ int pick(const Svc &p, bool short_only, uint32_t *h, uint32_t *k, boo
 __device__ bool idle(const Svc &p, bool short_only, uint64_t &idle_since, uint32_t version0, uint32_t sub0) {
   const uint64_t now = globaltimer_ns();
   if (idle_since == 0) idle_since = now;
-  if (ld_acquire(&p.ctl->stop.v) != 0u || ld_acquire(&p.ctl->quit.v) != 0u) return true;
+  if (ld_relaxed(&p.ctl->stop.v) != 0u || ld_relaxed(&p.ctl->quit.v) != 0u) return true;
   if (!short_only && now - idle_since > p.idle_ns) {
     atomicExch(&p.ctl->quit.v, 1u);
     return true;
   }
   for (int i = 0; i < 64; i++) {
-    if (ld_acquire(&p.ctl->version.v) != version0 || ld_acquire(&p.ctl->sub_tail.v) != sub0) break;
+    if (ld_relaxed(&p.ctl->version.v) != version0 || ld_relaxed(&p.ctl->sub_tail.v) != sub0) break;
     __nanosleep(600);
   }
   return false;
@@ -289,9 +310,13 @@ __global__ void __launch_bounds__(256, 2) service_kernel(Svc p) {
     if (warp == 0) {
       uint32_t h = 0, k = 0, ver = 0, sub = 0;
       bool w = false;
-      int q = kRetry;
-      for (int tries = 0; tries < 64 && q == kRetry; tries++) q = pick(p, short_only, &h, &k, &w, &ver, &sub);
+      int q = kRetry, tries = 0;
+      for (; tries < 64 && q == kRetry; tries++) {
+        if (tries) __nanosleep(32u << min(tries, 6));  // another CTA took it: back off a little
+        q = pick(p, short_only, &h, &k, &w, &ver, &sub);
+      }
       if (lane == 0) {
+        if (tries > 1) atomicAdd(p.stats + kQueues * 4 + 3, (unsigned long long)(tries - 1));
         s_q = q == kRetry ? kNone : q;  // lost every race: rescan after a short sleep
         s_h = h;
         s_k = k;
@@ -305,18 +330,27 @@ __global__ void __launch_bounds__(256, 2) service_kernel(Svc p) {
     const uint32_t h = s_h, k = s_k;
     const bool w = s_w != 0u;
     if (q == kNone) {
-      if (tid == 0) s_exit = idle(p, short_only, idle_since, s_ver, s_sub) ? 1u : 0u;
+      if (tid == 0) {
+        const uint64_t t0 = globaltimer_ns();
+        s_exit = idle(p, short_only, idle_since, s_ver, s_sub) ? 1u : 0u;
+        atomicAdd(p.stats + kQueues * 4, (unsigned long long)(globaltimer_ns() - t0));
+      }
       __syncthreads();
       if (s_exit) break;
       continue;
     }
     if (tid == 0) idle_since = 0;
     if (q == kAdmit) {
+      if (tid == 0) {
+        atomicAdd(p.stats + kQueues * 4 + 1, 1ull);
+        atomicAdd(p.stats + kQueues * 4 + 2, (unsigned long long)k);
+      }
       for (uint32_t i = tid; i < k; i += blockDim.x) {
         const uint32_t r = (h + i) & p.qmask;
         push(p, queue_of(p.req[r].scheme, p.req[r].op, 0), r);
       }
       __syncthreads();
+      if (tid == 0) wake(p);
       continue;
     }
     const int scheme = q_scheme(q), op = q_op(q), stage = q_stage(q);
@@ -324,25 +358,32 @@ __global__ void __launch_bounds__(256, 2) service_kernel(Svc p) {
     const int code = code_of(scheme, op, stage, p.form);
     if ((uint32_t)tid < k) s_r[tid] = take(p, q, h + tid);
     __syncthreads();
+    const uint64_t t_claim = tid == 0 ? globaltimer_ns() : 0;
     if (kind == K_CTA) {
-      const uint32_t r = s_r[0];
-      if (r != ~0u) cta_stage(code, p.req[r], smem, tbase, &p.ctl->err.v);
-      __syncthreads();
-      if (tid == 0 && r != ~0u) {
-        const uint32_t e = ld_relaxed(&p.ctl->err.v);  // an expired wait inside the stage
-        if (e != 0u) *p.host_err = e;
-        advance(p, scheme, op, stage, r);
+      for (uint32_t i = 0; i < k; i++) {
+        const uint32_t r = s_r[i];
+        if (r != ~0u) cta_stage(code, p.req[r], smem, tbase, &p.ctl->err.v);
+        __syncthreads();
+        if (tid == 0 && r != ~0u) {
+          const uint32_t e = ld_relaxed(&p.ctl->err.v);  // an expired wait inside the stage
+          if (e != 0u) *p.host_err = e;
+          advance(p, scheme, op, stage, r);
+          wake(p);
+        }
       }
     } else if (w) {
       const int slot = kind == K_THREAD2 ? warp >> 1 : warp, role = kind == K_THREAD2 ? warp & 1 : 0;
       if ((uint32_t)slot < k && s_r[slot] != ~0u) {  // warp-uniform: every lane runs the stage
         const uint32_t r = s_r[slot];
         warp_stage(p.key, code, p.req[r], role);
-        __threadfence_system();  // every lane's writes, before the hand-off (host-visible at the end)
+        // every lane's writes before the hand-off; host-visible after the last stage
+        if (stage + 1 == nstages(scheme, op)) __threadfence_system();
+        else __threadfence();
         __syncwarp();
         if (lane == 0) {
           if (kind == K_THREAD2) role_done(p, scheme, op, stage, r);
           else advance(p, scheme, op, stage, r);
+          wake(p);
         }
       }
     } else {
@@ -356,6 +397,14 @@ __global__ void __launch_bounds__(256, 2) service_kernel(Svc p) {
       }
     }
     __syncthreads();  // s_r and the claim words are rewritten by the next pick
+    if (tid == 0) {
+      if (kind != K_CTA && !w) wake(p);  // the thread-per-instance claim's pushes
+      unsigned long long *qs = p.stats + q * 4;
+      atomicAdd(qs, 1ull);
+      atomicAdd(qs + 1, (unsigned long long)k);
+      if (w) atomicAdd(qs + 2, 1ull);
+      atomicAdd(qs + 3, (unsigned long long)(globaltimer_ns() - t_claim));
+    }
   }
   tc_fence_before();
   __syncthreads();
@@ -534,7 +583,7 @@ int dpkem_service_open(dpkem_ctx *c, int form, const dpkem_service_config *cfg_i
   while (slots < cfg.max_inflight) slots <<= 1;
   const uint64_t scr = cfg.scratch_bytes ? cfg.scratch_bytes : (uint64_t)slots * mixed::kFrodoRec;
   if (scr < mixed::kFrodoRec) return set_status(DPKEM_EINVAL);
-  const size_t o_req = up(sizeof(serve::Ctl)), o_done = o_req + up((size_t)slots * sizeof(mixed::DevReq));
+  const size_t o_stats = up(sizeof(serve::Ctl)), o_req = o_stats + up(serve::kStats * 8), o_done = o_req + up((size_t)slots * sizeof(mixed::DevReq));
   const size_t o_ent = o_done + up((size_t)slots * 4), o_scr = o_ent + up((size_t)serve::kQueues * slots * 8);
   const size_t total = o_scr + up(scr);
   if (total > c->budget) return set_status(DPKEM_ENOMEM);
@@ -589,6 +638,7 @@ int dpkem_service_open(dpkem_ctx *c, int form, const dpkem_service_config *cfg_i
   }
   serve::Svc &p = s->p;
   p.ctl = s->ctl;
+  p.stats = reinterpret_cast<unsigned long long *>(s->dmem + o_stats);
   p.req = s->d_req;
   p.done = reinterpret_cast<uint32_t *>(s->dmem + o_done);
   p.ent = ent;
@@ -709,6 +759,18 @@ int dpkem_service_stats(dpkem_service *s, uint64_t *submitted, uint64_t *complet
   if (launches) *launches = s->launches;
   if (running) *running = s->running ? 1 : 0;
   return set_status(DPKEM_OK);
+}
+
+int dpkem_service_counters(dpkem_service *s, uint64_t *out, size_t n, int reset) {
+  if (!s || (n && !out)) return set_status(DPKEM_EINVAL);
+  std::lock_guard<std::mutex> lock(s->mu);
+  cudaSetDevice(s->c->device);
+  const size_t k = std::min<size_t>(n, serve::kStats);
+  cudaError_t e = cudaSuccess;
+  if (k) e = cudaMemcpyAsync(out, s->p.stats, k * 8, cudaMemcpyDeviceToHost, s->cst);
+  if (e == cudaSuccess && reset) e = cudaMemsetAsync(s->p.stats, 0, serve::kStats * 8, s->cst);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->cst);
+  return set_status(cuda_status(e));
 }
 
 int dpkem_service_close(dpkem_service *s) {

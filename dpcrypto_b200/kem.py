@@ -114,6 +114,7 @@ EXPORTS = {
     "dpkem_service_drain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
     "dpkem_service_stats": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_uint64)] * 3
                             + [ctypes.POINTER(ctypes.c_int)]),
+    "dpkem_service_counters": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]),
     "dpkem_service_close": (ctypes.c_int, [ctypes.c_void_p]),
     # wire format and shared-memory ring (include/dpkem_wire.h)
     "dpkem_frame_bytes": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t),
@@ -570,6 +571,23 @@ class Service:
         if rc != OK:
             raise DpkemError(rc, "service_stats")
         return {"submitted": a.value, "completed": b.value, "launches": c.value, "running": bool(r.value)}
+
+    def counters(self, reset: bool = False) -> dict:
+        """Per-queue claims / instances / warp claims / busy ms, keyed "scheme/op/stage", plus
+        idle_ms, admissions, admitted and lost_claims (dpkem_service_counters)."""
+        buf = np.zeros(244, np.uint64)
+        rc = self._lib.dpkem_service_counters(self._h, ctypes.c_void_p(buf.ctypes.data), len(buf), int(reset))
+        if rc != OK:
+            raise DpkemError(rc, "service_counters")
+        out = {}
+        for q in range(60):
+            c = buf[4 * q:4 * q + 4]
+            if c[0]:
+                out[f"{q // 12}/{(q >> 2) % 3}/{q & 3}"] = {"claims": int(c[0]), "instances": int(c[1]),
+                                                          "warp_claims": int(c[2]), "busy_ms": float(c[3]) * 1e-6}
+        out["idle_ms"] = float(buf[240]) * 1e-6
+        out["admissions"], out["admitted"], out["lost_claims"] = int(buf[241]), int(buf[242]), int(buf[243])
+        return out
 
     def close(self):
         if getattr(self, "_h", None):

@@ -176,6 +176,12 @@ int dpkem_service_drain(dpkem_service *svc, uint32_t timeout_ms);
 /* Counters: tickets issued, tickets completed in order, launches so far, launch running now. */
 int dpkem_service_stats(dpkem_service *svc, uint64_t *submitted, uint64_t *completed, uint64_t *launches,
                         int *running);
+/* Diagnostic counters since open (or the last reset), up to n of them: for each queue
+ * q = (scheme * 3 + op) * 4 + stage, out[4q .. 4q+3] = claims, instances, claims run as a warp
+ * per instance, busy ns (claim to hand-off, summed over CTAs); then out[240] = CTA idle ns,
+ * out[241] = admissions, out[242] = requests admitted, out[243] = claims lost to another CTA.  Counters are updated while the launch
+ * runs; a read during traffic is a snapshot. */
+int dpkem_service_counters(dpkem_service *svc, uint64_t *out, size_t n, int reset);
 /* Drains (30 s at most), ends the launch and frees the service. */
 int dpkem_service_close(dpkem_service *svc);
 

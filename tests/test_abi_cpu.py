@@ -86,7 +86,7 @@ def test_tuning_knobs():
                     "pipe_chunks": 4, "pipe_priority": 1, "saber_pair_max": 6144, "saber_five_max": 0,
                     "saber_finish_five_max": 0, "frodo_five_max": 0, "frodo_ss_five_max": 0,
                     "saber_tc_ctas_per_sm": 0, "saber_warp_max": 512, "saber_finish_warp_max": 1024,
-                    "frodo_warp_max": 1024, "frodo_ss_warp_max": 1024, "mixed_warp_max": 512}
+                    "frodo_warp_max": 1024, "frodo_ss_warp_max": 1024, "mixed_warp_max": 0}
         for k in kem.RUNTIME_KNOBS:
             lib.dpkem_set_tuning(k.encode(), saved.get(k, defaults[k]))
 
