@@ -133,6 +133,51 @@ def run_reference(args, world, rank):
 
 
 # ---------------------------------------------------------------- GPU helpers
+ONE_LANE = dict(saber_warp_max=0, saber_finish_warp_max=0, saber_five_max=0, saber_finish_five_max=0,
+                saber_pair_max=0, frodo_warp_max=0, frodo_ss_warp_max=0, frodo_five_max=0, frodo_ss_five_max=0)
+
+
+def bench_single(eng, reps: int = 7) -> dict:
+    """One request alone (n = 1, tc form): per-stage device times (stage timer, median of
+    `reps`) of FrodoKEM-976 and Saber l=3 encaps and decaps, the sponge stages on a warp per
+    state (the default at this size) and on one thread per state."""
+    from dpcrypto_b200 import kem as K
+
+    out = {}
+    for scheme, name in ((d.FRODO976, "frodo976"), (d.SABER, "saber_l3")):
+        z = d.sizes(scheme)
+        kc = torch.empty((1, z["kp_coins"]), dtype=torch.uint8, device="cuda")
+        ec = torch.empty((1, z["enc_coins"]), dtype=torch.uint8, device="cuda")
+        eng.coins(1, z["kp_coins"], "single-kp", out=kc)
+        eng.coins(1, z["enc_coins"], "single-enc", out=ec)
+        pk, sk = eng.keypair(scheme, kc, d.FORM_TC)
+        ct = torch.empty((1, z["ct"]), dtype=torch.uint8, device="cuda")
+        ss = torch.empty((1, z["ss"]), dtype=torch.uint8, device="cuda")
+        res = {"enc_stages": ["prologue", "product", "final hash"] if scheme == d.FRODO976 else
+               ["prologue", "product", "finish"],
+               "dec_stages": ["W / decode", "prologue", "product", "final hash"] if scheme == d.FRODO976 else
+               ["inner product", "prologue", "product", "finish"]}
+        for layout, kv in (("warp_per_state", {}), ("one_lane", ONE_LANE)):
+            with K.knobs(**kv):
+                eng.enc(scheme, pk, ec, d.FORM_TC, out=(ct, ss))
+                eng.dec(scheme, ct, sk, d.FORM_TC)
+                torch.cuda.synchronize()
+                eng.profile(True)
+                es, ds = [], []
+                for _ in range(reps):
+                    eng.enc(scheme, pk, ec, d.FORM_TC, out=(ct, ss))
+                    es.append(eng.stage_times())
+                    eng.dec(scheme, ct, sk, d.FORM_TC)
+                    ds.append(eng.stage_times())
+                eng.profile(False)
+            enc, dec = np.median(np.array(es), axis=0), np.median(np.array(ds), axis=0)
+            res[layout] = {"enc_stage_ms": [round(float(x), 4) for x in enc],
+                           "dec_stage_ms": [round(float(x), 4) for x in dec],
+                           "enc_ms": float(enc.sum()), "dec_ms": float(dec.sum())}
+        out[name] = res
+    return out
+
+
 def bench_frames(eng, form, n: int = 16384, reps: int = 3) -> dict:
     """dpkem_frames_run on n mixed request frames (pinned host block in, pinned block out,
     copies inside the timing), and the same block served through the ring by the frame
@@ -553,6 +598,7 @@ def main():
         sres["tc_product_tensor_frac"] = sres["tc_product_int8_macs_per_s"] / line["tensor"]["i8_mma_peak_macs_per_s"]
         sres["product_stage_tc_over_int32"] = sres["int32_product_ms"] / sres["tc_product_ms"]
         line["saber_l3_batch4096"] = dict(sres, unit=UNIT)
+        line["single_request"] = bench_single(eng)
 
     # ---- mixed persistent batch: 16384 requests, 4 schemes x 3 ops, one CUDA-graph launch ----
     if not args.no_secondary:
