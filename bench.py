@@ -141,6 +141,10 @@ def bench_single(eng, reps: int = 7) -> dict:
     """One request alone (n = 1, tc form): per-stage device times (stage timer, median of
     `reps`) of FrodoKEM-976 and Saber l=3 encaps and decaps, the sponge stages on a warp per
     state (the default at this size) and on one thread per state."""
+    import numpy as np
+    import torch
+
+    import dpcrypto_b200 as d
     from dpcrypto_b200 import kem as K
 
     out = {}
