@@ -368,7 +368,10 @@ int run_shared(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8
   if (cudaSetDevice(c->device) != cudaSuccess) return cuda_status(cudaErrorInvalidDevice);
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
   const size_t chunk = std::min(n, chunk_for(c, scheme, op, false));
-  int rc = ensure_arena(c, arena_need(scheme, op, chunk, false) + kAlign);
+  // With A in memory, the tensor-core form runs the products as one GEMM on tiled operands.
+  const bool gemm = amat && form == DPKEM_FORM_TC;
+  const size_t tiles = gemm ? up(frodo_gemm_ab_bytes()) + up(frodo_gemm_s_bytes(chunk)) : 0;
+  int rc = ensure_arena(c, arena_need(scheme, op, chunk, false) + kAlign + tiles);
   if (rc) return rc;
   cudaError_t e = cudaStreamWaitEvent(st, c->last, 0);
   if (e != cudaSuccess) return cuda_status(e);
@@ -380,6 +383,10 @@ int run_shared(dpkem_ctx *c, int scheme, int form, int op, size_t n, const uint8
   fb.fail = cv.take<uint32_t>(chunk * 4);
   fb.hs = cv.take<uint2>(chunk * 200);
   uint8_t *pkh = cv.take<uint8_t>(kAlign);
+  if (gemm) {
+    fb.abt = cv.take<uint8_t>(frodo_gemm_ab_bytes());
+    fb.stile = cv.take<uint8_t>(frodo_gemm_s_bytes(chunk));
+  }
   fb.aes = scheme == DPKEM_FRODO976AES;
   fb.err = c->d_err;
   fb.shared = 1;

@@ -94,6 +94,11 @@ struct FrodoBatch {
   int shared;
   const uint16_t *amat;
   const uint8_t *pkh;
+  // Shared key with A in memory, tensor-core form: the S'A and S'B products of all instances
+  // run as one GEMM (frodo_gemm.cuh) on operand tiles prepared in these scratch buffers
+  // ([A | B] limb tiles, fgemm::AB_BYTES; S' tiles, fgemm::s_bytes(n)); null: per-instance path.
+  uint8_t *abt;
+  uint8_t *stile;
 };
 
 struct SaberBatch {
@@ -121,6 +126,9 @@ cudaError_t frodo_dec(const FrodoBatch &b, int form, cudaStream_t st);
 // Shared-key helpers: A of one public key (aes: the AES-128 variant) into amat (976 x 976
 // LE u16), and H(pk) = SHAKE256(pk, 24) of one public key into out.
 cudaError_t frodo_expand_a(int aes, const uint8_t *pk, uint16_t *amat, cudaStream_t st);
+// Scratch of the shared-key tensor-core GEMM: [A | B] operand tiles, S' tiles for n instances.
+size_t frodo_gemm_ab_bytes();
+size_t frodo_gemm_s_bytes(size_t n);
 cudaError_t frodo_pk_digest(const uint8_t *pk, uint8_t *out, cudaStream_t st);
 
 cudaError_t saber_keypair(const SaberBatch &b, int form, cudaStream_t st);

@@ -2,6 +2,7 @@
 // stage over n instances.  The stage bodies live in frodo_dev.cuh (shared with the persistent
 // mixed-batch kernel); these wrappers only map blockIdx/threadIdx to instances.
 #include "frodo_dev.cuh"
+#include "frodo_gemm.cuh"
 
 namespace dpkem {
 namespace {
@@ -185,8 +186,25 @@ cudaError_t launch_sa_g(const FrodoBatch &b, int form, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// Shared key, A in memory, tensor-core form: one GEMM over all instances (frodo_gemm.cuh).
+template <int MODE>
+cudaError_t launch_sa_gemm(const FrodoBatch &b, cudaStream_t st) {
+  using namespace fgemm;
+  cudaError_t e;
+  const int groups = (b.n + INST - 1) / INST;
+  tile_ab_kernel<<<blocks_for(MT * KSTEPS * 2 * 8 * 32, 256), 256, 0, st>>>(b.amat, MODE == OP_ENC ? b.pk : b.sk + LENS,
+                                                                             b.abt);
+  tile_s_kernel<<<blocks_for(groups * INST * NBAR * 62, 256), 256, 0, st>>>(b.rw, b.n, b.stile);
+  if (MODE == OP_DEC && (e = cudaMemsetAsync(b.fail, 0, (size_t)b.n * 4, st)) != cudaSuccess) return e;
+  if ((e = set_smem(gemm_kernel<MODE>, SMEM_LAUNCH)) != cudaSuccess) return e;
+  const GemmArgs g{b.abt, b.stile, b.rw, MODE == OP_ENC ? b.coins : b.mu, b.ct, b.fail, b.err, b.n};
+  gemm_kernel<MODE><<<MT * groups, THREADS, SMEM_LAUNCH, st>>>(g);
+  return cudaGetLastError();
+}
+
 template <int MODE>
 cudaError_t launch_sa(const FrodoBatch &b, int form, cudaStream_t st) {
+  if (b.amat && b.abt && b.stile && form == FORM_TC) return launch_sa_gemm<MODE>(b, st);
   if (b.amat) return launch_sa_g<MODE, fdev::MemRows, fdev::MemRows, kTcStages>(b, form, st);
   if (b.aes) return launch_sa_g<MODE, fdev::AesRowsFull, fdev::AesRowsHalf, 1>(b, form, st);
   return launch_sa_g<MODE, fdev::ShakeRows, fdev::ShakeRows, kTcStages>(b, form, st);
@@ -260,6 +278,9 @@ cudaError_t frodo_expand_a(int aes, const uint8_t *pk, uint16_t *amat, cudaStrea
   }
   return cudaGetLastError();
 }
+
+size_t frodo_gemm_ab_bytes() { return fgemm::AB_BYTES; }
+size_t frodo_gemm_s_bytes(size_t n) { return fgemm::s_bytes((int)n); }
 
 cudaError_t frodo_pk_digest(const uint8_t *pk, uint8_t *out, cudaStream_t st) {
   pk_digest_kernel<<<1, 32, 0, st>>>(pk, out);

@@ -50,3 +50,35 @@ def test_shared_key_enc_dec_match_oracle(engine, oracle, scheme, form, with_a):
     torch.cuda.synchronize()
     assert (ss2.cpu().numpy() == ss_o).all()
     assert (ss3.cpu().numpy() == ssb_o).all()
+
+
+@pytest.mark.parametrize("scheme", [d.FRODO976, d.FRODO976AES])
+def test_shared_key_gemm_groups_and_tampering(engine, oracle, scheme):
+    """The tensor-core shared-key path (A in memory: the products as one GEMM over 16-instance
+    groups) at a size with a partial last group; decaps ciphertexts tampered in B' (one
+    instance in three), in C (one in three) or left intact, against the oracle and against the
+    same batch with A regenerated per instance."""
+    n = 37
+    kc = oracle.coins(1, 64, "kp", first=977)
+    pk, sk = oracle.keypair(scheme, kc)
+    ec = oracle.coins(n, 24, "enc", first=977)
+    pk_n, sk_n = np.repeat(pk, n, axis=0), np.repeat(sk, n, axis=0)
+    ct_o, ss_o = oracle.enc(scheme, pk_n, ec, threads=8)
+    bad = ct_o.copy()
+    pkb = 2 * 976 * 8
+    for i in range(n):
+        if i % 3 == 0:
+            bad[i, pkb + (13 * i) % 128] ^= 1 << (i % 8)
+        elif i % 3 == 1:
+            bad[i, (7919 * i) % pkb] ^= 1 << (i % 8)
+    ssb_o = oracle.dec(scheme, bad, sk_n, threads=8)
+    dpk, dsk = torch.from_numpy(pk[0].copy()).cuda(), torch.from_numpy(sk[0].copy()).cuda()
+    amat = engine.expand_a(scheme, dpk)
+    ct, ss = engine.enc_shared(scheme, dpk, torch.from_numpy(ec).cuda(), d.FORM_TC, amat)
+    ssb = engine.dec_shared(scheme, torch.from_numpy(bad).cuda(), dsk, d.FORM_TC, amat)
+    ssb_regen = engine.dec_shared(scheme, torch.from_numpy(bad).cuda(), dsk, d.FORM_TC, None)
+    torch.cuda.synchronize()
+    assert (ct.cpu().numpy() == ct_o).all() and (ss.cpu().numpy() == ss_o).all()
+    assert (ssb.cpu().numpy() == ssb_o).all()
+    assert torch.equal(ssb, ssb_regen)
+    assert not (ssb_o[2::3] != ss_o[2::3]).any() and (ssb_o[0::3] != ss_o[0::3]).all()
