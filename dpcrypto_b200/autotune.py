@@ -12,7 +12,7 @@ Knobs:
                      Frodo shared-secret hash) and batch size: a warp per state
                      (*_warp_max), five lanes (*_five_max), a lane pair (saber_pair_max,
                      Saber only) or one lane.  Each layout is forced in turn at 64-16k
-                     instances and timed with the stage timer; a layout covers batches up
+                     instances (Frodo 64-8k) and timed with the stage timer; a layout covers batches up
                      to the largest swept size at which it was the fastest
   saber_tc_ctas_per_sm  persistent Saber tensor-core product (CTAs per SM) or a CTA per
                      instance (0)
@@ -160,7 +160,7 @@ def _child(u: int) -> dict:
 # one lane); the stage's device time comes from the stage timer of an encaps + decaps.
 BIG = 1 << 30
 SABER_SIZES = (64, 256, 512, 1024, 2048, 4096, 8192, 16384)
-FRODO_SIZES = (64, 256, 512, 1024, 2048, 4096)
+FRODO_SIZES = (64, 256, 512, 1024, 2048, 4096, 8192)
 LAYOUTS = {
     # stage: {layout: knob values}, and the stage timer slots (encaps, decaps) it owns
     "saber_prologue": ({"warp": dict(saber_warp_max=BIG),

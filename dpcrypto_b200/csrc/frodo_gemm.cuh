@@ -19,11 +19,14 @@
 // (tile_ab_kernel); the S' tiles from the sampled words of each instance (tile_s_kernel).
 //
 // CTA (192 threads): warp 0 lane 0 issues the bulk copies of a 6-stage ring, warp 1 lane 0 the
-// MMAs (two per K step, one per limb), warps 2-5 read the accumulators back (warp w reads
-// TMEM lanes 32 (w % 4) .. +31, the rows of D its lanes own) and add E' (or E'' and the
-// encoded message), then store the ciphertext (encaps) or compare it (decaps: an OR of the
-// differences into each instance's fail word, zeroed before the launch).  Every wait is a
-// bounded mbarrier wait; an expired one sets the error word and the CTA skips the rest.
+// MMAs (two per K step, one per limb), warps 2-5 handle the epilogue.  While the MMAs run
+// they load the tile's terms into shared memory with 16-byte loads (E', or E'' + encode(mu)
+// for V's columns; decaps: the expected product ct - term), then read the accumulators back
+// (warp w reads TMEM lanes 32 (w % 4) .. +31, the columns m its lanes own), and either write
+// the sums into the same buffer and store the ciphertext rows with 16-byte stores (encaps)
+// or compare (decaps: an OR of the differences into each instance's fail word, zeroed
+// before the launch).  Every wait is a bounded mbarrier wait; an expired one sets the error
+// word and the CTA skips the rest.
 #pragma once
 #include <cstdint>
 
@@ -43,10 +46,13 @@ constexpr int NST = 6;                     // ring stages
 constexpr int STAGE = 3 * CHUNK;           // A lo, A hi, S'
 constexpr int BARS = NST * STAGE;          // full[NST], empty[NST], done
 constexpr int TSLOT = BARS + (2 * NST + 1) * 8;
-constexpr int SMEM = TSLOT + 16;
+// Epilogue terms of the tile, [128 rows n][128 columns m] u16 (32 KB): encaps the term to add
+// (E', or E'' + encode(mu) in the 8 columns of V), decaps the expected product (ct - that term).
+constexpr int EBUF = (TSLOT + 16 + 127) & ~127;
+constexpr int SMEM = EBUF + 128 * 128 * 2;
 // Requested per CTA: more than the layout needs, so that at most two CTAs share an SM and
 // their TMEM allocations (256 columns each) always fit.
-constexpr int SMEM_LAUNCH = 100 * 1024;
+constexpr int SMEM_LAUNCH = 110 * 1024;
 static_assert(SMEM <= SMEM_LAUNCH, "layout exceeds the requested shared memory");
 constexpr int THREADS = 192;
 constexpr int TMEM_COLS = 256;             // lo accumulators 0..127, hi 128..255
@@ -171,11 +177,49 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(GemmArgs g) {
       if (ok) mma_commit(done);
       else atomicOr(g.err, DEV_ERR_TIMEOUT);
     }
-  } else {  // epilogue: warps 2..5, TMEM lanes 32 (warp % 4) ..
-    const int lg = warp & 3, m = 128 * mt + 32 * lg + lane;
-    ok = mbar_wait(done, 0);
+  } else {  // epilogue: warps 2..5 (128 threads), TMEM lanes 32 (warp % 4) ..
+    const int et = tid - 64, lg = warp & 3, ml = 32 * lg + lane;
+    uint16_t *eb = reinterpret_cast<uint16_t *>(sm + EBUF);
+    // While the MMAs run: the tile's epilogue terms, 16 bytes (8 columns of one row n) per step.
+    for (int x = et; x < 128 * 16; x += 128) {
+      const int n = x >> 4, q = x & 15, i = grp * INST + (n >> 3), k = n & 7, m0 = 128 * mt + 8 * q;
+      uint4 e = make_uint4(0, 0, 0, 0);
+      if (i < g.n && m0 < N + NBAR) {
+        const uint16_t *rwi = g.rw + (size_t)i * RW;
+        uint32_t t[8];
+        if (m0 < N) {
+          const uint4 v = *reinterpret_cast<const uint4 *>(rwi + N * NBAR + k * N + m0);  // E'
+          t[0] = v.x & 0xFFFFu, t[1] = v.x >> 16, t[2] = v.y & 0xFFFFu, t[3] = v.y >> 16;
+          t[4] = v.z & 0xFFFFu, t[5] = v.z >> 16, t[6] = v.w & 0xFFFFu, t[7] = v.w >> 16;
+        } else {  // V's columns: E'' + encode(mu), 3 bits of mu per entry
+          const uint4 v = *reinterpret_cast<const uint4 *>(rwi + 2 * N * NBAR + k * NBAR);
+          const uint8_t *mu = g.mu + (size_t)i * 24 + 3 * k;
+          const uint32_t t3 = mu[0] | ((uint32_t)mu[1] << 8) | ((uint32_t)mu[2] << 16);
+          t[0] = v.x & 0xFFFFu, t[1] = v.x >> 16, t[2] = v.y & 0xFFFFu, t[3] = v.y >> 16;
+          t[4] = v.z & 0xFFFFu, t[5] = v.z >> 16, t[6] = v.w & 0xFFFFu, t[7] = v.w >> 16;
+#pragma unroll
+          for (int l = 0; l < 8; l++) t[l] += ((t3 >> (3 * l)) & 7u) << 13;
+        }
+        if (MODE == OP_DEC) {  // expected product = ct - term (mod 2^16), ct big-endian
+          const uint8_t *c = g.ct + (size_t)i * CT + (m0 < N ? 2 * (k * N + m0) : PKB + 2 * k * NBAR);
+          const uint4 cv = *reinterpret_cast<const uint4 *>(c);
+          const uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
+#pragma unroll
+          for (int l = 0; l < 8; l++) {
+            const uint32_t b = (cw[l >> 1] >> (16 * (l & 1))) & 0xFFFFu;
+            t[l] = (((b & 0xFFu) << 8) | (b >> 8)) - t[l];
+          }
+        }
+        e = make_uint4((t[0] & 0xFFFFu) | (t[1] << 16), (t[2] & 0xFFFFu) | (t[3] << 16),
+                       (t[4] & 0xFFFFu) | (t[5] << 16), (t[6] & 0xFFFFu) | (t[7] << 16));
+      }
+      *reinterpret_cast<uint4 *>(eb + n * 128 + 8 * q) = e;
+    }
+    asm volatile("bar.sync 1, 128;" ::: "memory");  // the epilogue warps' terms are in place
+    ok = __all_sync(0xffffffffu, mbar_wait(done, 0));  // warp-uniform: tcgen05.ld is warp-wide
     if (!ok && lane == 0) atomicOr(g.err, DEV_ERR_TIMEOUT);
     tc_fence_after();
+    uint32_t diff = 0;  // decaps: bit h of instance slot h differs
     if (ok) {
 #pragma unroll 1
       for (int c0 = 0; c0 < 128; c0 += 16) {
@@ -184,40 +228,31 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(GemmArgs g) {
         tmem_ld16(tbase + ((uint32_t)(32 * lg) << 16) + 128 + c0, hi);
         tmem_wait_ld();
 #pragma unroll
-        for (int h = 0; h < 2; h++) {  // two instances per 16 columns
-          const int i = grp * INST + c0 / 8 + h;
-          uint32_t diff = 0;
-          if (i < g.n && m < N + NBAR) {
-            const uint16_t *rwi = g.rw + (size_t)i * RW;
-            uint8_t *ct = g.ct + (size_t)i * CT;
-            uint32_t t3[8];
-            if (m >= N) {
-              const uint8_t *mu = g.mu + (size_t)i * 24;
-#pragma unroll
-              for (int k = 0; k < 8; k++) t3[k] = mu[3 * k] | ((uint32_t)mu[3 * k + 1] << 8) | ((uint32_t)mu[3 * k + 2] << 16);
-            }
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-              uint32_t x = lo[8 * h + k] + (hi[8 * h + k] << 8);
-              uint8_t *d;
-              if (m < N) {
-                x += rwi[N * NBAR + k * N + m];  // E'
-                d = ct + 2 * (k * N + m);
-              } else {
-                const int l = m - N;
-                x += rwi[2 * N * NBAR + k * NBAR + l] + (((t3[k] >> (3 * l)) & 7u) << 13);  // E'' + encode(mu)
-                d = ct + PKB + 2 * (k * NBAR + l);
-              }
-              x &= 0xFFFFu;
-              if (MODE == OP_ENC) *reinterpret_cast<uint16_t *>(d) = (uint16_t)((x >> 8) | (x << 8));
-              else diff |= x ^ (((uint32_t)d[0] << 8) | d[1]);
-            }
-          }
-          if (MODE == OP_DEC) {
-            const unsigned any = __ballot_sync(0xffffffffu, diff != 0);
-            if (lane == 0 && any && i < g.n) atomicOr(g.fail + i, 1u);
-          }
+        for (int q = 0; q < 16; q++) {
+          const int n = c0 + q;
+          uint16_t *e = eb + n * 128 + ml;
+          const uint32_t x = (lo[q] + (hi[q] << 8) + (MODE == OP_ENC ? (uint32_t)*e : 0u)) & 0xFFFFu;
+          if (MODE == OP_ENC) *e = (uint16_t)((x >> 8) | (x << 8));  // big-endian bytes
+          else if (x != *e) diff |= 1u << (n >> 3);
         }
+      }
+    }
+    if (MODE == OP_ENC) {
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+      if (ok)  // coalesced: 16 bytes per thread, a row's 256 bytes per 16 threads
+        for (int x = et; x < 128 * 16; x += 128) {
+          const int n = x >> 4, q = x & 15, i = grp * INST + (n >> 3), k = n & 7, m0 = 128 * mt + 8 * q;
+          if (i >= g.n || m0 >= N + NBAR) continue;
+          uint8_t *c = g.ct + (size_t)i * CT + (m0 < N ? 2 * (k * N + m0) : PKB + 2 * k * NBAR);
+          *reinterpret_cast<uint4 *>(c) = *reinterpret_cast<const uint4 *>(eb + n * 128 + 8 * q);
+        }
+    } else {
+      // rows m >= 984 are padding (their terms and products are zero)
+#pragma unroll
+      for (int h = 0; h < INST; h++) {
+        const unsigned any = __ballot_sync(0xffffffffu, (diff >> h) & 1u);
+        const int i = grp * INST + h;
+        if (lane == 0 && any && i < g.n) atomicOr(g.fail + i, 1u);
       }
     }
   }
