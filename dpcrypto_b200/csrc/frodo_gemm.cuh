@@ -64,6 +64,13 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
+// 16 bytes global -> shared, asynchronous (L2 only); completion by cp_async_wait_all.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_all;" ::: "memory");
+}
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
@@ -180,46 +187,51 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(GemmArgs g) {
   } else {  // epilogue: warps 2..5 (128 threads), TMEM lanes 32 (warp % 4) ..
     const int et = tid - 64, lg = warp & 3, ml = 32 * lg + lane;
     uint16_t *eb = reinterpret_cast<uint16_t *>(sm + EBUF);
-    // While the MMAs run: the tile's epilogue terms, 16 bytes (8 columns of one row n) per step.
+    // While the MMAs run: the tile's terms, row n = 8 slot + k, columns m - 128 mt.  E' rows by
+    // asynchronous 16-byte copies (8 columns each); V's 8 columns (tile MT - 1, columns 80..87)
+    // E'' + encode(mu), one row per thread; zeros for padding columns and absent instances.
     for (int x = et; x < 128 * 16; x += 128) {
       const int n = x >> 4, q = x & 15, i = grp * INST + (n >> 3), k = n & 7, m0 = 128 * mt + 8 * q;
-      uint4 e = make_uint4(0, 0, 0, 0);
-      if (i < g.n && m0 < N + NBAR) {
-        const uint16_t *rwi = g.rw + (size_t)i * RW;
-        uint32_t t[8];
-        if (m0 < N) {
-          const uint4 v = *reinterpret_cast<const uint4 *>(rwi + N * NBAR + k * N + m0);  // E'
-          t[0] = v.x & 0xFFFFu, t[1] = v.x >> 16, t[2] = v.y & 0xFFFFu, t[3] = v.y >> 16;
-          t[4] = v.z & 0xFFFFu, t[5] = v.z >> 16, t[6] = v.w & 0xFFFFu, t[7] = v.w >> 16;
-        } else {  // V's columns: E'' + encode(mu), 3 bits of mu per entry
-          const uint4 v = *reinterpret_cast<const uint4 *>(rwi + 2 * N * NBAR + k * NBAR);
-          const uint8_t *mu = g.mu + (size_t)i * 24 + 3 * k;
-          const uint32_t t3 = mu[0] | ((uint32_t)mu[1] << 8) | ((uint32_t)mu[2] << 16);
-          t[0] = v.x & 0xFFFFu, t[1] = v.x >> 16, t[2] = v.y & 0xFFFFu, t[3] = v.y >> 16;
-          t[4] = v.z & 0xFFFFu, t[5] = v.z >> 16, t[6] = v.w & 0xFFFFu, t[7] = v.w >> 16;
-#pragma unroll
-          for (int l = 0; l < 8; l++) t[l] += ((t3 >> (3 * l)) & 7u) << 13;
-        }
-        if (MODE == OP_DEC) {  // expected product = ct - term (mod 2^16), ct big-endian
-          const uint8_t *c = g.ct + (size_t)i * CT + (m0 < N ? 2 * (k * N + m0) : PKB + 2 * k * NBAR);
-          const uint4 cv = *reinterpret_cast<const uint4 *>(c);
-          const uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
-#pragma unroll
-          for (int l = 0; l < 8; l++) {
-            const uint32_t b = (cw[l >> 1] >> (16 * (l & 1))) & 0xFFFFu;
-            t[l] = (((b & 0xFFu) << 8) | (b >> 8)) - t[l];
-          }
-        }
-        e = make_uint4((t[0] & 0xFFFFu) | (t[1] << 16), (t[2] & 0xFFFFu) | (t[3] << 16),
-                       (t[4] & 0xFFFFu) | (t[5] << 16), (t[6] & 0xFFFFu) | (t[7] << 16));
-      }
-      *reinterpret_cast<uint4 *>(eb + n * 128 + 8 * q) = e;
+      uint16_t *dst = eb + n * 128 + 8 * q;
+      if (i < g.n && m0 < N) cp_async16(dst, g.rw + (size_t)i * RW + N * NBAR + k * N + m0);
+      else if (!(i < g.n && m0 == N)) *reinterpret_cast<uint4 *>(dst) = make_uint4(0, 0, 0, 0);
     }
-    asm volatile("bar.sync 1, 128;" ::: "memory");  // the epilogue warps' terms are in place
+    if (mt == MT - 1) {
+      const int n = et, i = grp * INST + (n >> 3), k = n & 7;
+      if (i < g.n) {
+        const uint4 v = *reinterpret_cast<const uint4 *>(g.rw + (size_t)i * RW + 2 * N * NBAR + k * NBAR);
+        const uint8_t *mu = g.mu + (size_t)i * 24 + 3 * k;
+        const uint32_t t3 = mu[0] | ((uint32_t)mu[1] << 8) | ((uint32_t)mu[2] << 16);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        uint32_t o[4];
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+          const uint32_t e0 = (w[h] + (((t3 >> (6 * h)) & 7u) << 13)) & 0xFFFFu;
+          const uint32_t e1 = ((w[h] >> 16) + (((t3 >> (6 * h + 3)) & 7u) << 13)) & 0xFFFFu;
+          o[h] = e0 | (e1 << 16);
+        }
+        *reinterpret_cast<uint4 *>(eb + n * 128 + (N - 128 * mt)) = make_uint4(o[0], o[1], o[2], o[3]);
+      }
+    }
+    // Decaps: this thread's pieces of the ciphertext tile (the compare pass below), loaded
+    // now so that they arrive while the MMAs run.
+    uint4 cv[INST];
+    if (MODE == OP_DEC) {
+#pragma unroll
+      for (int sl = 0; sl < INST; sl++) {
+        const int x = et + 128 * sl, n = x >> 4, q = x & 15, i = grp * INST + sl, k = n & 7, m0 = 128 * mt + 8 * q;
+        cv[sl] = make_uint4(0, 0, 0, 0);
+        if (i < g.n && m0 < N + NBAR)
+          cv[sl] = *reinterpret_cast<const uint4 *>(g.ct + (size_t)i * CT +
+                                                     (m0 < N ? 2 * (k * N + m0) : PKB + 2 * k * NBAR));
+      }
+    }
+    cp_async_wait_all();
+    asm volatile("bar.sync 1, 128;" ::: "memory");  // every epilogue warp's terms are in place
     ok = __all_sync(0xffffffffu, mbar_wait(done, 0));  // warp-uniform: tcgen05.ld is warp-wide
     if (!ok && lane == 0) atomicOr(g.err, DEV_ERR_TIMEOUT);
     tc_fence_after();
-    uint32_t diff = 0;  // decaps: bit h of instance slot h differs
+    // D + term (mod 2^16) over the terms: big-endian bytes (encaps, ready to store) or the value
     if (ok) {
 #pragma unroll 1
       for (int c0 = 0; c0 < 128; c0 += 16) {
@@ -229,30 +241,30 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_kernel(GemmArgs g) {
         tmem_wait_ld();
 #pragma unroll
         for (int q = 0; q < 16; q++) {
-          const int n = c0 + q;
-          uint16_t *e = eb + n * 128 + ml;
-          const uint32_t x = (lo[q] + (hi[q] << 8) + (MODE == OP_ENC ? (uint32_t)*e : 0u)) & 0xFFFFu;
-          if (MODE == OP_ENC) *e = (uint16_t)((x >> 8) | (x << 8));  // big-endian bytes
-          else if (x != *e) diff |= 1u << (n >> 3);
+          uint16_t *e = eb + (c0 + q) * 128 + ml;
+          const uint32_t x = (lo[q] + (hi[q] << 8) + (uint32_t)*e) & 0xFFFFu;
+          *e = MODE == OP_ENC ? (uint16_t)((x >> 8) | (x << 8)) : (uint16_t)x;
         }
       }
     }
-    if (MODE == OP_ENC) {
-      asm volatile("bar.sync 1, 128;" ::: "memory");
-      if (ok)  // coalesced: 16 bytes per thread, a row's 256 bytes per 16 threads
-        for (int x = et; x < 128 * 16; x += 128) {
-          const int n = x >> 4, q = x & 15, i = grp * INST + (n >> 3), k = n & 7, m0 = 128 * mt + 8 * q;
-          if (i >= g.n || m0 >= N + NBAR) continue;
-          uint8_t *c = g.ct + (size_t)i * CT + (m0 < N ? 2 * (k * N + m0) : PKB + 2 * k * NBAR);
-          *reinterpret_cast<uint4 *>(c) = *reinterpret_cast<const uint4 *>(eb + n * 128 + 8 * q);
-        }
-    } else {
-      // rows m >= 984 are padding (their terms and products are zero)
+    asm volatile("bar.sync 1, 128;" ::: "memory");
+    // Rows in 16-byte pieces: iteration s covers instance slot s (8 rows x 16 pieces = 128).
+    if (ok) {
 #pragma unroll
-      for (int h = 0; h < INST; h++) {
-        const unsigned any = __ballot_sync(0xffffffffu, (diff >> h) & 1u);
-        const int i = grp * INST + h;
-        if (lane == 0 && any && i < g.n) atomicOr(g.fail + i, 1u);
+      for (int sl = 0; sl < INST; sl++) {
+        const int x = et + 128 * sl, n = x >> 4, q = x & 15, i = grp * INST + sl, k = n & 7, m0 = 128 * mt + 8 * q;
+        const bool live = i < g.n && m0 < N + NBAR;
+        const uint4 v = *reinterpret_cast<const uint4 *>(eb + n * 128 + 8 * q);
+        if (MODE == OP_ENC) {
+          if (live)
+            *reinterpret_cast<uint4 *>(g.ct + (size_t)i * CT + (m0 < N ? 2 * (k * N + m0) : PKB + 2 * k * NBAR)) = v;
+        } else {
+          // ct is big-endian: swap each 16-bit half before comparing; rows m >= 984 and
+          // absent instances hold zeros on both sides
+          const uint32_t d = (__byte_perm(cv[sl].x, 0, 0x2301) ^ v.x) | (__byte_perm(cv[sl].y, 0, 0x2301) ^ v.y) |
+                             (__byte_perm(cv[sl].z, 0, 0x2301) ^ v.z) | (__byte_perm(cv[sl].w, 0, 0x2301) ^ v.w);
+          if (__ballot_sync(0xffffffffu, live && d != 0) && lane == 0 && i < g.n) atomicOr(g.fail + i, 1u);
+        }
       }
     }
   }

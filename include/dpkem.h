@@ -212,8 +212,10 @@ int dpkem_probe_i8_mma_peak(dpkem_ctx *ctx, double *macs_per_s);
  * Many encapsulations to one public key, or many decapsulations with one secret key (a
  * server decapsulating under its own key): the n instances share the key's matrix A, so it
  * can be expanded once (dpkem_frodo_expand_a: A as 976 x 976 little-endian u16, row-major,
- * 1,905,152 bytes, 16-byte aligned) and read by every instance's S'A stage instead of being
- * regenerated by each (amat NULL keeps the generation).  Encaps also hashes pk once.  Byte
+ * 1,905,152 bytes, 16-byte aligned) and read from memory instead of being regenerated by each
+ * instance (amat NULL keeps the generation).  With amat and DPKEM_FORM_TC the products of all
+ * instances run as one int8 tcgen05 GEMM (S' of every instance times [A | B]); the other forms
+ * read A's rows per instance.  Encaps also hashes pk once.  Byte
  * layouts are the batched calls'; results equal dpkem_enc_batch / dpkem_dec_batch with the
  * key repeated n times.  dpkem_sync() reports device-side errors.  No counterpart in the
  * reference, whose instances all regenerate A (FrodoKEM976-GPU/src/cuda_kernel.cu:172-173,
