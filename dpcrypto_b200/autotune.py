@@ -143,7 +143,7 @@ def _child(u: int) -> dict:
     psweep = {}
     for prio in (0, 1):
         kem.set_tuning("pipe_priority", prio)
-        for pc in (2, 4, 6, 8):
+        for pc in (4, 8, 12, 16):
             kem.set_tuning("pipe_chunks", pc)
             eng.enc(d.FRODO976, h_pk, h_ec, d.FORM_TC, out=(h_ct, h_ss))
             t0 = time.perf_counter()
@@ -331,7 +331,9 @@ def measure() -> dict:
         "chosen": {"keccak_unroll": best["keccak_unroll"], "thread_block": int(tb), "mixed_frodo_task": ft,
                    "mixed_pair_task": stt, "mixed_thread_task": tt, "pipe_chunks": pc,
                    "pipe_priority": prio, **lanes},
-        "fixed": {"mma_tile": "M=128 (N=8 Frodo, N=8/16 Saber), K=32: int8 MMA <1% of the tensor pipe",
+        "fixed": {"mma_tile": "M=128 (N=8 Frodo, N=8/16 Saber), K=32: int8 MMA <1% of the tensor pipe in the fused "
+                              "per-instance kernels; the shared-key GEMM: M=128 columns of [A | B] x N=128 rows (16 "
+                              "instances), two CTAs per SM (TMEM)",
                   "keccak_lanes_per_state_fused_sa_stages": 1},
         "measurements": results,
         "command": "python -m dpcrypto_b200.autotune --measure",

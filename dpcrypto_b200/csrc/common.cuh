@@ -46,7 +46,7 @@ struct Tuning {
   // groups of up to this many requests run their sponge stages on a warp each (0: never).
   // Off: a planned batch of 32 mixed requests took 12.2 ms with warp tasks, 4.5 ms without
   int mixed_warp_max = 0;
-  int pipe_chunks = 4;          // chunks (one stream each) of a pipelined host-mode batch, <= 8
+  int pipe_chunks = 4;          // chunks (one stream each) of a pipelined host-mode batch, <= 16
   int pipe_priority = 1;        // 1: chunk streams get descending priorities (earlier chunks finish first)
   int saber_pair_max = 6144;    // largest Saber batch whose prologue runs GenMatrix on lane pairs (0: never)
   int saber_warp_max = 512;     // largest Saber batch whose prologue sponges run on a warp per state (0: never)

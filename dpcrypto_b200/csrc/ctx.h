@@ -15,16 +15,16 @@ struct dpkem_ctx {
   size_t budget = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t last = nullptr;  // recorded after every launch chain that used the arena
-  cudaStream_t pipe[8] = {};   // host-mode copy/compute pipeline, one stream per chunk
-  cudaStream_t ppipe[8] = {};  // the same with descending priorities (chunk 0 highest)
-  cudaEvent_t pev[8] = {};
+  cudaStream_t pipe[16] = {};   // host-mode copy/compute pipeline, one stream per chunk
+  cudaStream_t ppipe[16] = {};  // the same with descending priorities (chunk 0 highest)
+  cudaEvent_t pev[16] = {};
   uint8_t *arena = nullptr;
   size_t arena_bytes = 0;
   uint32_t *d_err = nullptr;
   int max_ctas = 0;  // persistent launches use at most this many CTAs (0: two per SM)
-  uint8_t *h_stage[8] = {};      // pinned plan-table images, one per pipeline slot
-  size_t h_stage_bytes[8] = {};
-  cudaEvent_t stage_ev[8] = {};  // recorded after each stage's last upload
+  uint8_t *h_stage[16] = {};      // pinned plan-table images, one per pipeline slot
+  size_t h_stage_bytes[16] = {};
+  cudaEvent_t stage_ev[16] = {};  // recorded after each stage's last upload
   bool profile = false;
   dpkem::StageTimer timer;
   int timer_stages = 0;
@@ -35,7 +35,7 @@ namespace dpkem {
 namespace abi {
 
 constexpr size_t kAlign = 256;
-constexpr int kPipeChunks = 8;  // most chunks (and streams) of a pipelined host-mode batch
+constexpr int kPipeChunks = 16;  // most chunks (and streams) of a pipelined host-mode batch
 
 inline size_t up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 

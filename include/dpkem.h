@@ -256,7 +256,7 @@ int dpkem_saber_enc_batch_static(int scheme, int form, size_t n, const uint8_t *
 /* Runtime tuning knobs (process-wide): "thread_block" (block size of the thread-per-instance
  * kernels, multiple of 32, <= 256), "mixed_frodo_task" / "mixed_pair_task" /
  * "mixed_thread_task" (instances per thread-level task in mixed batches), "pipe_chunks"
- * (chunks, one stream each, of a pipelined host-buffer batch, <= 8), "pipe_priority" (0/1:
+ * (chunks, one stream each, of a pipelined host-buffer batch, <= 16), "pipe_priority" (0/1:
  * chunk streams with descending priorities, so earlier chunks finish first),
  * "saber_pair_max" (Keccak lanes per state in the Saber prologue: batches of up to this many
  * instances run GenMatrix on two lanes per state, larger ones on one; 0 = never).  Chosen by
