@@ -478,10 +478,13 @@ __device__ __forceinline__ void pack_group(const uint16_t *v, uint8_t *out) {
   }
 }
 // n coefficients (a multiple of the group size) into `out` (shared memory), CTA-wide.
+// Group g on thread (off + g) mod blockDim: a second pack in the same phase starts where the
+// first one's groups end.
 template <int BITS>
-__device__ __forceinline__ void pack_poly(const uint16_t *v, int n, uint8_t *out) {
+__device__ __forceinline__ void pack_poly(const uint16_t *v, int n, uint8_t *out, int off = 0) {
   constexpr int G = group_coefs<BITS>(), NB = G * BITS / 8;
-  for (int g = threadIdx.x; g < n / G; g += blockDim.x) pack_group<BITS>(v + g * G, out + g * NB);
+  const int nt = blockDim.x;
+  for (int g = ((int)threadIdx.x + nt - off % nt) % nt; g < n / G; g += nt) pack_group<BITS>(v + g * G, out + g * NB);
 }
 
 __device__ __forceinline__ uint32_t pack_byte(const uint16_t *v, int q, int bits) {
@@ -634,8 +637,12 @@ __device__ __forceinline__ void unpack_operands(const Inst &v, uint8_t *sm) {
   uint16_t *cm = reinterpret_cast<uint16_t *>(sm + Y::CM);
   // Public polynomials with 10-bit coefficients: 16 coefficients (5 words) per thread, two
   // 16-byte stores.
-  auto unpack_p = [&](const uint8_t *src) {
-    for (int g = tid; g < L * SN / 16; g += blockDim.x) {
+  // The unpack loops of one mode start at disjoint thread ranges (job g of a loop that starts
+  // at thread `off` runs on thread off + g), so no thread does two jobs while others wait at
+  // the barrier that follows: l = 3 encaps has 48 + 72 + 48 jobs for 256 threads.
+  auto job0 = [&](int off) { return (tid + (int)blockDim.x - off) % (int)blockDim.x; };
+  auto unpack_p = [&](const uint8_t *src, int off) {
+    for (int g = job0(off); g < L * SN / 16; g += blockDim.x) {
       uint32_t o[8];
       unpack_words<EP, 16>(reinterpret_cast<const uint32_t *>(src) + 5 * g, [&](int i, uint32_t x) {
         if (i & 1) o[i >> 1] |= x << 16;
@@ -660,12 +667,12 @@ __device__ __forceinline__ void unpack_operands(const Inst &v, uint8_t *sm) {
       d[0] = make_uint4(o[0], o[1], o[2], o[3]);
       d[1] = make_uint4(o[4], o[5], o[6], o[7]);
     }
-    unpack_p(ct);
+    unpack_p(ct, L * SN / 32);
     for (int c = tid; c < SN; c += blockDim.x) cm[c] = (uint16_t)unpack_smem(ct + P::POLYVECCOMP, c, P::ET);
   } else {
     // CBD_mu from the GenSecret bytes: 16 coefficients (mu/2 words) per thread.
     constexpr uint32_t hm = (1u << (P::MU / 2)) - 1u;
-    for (int g = tid; g < L * SN / 16; g += blockDim.x) {
+    for (int g = job0(0); g < L * SN / 16; g += blockDim.x) {
       uint32_t o[4];
       unpack_words<P::MU, 16>(reinterpret_cast<const uint32_t *>(sm + Y::ST_S) + (P::MU / 2) * g,
                               [&](int i, uint32_t x) {
@@ -676,7 +683,7 @@ __device__ __forceinline__ void unpack_operands(const Inst &v, uint8_t *sm) {
       reinterpret_cast<uint4 *>(secw)[g] = make_uint4(o[0], o[1], o[2], o[3]);
     }
     // GenMatrix: 13-bit coefficients, 32 (13 words) per thread, four 16-byte stores.
-    for (int g = tid; g < L * L * SN / 32; g += blockDim.x) {
+    for (int g = job0(L * SN / 16); g < L * L * SN / 32; g += blockDim.x) {
       uint32_t o[16];
       unpack_words<EQ, 32>(reinterpret_cast<const uint32_t *>(sm + Y::ST_A) + 13 * g, [&](int i, uint32_t x) {
         if (i & 1) o[i >> 1] |= x << 16;
@@ -686,7 +693,7 @@ __device__ __forceinline__ void unpack_operands(const Inst &v, uint8_t *sm) {
 #pragma unroll
       for (int q = 0; q < 4; q++) d[q] = make_uint4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
     }
-    if (MODE != PM_KEYPAIR) unpack_p(sm + Y::ST_P);
+    if (MODE != PM_KEYPAIR) unpack_p(sm + Y::ST_P, L * SN / 16 + L * L * SN / 32);
   }
 }
 
@@ -769,7 +776,7 @@ __device__ __forceinline__ void epilogue(const Inst &v, uint8_t *sm) {
     return;
   }
   pack_poly<EP>(res, L * SN, stg);
-  pack_poly<P::ET>(res + L * SN, SN, stg + P::POLYVECCOMP);
+  pack_poly<P::ET>(res + L * SN, SN, stg + P::POLYVECCOMP, L * SN / group_coefs<EP>());
   __syncthreads();
   if (MODE == PM_ENC) {
     copy8(v.ct, stg, P::CT);
