@@ -150,3 +150,26 @@ def test_i8_mma_peak_probe(engine):
     int8 MAC rate for a B200-class GPU (dense int8 is ~2 P MAC/s)."""
     macs = engine.probe_i8_mma_peak()
     assert 1e14 < macs < 1e16
+
+
+@pytest.mark.parametrize("chunks,prio", [(2, 0), (8, 1), (16, 1)])
+def test_host_pipeline_depths(engine, chunks, prio):
+    """Host-buffer batches split into up to 16 pipelined chunks (one stream each, with or
+    without descending priorities) give the device-pointer results on every instance."""
+    from dpcrypto_b200 import kem
+
+    for scheme, n in ((d.SABER, 4096), (d.FRODO976, 4096)):
+        z = d.sizes(scheme)
+        kc = torch.empty((n, z["kp_coins"]), dtype=torch.uint8, device="cuda")
+        ec = torch.empty((n, z["enc_coins"]), dtype=torch.uint8, device="cuda")
+        engine.coins(n, z["kp_coins"], "pipe-kp", first=chunks, out=kc)
+        engine.coins(n, z["enc_coins"], "pipe-enc", first=chunks, out=ec)
+        pk, sk = engine.keypair(scheme, kc, d.FORM_TC)
+        ct, ss = engine.enc(scheme, pk, ec, d.FORM_TC)
+        ss2 = engine.dec(scheme, ct, sk, d.FORM_TC)
+        torch.cuda.synchronize()
+        with kem.knobs(pipe_chunks=chunks, pipe_priority=prio):
+            h_ct, h_ss = engine.enc(scheme, pk.cpu().numpy(), ec.cpu().numpy(), d.FORM_TC)
+            h_ss2 = engine.dec(scheme, h_ct, sk.cpu().numpy(), d.FORM_TC)
+        assert (h_ct == ct.cpu().numpy()).all() and (h_ss == ss.cpu().numpy()).all()
+        assert (h_ss2 == ss2.cpu().numpy()).all() and (h_ss2 == h_ss).all()
