@@ -195,19 +195,21 @@ cudaError_t launch_product(const SaberBatch &b, int form, cudaStream_t st) {
     constexpr int bytes = Y::TC_TOTAL;
     const int per_sm = tuning().saber_tc_ctas_per_sm;
     if (per_sm > 0) {
-      // persistent: at most per_sm CTAs per SM (capped by what fits), several instances each
-      static int fits = 0, sms = 0;  // per process and instantiation: the kernel's resources are fixed
-      if (!fits) {
+      // persistent: per_sm CTAs per SM, several instances each.  The CTAs never wait on one
+      // another, so a grid larger than what is resident only queues; TMEM (32 columns per
+      // CTA) fits 16 CTAs per SM.
+      static int sms = 0;  // per process and instantiation
+      if (!sms) {
         if ((e = prep(product_tc_persistent_kernel<L, MODE>, bytes)) != cudaSuccess) return e;
-        int dev = 0, f = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f, product_tc_persistent_kernel<L, MODE>, 256,
-                                                                bytes)) != cudaSuccess)
+        if ((e = cudaFuncSetAttribute(product_tc_persistent_kernel<L, MODE>,
+                                      cudaFuncAttributePreferredSharedMemoryCarveout, 100)) != cudaSuccess)
           return e;
-        fits = f > 0 ? f : 1;
+        int dev = 0, m = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        sms = m > 0 ? m : 1;
       }
-      const int grid = std::min(b.n, sms * std::min(per_sm, fits));
+      const int grid = std::min(b.n, sms * per_sm);
       product_tc_persistent_kernel<L, MODE><<<grid, 256, bytes, st>>>(b);
     } else {
       if ((e = prep(product_tc_kernel<L, MODE>, bytes)) != cudaSuccess) return e;
