@@ -567,21 +567,27 @@ struct Staged {
   static constexpr int W0 = (INNER ? P::POLYVEC : P::ARAW) / 8;                      // words of piece 0
   static constexpr int W1 = (INNER ? P::CT : P::SRAW) / 8;                            // piece 1
   static constexpr int W2 = (INNER || MODE == PM_KEYPAIR) ? 0 : P::POLYVECCOMP / 8;  // piece 2
-  static constexpr int WORDS = W0 + W1 + W2;
+  // piece 3: the message bits m (32 bytes of scratch) that the epilogue encodes into v'
+  // (encaps, decaps re-encryption), staged in the CM region, which only the inner pass uses
+  static constexpr int W3 = (INNER || MODE == PM_KEYPAIR) ? 0 : 4;
+  static constexpr int WORDS = W0 + W1 + W2 + W3;
   static constexpr int PER_THREAD = (WORDS + 255) / 256;  // with 256 threads
   __device__ __forceinline__ static const uint2 *src(const Inst &v, int w) {
     if (INNER)
       return w < W0 ? reinterpret_cast<const uint2 *>(v.sk) + w : reinterpret_cast<const uint2 *>(v.ct) + (w - W0);
     if (w < W0) return reinterpret_cast<const uint2 *>(v.scr + Scr<L>::ARAW) + w;
     if (w < W0 + W1) return reinterpret_cast<const uint2 *>(v.scr + Scr<L>::SRAW) + (w - W0);
-    return reinterpret_cast<const uint2 *>(MODE == PM_ENC ? v.pk : v.sk + P::POLYVEC) + (w - W0 - W1);
+    if (w < W0 + W1 + W2)
+      return reinterpret_cast<const uint2 *>(MODE == PM_ENC ? v.pk : v.sk + P::POLYVEC) + (w - W0 - W1);
+    return reinterpret_cast<const uint2 *>(v.scr + Scr<L>::MTXT) + (w - W0 - W1 - W2);
   }
   __device__ __forceinline__ static uint2 *dst(uint8_t *sm, int w) {
     if (INNER)
       return w < W0 ? reinterpret_cast<uint2 *>(sm + Y::ST_SK) + w : reinterpret_cast<uint2 *>(sm + Y::ST_CT) + (w - W0);
     if (w < W0) return reinterpret_cast<uint2 *>(sm + Y::ST_A) + w;
     if (w < W0 + W1) return reinterpret_cast<uint2 *>(sm + Y::ST_S) + (w - W0);
-    return reinterpret_cast<uint2 *>(sm + Y::ST_P) + (w - W0 - W1);
+    if (w < W0 + W1 + W2) return reinterpret_cast<uint2 *>(sm + Y::ST_P) + (w - W0 - W1);
+    return reinterpret_cast<uint2 *>(sm + Y::CM) + (w - W0 - W1 - W2);
   }
 };
 
@@ -753,7 +759,7 @@ __device__ __forceinline__ void epilogue(const Inst &v, uint8_t *sm) {
   }
   for (int c = tid; c < L * SN; c += nt) res[c] = (uint16_t)((((uint32_t)res[c] + P::H1) >> (EQ - EP)) & 0x3FFu);
   if (MODE != PM_KEYPAIR) {
-    const uint8_t *mt = scr + S::MTXT;
+    const uint8_t *mt = sm + Y::CM;  // staged with the operands
     for (int c = tid; c < SN; c += nt) {
       const uint32_t mb = (mt[c >> 3] >> (c & 7)) & 1u;
       res[L * SN + c] = (uint16_t)((((uint32_t)res[L * SN + c] - (mb << (EP - 1)) + P::H1) >> (EP - P::ET)) &
