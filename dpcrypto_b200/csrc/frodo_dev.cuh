@@ -796,13 +796,16 @@ __device__ __forceinline__ void sa_dp4a_cta(const Inst &v, uint8_t *smem) {
 // B' = lo + 256 hi (mod 2^16).  Every producer warp issues its own MMAs and commits
 // them to its stage barrier; the tile ring has NST stages per warp.
 constexpr int TC_SP_BYTES = 62 * 128;
-constexpr int TC_STAGE = 6144;  // lo plane (6 x 512) + hi plane (6 x 512)
+// A tile stage: a warp's 32 squeezed blocks as an MN-major u8 operand, M = the block's 168
+// bytes in stream order (11 M-chunks of 16 bytes x 32 rows, 512 bytes each).
+constexpr int TC_STAGE = 6144;
 constexpr int TC_TMEM_COLS = 256;
 
 template <int NST>
 struct TcLayout {
   static constexpr int ring = TC_SP_BYTES;
-  static constexpr int bars = ring + 8 * NST * TC_STAGE + 1024;  // +1 KB: MMA reads M rows 96..127 past the last plane
+  // +2 KB: the second MMA of a stage reads M-chunks 8..15, up to 8 KB past the stage start
+  static constexpr int bars = ring + 8 * NST * TC_STAGE + 2048;
   static constexpr int tslot = bars + (8 * NST + 1) * 8;
   static constexpr int red = (tslot + 4 + 15) & ~15;
   static constexpr int total = red + 4 * 64 * 4;
@@ -860,38 +863,32 @@ __device__ __forceinline__ bool sa_tc_cta(const Inst &v, uint8_t *smem, uint32_t
     const uint64_t bdesc = sdesc(sp_addr + 256 * c, 128, 1024);
     for (int blk = 0; blk < 12; blk++, u++) {
       gen.next(a);
-      uint32_t lo[21], hi[21];
-#pragma unroll
-      for (int q = 0; q < 21; q++) {
-        lo[q] = prmt(a[q].x, a[q].y, 0x6420);
-        hi[q] = prmt(a[q].x, a[q].y, 0x7531);
-      }
       const int s = u % NST;
       if (u >= NST && ok) ok = mbar_wait(&bars[warp * NST + s], ((u / NST) - 1) & 1);
       ok = __all_sync(0xffffffffu, ok);
       uint8_t *stg = ring + (warp * NST + s) * TC_STAGE;
+      // The block's bytes as squeezed: entry e is M-row 2e (low byte) and 2e + 1 (high byte),
+      // so the u8 limbs need no byte permutes; the epilogue pairs the two rows' sums.
 #pragma unroll
-      for (int cc = 0; cc < 5; cc++) {
-        *reinterpret_cast<uint4 *>(stg + cc * 512 + roff) = make_uint4(lo[4 * cc], lo[4 * cc + 1], lo[4 * cc + 2], lo[4 * cc + 3]);
-        *reinterpret_cast<uint4 *>(stg + 3072 + cc * 512 + roff) =
-            make_uint4(hi[4 * cc], hi[4 * cc + 1], hi[4 * cc + 2], hi[4 * cc + 3]);
-      }
-      *reinterpret_cast<uint32_t *>(stg + 5 * 512 + roff) = lo[20];
-      *reinterpret_cast<uint32_t *>(stg + 3072 + 5 * 512 + roff) = hi[20];
+      for (int cc = 0; cc < 10; cc++)
+        *reinterpret_cast<uint4 *>(stg + cc * 512 + roff) =
+            make_uint4(a[2 * cc].x, a[2 * cc].y, a[2 * cc + 1].x, a[2 * cc + 1].y);
+      *reinterpret_cast<uint2 *>(stg + 10 * 512 + roff) = a[20];
       fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0 && ok) {
         tc_fence_after();
         const uint32_t sa = smem_u32(stg);
-        mma_i8(tbase + blk * 16, sdesc(sa, 128, 512), bdesc, idesc, 1u);
-        mma_i8(tbase + blk * 16 + 8, sdesc(sa + 3072, 128, 512), bdesc, idesc, 1u);
+        mma_i8(tbase + blk * 16, sdesc(sa, 128, 512), bdesc, idesc, 1u);             // entries 0..63
+        mma_i8(tbase + blk * 16 + 8, sdesc(sa + 4096, 128, 512), bdesc, idesc, 1u);  // entries 64..83
         mma_commit(&bars[warp * NST + s]);
       }
       __syncwarp();
     }
   }
   if (lane == 0) mma_commit(&bars[8 * NST]);
-  bool fin = mbar_wait(&bars[8 * NST], 0);
+  // 31 row groups over 8 warps: warp 7 finishes a group early and waits here asleep.
+  bool fin = mbar_wait_idle(&bars[8 * NST], 0);
   // Drain: observe each stage barrier's last phase, so no arrival is still pending
   // when the barriers are initialised again for the next instance.
   for (int s = 0; s < NST; s++)
@@ -899,23 +896,32 @@ __device__ __forceinline__ bool sa_tc_cta(const Inst &v, uint8_t *smem, uint32_t
   if ((!fin || !ok) && lane == 0) atomicOr(err, DEV_ERR_TIMEOUT);
   tc_fence_after();
 
-  // Epilogue: B'[k][84 blk + m] = lo + 256 hi + E' (mod 2^16).
+  // Epilogue: B'[k][84 blk + e] = lo + 256 hi + E' (mod 2^16).  TMEM lane 2e holds the
+  // low-byte sums of entry e, lane 2e + 1 the high-byte sums: columns 0..7 entries 0..63,
+  // columns 8..15 entries 64..83 (lanes 0..39).  Even lanes take the pair's result.
   uint32_t diff = 0;
-  const int qd = warp & 3, m = qd * 32 + lane, b0 = warp < 4 ? 0 : 6;
+  const int qd = warp & 3, t = qd * 32 + lane, b0 = warp < 4 ? 0 : 6;
   for (int blk = b0; blk < b0 + 6; blk++) {
     uint32_t r[16];
     tmem_ld16(tbase + ((uint32_t)(qd * 32) << 16) + blk * 16, r);
     tmem_wait_ld();
-    if (m < (blk < 11 ? 84 : 52)) {
-      const int col = 84 * blk + m;
 #pragma unroll
-      for (int k = 0; k < 8; k++) {
-        const uint32_t x = (r[k] + (r[8 + k] << 8) + rw[N * NBAR + k * N + col]) & 0xFFFFu;
-        uint8_t *d = v.ct + 2 * (k * N + col);
-        if (MODE == OP_ENC) {
-          *reinterpret_cast<uint16_t *>(d) = (uint16_t)((x >> 8) | (x << 8));
-        } else {
-          diff |= x ^ (((uint32_t)d[0] << 8) | d[1]);
+    for (int q = 0; q < 16; q++) r[q] += __shfl_down_sync(0xffffffffu, r[q], 1) << 8;
+    const int valid = blk < 11 ? 84 : 52;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int e = 64 * h + (t >> 1);
+      if ((lane & 1) == 0 && e < valid && (h == 0 || t < 40)) {
+        const int col = 84 * blk + e;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const uint32_t x = (r[8 * h + k] + rw[N * NBAR + k * N + col]) & 0xFFFFu;
+          uint8_t *d = v.ct + 2 * (k * N + col);
+          if (MODE == OP_ENC) {
+            *reinterpret_cast<uint16_t *>(d) = (uint16_t)((x >> 8) | (x << 8));
+          } else {
+            diff |= x ^ (((uint32_t)d[0] << 8) | d[1]);
+          }
         }
       }
     }

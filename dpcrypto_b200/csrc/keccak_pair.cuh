@@ -63,7 +63,7 @@ __device__ __forceinline__ void round(uint32_t (&a)[25], uint32_t rc, uint32_t q
   for (int x = 0; x < 5; x++) {
     const uint32_t r = rot<1>(c[(x + 1) % 5], q), l = c[(x + 4) % 5];
 #pragma unroll
-    for (int y = 0; y < 5; y++) a[x + 5 * y] ^= l ^ r;
+    for (int y = 0; y < 5; y++) a[x + 5 * y] = lop3_xor3(a[x + 5 * y], l, r);
   }
 #define DPKEM_RHOPI(i) b[kc::pi_dst(i)] = rot<kc::rho(i)>(a[i], q);
   DPKEM_RHOPI(0) DPKEM_RHOPI(1) DPKEM_RHOPI(2) DPKEM_RHOPI(3) DPKEM_RHOPI(4)
