@@ -2,6 +2,8 @@
 
 Knobs:
   keccak_unroll      rounds per iteration of the Keccak-f[1600] round loop (compile time)
+  keccak_unroll_rows the same for the A-row generators of the fused S'A / A S stages, timed
+                     on the S'A stages alone (compile time)
   thread_block       block size of the latency-bound thread-per-instance kernels
   mixed_frodo_task   instances per Frodo thread-level task in the persistent mixed kernel
   mixed_pair_task    instances per two-role prologue task (two threads per instance)
@@ -43,10 +45,22 @@ ROOT = os.path.dirname(HERE)
 VARIANTS = os.path.join(HERE, "_build", "variants")
 OUT = os.path.join(HERE, "tuning.json")
 UNROLLS = (1, 2, 3, 4)
+ROWS_UNROLLS = (1, 3, 6, 12)
 
 
 def variant_lib(u: int) -> str:
     return os.path.join(VARIANTS, f"unroll{u}", "libdpkem.so")
+
+
+def rows_variant_lib(r: int) -> str:
+    return os.path.join(VARIANTS, f"rows{r}", "libdpkem.so")
+
+
+def _chosen_unroll() -> int:
+    if os.path.exists(OUT):
+        with open(OUT) as f:
+            return int(json.load(f).get("chosen", {}).get("keccak_unroll", 1))
+    return 1
 
 
 def build_variants() -> None:
@@ -57,6 +71,41 @@ def build_variants() -> None:
         t = time.time()
         b.build(out=variant_lib(u), defines=[f"-DDPKEM_KECCAK_UNROLL={u}"])
         print(f"built unroll={u} in {time.time() - t:.0f} s", flush=True)
+    u = _chosen_unroll()
+    for r in ROWS_UNROLLS:
+        t = time.time()
+        b.build(out=rows_variant_lib(r), defines=[f"-DDPKEM_KECCAK_UNROLL={u}", f"-DDPKEM_KECCAK_UNROLL_ROWS={r}"])
+        print(f"built rows unroll={r} in {time.time() - t:.0f} s", flush=True)
+
+
+def _rows_child(r: int) -> dict:
+    """S'A stage milliseconds (encaps + decaps) at batch 8,192 with this library."""
+    import numpy as np
+    import torch
+
+    sys.path.insert(0, ROOT)
+    import dpcrypto_b200 as d
+
+    eng = d.Engine(0)
+    B = 8192
+    kc = torch.empty((B, 64), dtype=torch.uint8, device="cuda")
+    ec = torch.empty((B, 24), dtype=torch.uint8, device="cuda")
+    eng.coins(B, 64, "tune-kp", out=kc)
+    eng.coins(B, 24, "tune-enc", out=ec)
+    pk, sk = eng.keypair(d.FRODO976, kc, d.FORM_TC)
+    ct = torch.empty((B, 15744), dtype=torch.uint8, device="cuda")
+    ss = torch.empty((B, 24), dtype=torch.uint8, device="cuda")
+    eng.enc(d.FRODO976, pk, ec, d.FORM_TC, out=(ct, ss))
+    eng.dec(d.FRODO976, ct, sk, d.FORM_TC)
+    eng.profile(True)
+    ts = []
+    for _ in range(3):
+        eng.enc(d.FRODO976, pk, ec, d.FORM_TC, out=(ct, ss))
+        e = eng.stage_times()
+        eng.dec(d.FRODO976, ct, sk, d.FORM_TC)
+        ts.append(e[1] + eng.stage_times()[2])
+    eng.profile(False)
+    return {"keccak_unroll_rows": r, "sa_stages_b8192_ms": float(np.median(ts))}
 
 
 # ---------------------------------------------------------------- child: measure one library
@@ -319,6 +368,19 @@ def measure() -> dict:
         results.append(json.loads(r.stdout.strip().splitlines()[-1]))
         print(json.dumps(results[-1]), flush=True)
     best = min(results, key=lambda x: x["frodo_b4096_ms"])
+    rows = {}
+    for r in ROWS_UNROLLS:
+        lib = rows_variant_lib(r)
+        if not os.path.exists(lib):
+            print(f"missing {lib}; run --build first", file=sys.stderr)
+            continue
+        env = dict(os.environ, DPKEM_LIB=lib)
+        p = subprocess.run([sys.executable, "-m", "dpcrypto_b200.autotune", "--rows-child", str(r)], cwd=ROOT,
+                           env=env, capture_output=True, text=True, timeout=900)
+        if p.returncode != 0:
+            raise RuntimeError(f"rows variant {r} failed:\n{p.stdout}\n{p.stderr}")
+        rows[r] = json.loads(p.stdout.strip().splitlines()[-1])["sa_stages_b8192_ms"]
+        print(json.dumps({"keccak_unroll_rows": r, "sa_stages_b8192_ms": rows[r]}), flush=True)
     tb = min(best["thread_block_ms"], key=lambda k: best["thread_block_ms"][k])
     mk = min(best["mixed_task_ms"], key=best["mixed_task_ms"].get)
     pc, prio = (int(x) for x in min(best["pipe_chunks_priority_ms"], key=best["pipe_chunks_priority_ms"].get).split("/"))
@@ -328,7 +390,9 @@ def measure() -> dict:
 
     out = {
         "device": torch.cuda.get_device_name(0),
-        "chosen": {"keccak_unroll": best["keccak_unroll"], "thread_block": int(tb), "mixed_frodo_task": ft,
+        "chosen": {"keccak_unroll": best["keccak_unroll"],
+                   **({"keccak_unroll_rows": min(rows, key=rows.get)} if rows else {}),
+                   "thread_block": int(tb), "mixed_frodo_task": ft,
                    "mixed_pair_task": stt, "mixed_thread_task": tt, "pipe_chunks": pc,
                    "pipe_priority": prio, **lanes},
         "fixed": {"mma_tile": "M=128 (N=8 Frodo, N=8/16 Saber), K=32: int8 MMA <1% of the tensor pipe in the fused "
@@ -336,6 +400,7 @@ def measure() -> dict:
                               "instances), two CTAs per SM (TMEM)",
                   "keccak_lanes_per_state_fused_sa_stages": 1},
         "measurements": results,
+        "measurements_rows_unroll": {str(r): v for r, v in rows.items()},
         "command": "python -m dpcrypto_b200.autotune --measure",
         "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
     }
@@ -354,9 +419,13 @@ def main():
     ap.add_argument("--build", action="store_true")
     ap.add_argument("--measure", action="store_true")
     ap.add_argument("--child", type=int)
+    ap.add_argument("--rows-child", type=int)
     a = ap.parse_args()
     if a.child is not None:
         print(json.dumps(_child(a.child)))
+        return
+    if a.rows_child is not None:
+        print(json.dumps(_rows_child(a.rows_child)))
         return
     if a.build:
         build_variants()

@@ -55,7 +55,11 @@ def tuning_defines() -> list:
         return []
     with open(TUNING) as f:
         chosen = json.load(f).get("chosen", {})
-    return [f"-DDPKEM_KECCAK_UNROLL={int(chosen['keccak_unroll'])}"] if "keccak_unroll" in chosen else []
+    defs = []
+    for key, macro in (("keccak_unroll", "DPKEM_KECCAK_UNROLL"), ("keccak_unroll_rows", "DPKEM_KECCAK_UNROLL_ROWS")):
+        if key in chosen:
+            defs.append(f"-D{macro}={int(chosen[key])}")
+    return defs
 
 
 def build(verbose: bool = False, out: str | None = None, defines: list | None = None) -> str:

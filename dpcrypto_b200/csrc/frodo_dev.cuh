@@ -458,7 +458,7 @@ struct ShakeRows {
     sa1 = ld_lane(seed + 8);
   }
   __device__ __forceinline__ void start(uint2 (&a)[25], uint32_t j) { row_init(a, j, sa0, sa1); }
-  __device__ __forceinline__ void next(uint2 (&a)[25]) { keccak_f1600(a); }
+  __device__ __forceinline__ void next(uint2 (&a)[25]) { keccak_f1600_u<kKeccakUnrollRows>(a); }
 };
 
 // MemRows: rows of an A expanded once in memory (976 x 976 LE u16, row-major; shared-key
@@ -887,8 +887,11 @@ __device__ __forceinline__ bool sa_tc_cta(const Inst &v, uint8_t *smem, uint32_t
     }
   }
   if (lane == 0) mma_commit(&bars[8 * NST]);
-  // 31 row groups over 8 warps: warp 7 finishes a group early and waits here asleep.
-  bool fin = mbar_wait_idle(&bars[8 * NST], 0);
+  // 31 row groups over 8 warps: warp 7 runs out of rows a group early.  It waits in the
+  // hardware barrier, which issues nothing, not in an mbarrier poll loop whose compares and
+  // branches would take ALU slots from the warps still hashing.
+  __syncthreads();
+  bool fin = mbar_wait(&bars[8 * NST], 0);
   // Drain: observe each stage barrier's last phase, so no arrival is still pending
   // when the barriers are initialised again for the next instance.
   for (int s = 0; s < NST; s++)

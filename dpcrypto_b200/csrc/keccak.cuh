@@ -116,12 +116,23 @@ __device__ __forceinline__ void keccak_round(uint2 (&a)[25], uint2 rcv) {
 #define DPKEM_KECCAK_UNROLL 2
 #endif
 
-constexpr int kKeccakUnroll = DPKEM_KECCAK_UNROLL;
+// Rounds per loop iteration in the A-row generators' permutation: one call site per kernel,
+// in a loop the compiler keeps in vector registers (a counter and a constant address
+// updated per iteration), so a longer body pays there.
+#ifndef DPKEM_KECCAK_UNROLL_ROWS
+#define DPKEM_KECCAK_UNROLL_ROWS 1
+#endif
 
-__device__ __forceinline__ void keccak_f1600(uint2 (&a)[25]) {
-#pragma unroll kKeccakUnroll
+constexpr int kKeccakUnroll = DPKEM_KECCAK_UNROLL;
+constexpr int kKeccakUnrollRows = DPKEM_KECCAK_UNROLL_ROWS;
+
+template <int U>
+__device__ __forceinline__ void keccak_f1600_u(uint2 (&a)[25]) {
+#pragma unroll U
   for (int r = 0; r < 24; r++) keccak_round(a, c_keccak_rc[r]);
 }
+
+__device__ __forceinline__ void keccak_f1600(uint2 (&a)[25]) { keccak_f1600_u<kKeccakUnroll>(a); }
 
 __device__ __forceinline__ void keccak_zero(uint2 (&a)[25]) {
 #pragma unroll

@@ -57,19 +57,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   }
 }
 
-// The same bounded wait for a phase that may be far off, such as a warp that has run out of
-// work waiting on the rest of its CTA: the warp sleeps between polls, so the wait takes no
-// issue slots (nor ALU slots for its timeout arithmetic) from the warps still computing.
-__device__ __forceinline__ bool mbar_wait_idle(uint64_t *bar, uint32_t parity, uint32_t sleep_ns = 256) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const uint64_t t0 = globaltimer_ns();
-  while (true) {
-    __nanosleep(sleep_ns);
-    if (mbar_try_wait(bar, parity)) return true;
-    if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
-  }
-}
-
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
