@@ -275,7 +275,7 @@ def _lanes_sweep(eng, d, kem) -> dict:
     psweep = {}
     for n in (1024, 4096, 16384):
         inputs = keys(d.SABER, n)
-        for per_sm in (0, 1, 2, 4, 8):
+        for per_sm in (0, 1, 2, 4, 5, 8):
             with kem.knobs(saber_tc_ctas_per_sm=per_sm):
                 psweep[f"{n}/{per_sm}"] = stage_ms(d.SABER, inputs, (1,), (0, 2))
         del inputs

@@ -163,7 +163,7 @@ def test_saber_sponges_on_several_lanes(engine, oracle, level, layout):
 
 
 @pytest.mark.parametrize("level", LEVELS)
-@pytest.mark.parametrize("per_sm", [0, 1, 4])
+@pytest.mark.parametrize("per_sm", [0, 1, 4, 5])
 def test_saber_tc_product_persistent(engine, oracle, level, per_sm):
     """The tensor-core product with a CTA per instance (0) or as persistent CTAs that each
     take several instances and prefetch the next one's operands (1: 148 CTAs, so n = 333
