@@ -10,10 +10,15 @@ namespace {
 using namespace frodo;
 using fdev::inst_of;
 
+// Thread-per-instance prologues: dynamic shared memory of kParkBytes per thread parks the
+// sampling stream's blocks (fdev::sample_stream).
+constexpr int kParkBytes = 17 * 8;
+
 template <int OP>
 __global__ void __launch_bounds__(256) kp_prologue_kernel(FrodoBatch b) {
+  extern __shared__ uint2 park[];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < b.n) fdev::kp_prologue_inst(inst_of(b, i, OP));
+  if (i < b.n) fdev::kp_prologue_inst(inst_of(b, i, OP), park + threadIdx.x, blockDim.x);
 }
 
 template <int OP>
@@ -24,16 +29,18 @@ __global__ void __launch_bounds__(256) pk_hash_kernel(FrodoBatch b) {
 
 template <int MODE>
 __global__ void __launch_bounds__(256) prologue_kernel(FrodoBatch b) {
+  extern __shared__ uint2 park[];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < b.n) fdev::prologue_inst<MODE>(inst_of(b, i, MODE));
+  if (i < b.n) fdev::prologue_inst<MODE>(inst_of(b, i, MODE), park + threadIdx.x, blockDim.x);
 }
 
 // Decaps prologue, 64 threads = 32 instances: warp 0 runs the sampling chain, warp 1 the
 // ciphertext pre-absorb of the final hash.
 __global__ void __launch_bounds__(64) dec_prologue_kernel(FrodoBatch b) {
+  __shared__ uint2 park[17 * 32];
   const int i = blockIdx.x * 32 + (threadIdx.x & 31);
   if (i >= b.n) return;
-  if (threadIdx.x < 32) fdev::prologue_inst<OP_DEC>(inst_of(b, i, OP_DEC));
+  if (threadIdx.x < 32) fdev::prologue_inst<OP_DEC>(inst_of(b, i, OP_DEC), park + threadIdx.x, 32);
   else fdev::ct_absorb_inst(inst_of(b, i, OP_DEC));
 }
 
@@ -292,7 +299,7 @@ cudaError_t frodo_keypair(const FrodoBatch &b, int form, cudaStream_t st) {
   const int tb = tuning().thread_block;
   mark(b, st);
   if (!launch_multi<0>(b, tuning().frodo_warp_max, tuning().frodo_five_max, st))
-    kp_prologue_kernel<OP_KEYPAIR><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
+    kp_prologue_kernel<OP_KEYPAIR><<<blocks_for(b.n, tb), tb, kParkBytes * tb, st>>>(b);
   mark(b, st);
   const cudaError_t e = b.aes ? launch_kp_as<fdev::AesRowsFull, 1>(b, form, st)
                              : launch_kp_as<fdev::ShakeRows, fdev::KPT_NST>(b, form, st);
@@ -307,7 +314,7 @@ cudaError_t frodo_enc(const FrodoBatch &b, int form, cudaStream_t st) {
   if (b.n <= 0) return cudaSuccess;
   const int tb = tuning().thread_block;
   mark(b, st);
-  if (!launch_multi<2>(b, tuning().frodo_warp_max, tuning().frodo_five_max, st)) prologue_kernel<OP_ENC><<<blocks_for(b.n, tb), tb, 0, st>>>(b);
+  if (!launch_multi<2>(b, tuning().frodo_warp_max, tuning().frodo_five_max, st)) prologue_kernel<OP_ENC><<<blocks_for(b.n, tb), tb, kParkBytes * tb, st>>>(b);
   mark(b, st);
   cudaError_t e = launch_sa<OP_ENC>(b, form, st);
   if (e != cudaSuccess) return e;

@@ -111,11 +111,42 @@ __device__ __forceinline__ void seed_stream_init(uint2 (&a)[25], uint32_t dom, u
   absorb_finish<136>(a, 25, 0x1Fu);
 }
 
+// Sample one squeezed lane (four 16-bit values) to dst[at..at+3] if at < words, and to
+// dst_le too while at < le_words.  The stores are predicated, not branched around.
+__device__ __forceinline__ void sample_store(uint2 w, int at, uint16_t *dst, int words, uint8_t *dst_le,
+                                             int le_words) {
+  const uint2 v = sample_lane(w);
+  if (at < words) *reinterpret_cast<uint2 *>(dst + at) = v;
+  if (dst_le && at < le_words) *reinterpret_cast<uint2 *>(dst_le + 2 * at) = v;
+}
+
 // Squeeze `words` sampled 16-bit values of the stream into dst (8-byte aligned);
 // when dst_le is non-null the first `le_words` values are also written there (sk's S^T).
+// With `park` (this thread's column of 17 uint2 in shared memory, `stride` apart), every block
+// but the last is parked there and sampled during the permutation that produces the next one,
+// one lane per round for the first 17 rounds: the CDF comparisons (FMA pipe) and the stores
+// then issue between the round's ALU ops.  A thread-per-instance prologue runs about one warp
+// per SM sub-partition, where the ALU pipe bounds the permutation and issue slots are free;
+// sampled after the permutation instead, a block cost about 40 % more than its permutation.
 __device__ __forceinline__ void sample_stream(uint2 (&a)[25], uint16_t *dst, int words, uint8_t *dst_le,
-                                              int le_words) {
+                                              int le_words, uint2 *park = nullptr, int stride = 0) {
   const int nblk = (words + 67) / 68;
+  if (park != nullptr) {
+    for (int blk = 0; blk + 1 < nblk; blk++) {
+#pragma unroll
+      for (int q = 0; q < 17; q++) park[q * stride] = a[q];
+#pragma unroll 1
+      for (int r = 0; r < 17; r++) {
+        keccak_round(a, c_keccak_rc[r]);
+        sample_store(park[r * stride], blk * 68 + 4 * r, dst, words, dst_le, le_words);
+      }
+#pragma unroll 1
+      for (int r = 17; r < 24; r++) keccak_round(a, c_keccak_rc[r]);
+    }
+#pragma unroll
+    for (int q = 0; q < 17; q++) sample_store(a[q], (nblk - 1) * 68 + 4 * q, dst, words, dst_le, le_words);
+    return;
+  }
   for (int blk = 0; blk < nblk; blk++) {
     if (blk) keccak_f1600(a);
 #pragma unroll
@@ -131,7 +162,7 @@ __device__ __forceinline__ void sample_stream(uint2 (&a)[25], uint16_t *dst, int
 }
 
 // ---------------------------------------------------------------- thread-level stages
-__device__ __forceinline__ void kp_prologue_inst(const Inst &v) {
+__device__ __forceinline__ void kp_prologue_inst(const Inst &v, uint2 *park = nullptr, int stride = 0) {
   uint2 a[25];
   // seedA = SHAKE256(z, 16)
   keccak_zero(a);
@@ -146,7 +177,7 @@ __device__ __forceinline__ void kp_prologue_inst(const Inst &v) {
   for (int q = 0; q < 3; q++) *reinterpret_cast<uint2 *>(v.sk + 8 * q) = ld_lane(v.coins + 8 * q);
   // S^T || E = sample(SHAKE256(0x5F || seedSE))
   seed_stream_init(a, 0x5Fu, ld_lane(v.coins + 24), ld_lane(v.coins + 32), ld_lane(v.coins + 40));
-  sample_stream(a, v.rw, 2 * N * NBAR, v.sk + SK_S, N * NBAR);
+  sample_stream(a, v.rw, 2 * N * NBAR, v.sk + SK_S, N * NBAR, park, stride);
 }
 
 // H(pk) = SHAKE256(pk, 24) into sk.
@@ -159,8 +190,10 @@ __device__ __forceinline__ void pk_hash_inst(const Inst &v) {
   for (int q = 0; q < 3; q++) *reinterpret_cast<uint2 *>(v.sk + SK_PKH + 8 * q) = a[q];
 }
 
+// park / stride: shared memory for sample_stream's overlapped form (null: sample after each
+// permutation, as the stages of the persistent kernels do).
 template <int MODE>
-__device__ __forceinline__ void prologue_inst(const Inst &v) {
+__device__ __forceinline__ void prologue_inst(const Inst &v, uint2 *park = nullptr, int stride = 0) {
   uint2 a[25], pkh[3], mu[3];
   if (MODE == OP_ENC) {
     if (v.pkh) {  // shared-key batch: H(pk) hashed once
@@ -194,7 +227,7 @@ __device__ __forceinline__ void prologue_inst(const Inst &v) {
 #pragma unroll
   for (int q = 0; q < 3; q++) *reinterpret_cast<uint2 *>(v.kk + 8 * q) = a[3 + q];
   seed_stream_init(a, 0x96u, a[0], a[1], a[2]);
-  sample_stream(a, v.rw, RW, nullptr, 0);
+  sample_stream(a, v.rw, RW, nullptr, 0, park, stride);
 }
 
 // Decaps: ss = SHAKE256(ct || k-hat) absorbs the input ciphertext's 115 full rate blocks
