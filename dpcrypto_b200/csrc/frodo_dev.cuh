@@ -65,10 +65,13 @@ __device__ __forceinline__ uint32_t sample16(uint32_t v) {
   return (((0u - sign) ^ s) + sign) & 0xFFFFu;
 }
 
-// The same sampler with its ten comparisons on the FMA pipe, which Keccak leaves idle:
-// x = CDF[c] - t by mad.lo (t * (2^32 - 1) + CDF[c]) and s += x >> 31 by mad.hi (hi32(x * 2)).
-// The multipliers come from opaque registers so the compiler cannot turn them back into
-// integer-ALU adds and shifts.  Bit-identical to sample16 (checked exhaustively on the GPU).
+// The same sampler written as multiply-adds: x = CDF[c] - t by mad.lo (t * (2^32 - 1) + CDF[c])
+// and s += x >> 31 by mad.hi (hi32(x * 2)), multipliers moved into registers.  The compiler
+// still sees the constants: in the thread-per-instance prologue ncu shows the FMA pipe 0.4 %
+// active, so these run as integer-ALU ops.  Multipliers read from constant memory do keep
+// them on the FMA pipe, and that form made the prologues slower (encaps 2.10 -> 2.50 ms,
+// decaps 1.50 -> 1.76 ms at 8,192), so this one stays.  Bit-identical to sample16 (checked
+// exhaustively on the GPU).
 struct FmaConsts {
   uint32_t neg1, two;
 };
