@@ -155,16 +155,28 @@ __device__ __forceinline__ int absorb_aligned(uint2 (&a)[25], int pos, const uin
     p += 8;
     len -= 8;
   }
-  while (len >= RATE) {
+  // Whole blocks: the next block's words are loaded before the permutation of this one, so
+  // their global-load latency passes during the permutation instead of before the XOR.
+  if (len >= RATE) {
+    uint2 w[RATE / 8];
 #pragma unroll
-    for (int q = 0; q < RATE / 8; q++) {
-      const uint2 w = ld_lane(p + 8 * q);
-      a[q].x ^= w.x;
-      a[q].y ^= w.y;
+    for (int q = 0; q < RATE / 8; q++) w[q] = ld_lane(p + 8 * q);
+    while (true) {
+#pragma unroll
+      for (int q = 0; q < RATE / 8; q++) {
+        a[q].x ^= w[q].x;
+        a[q].y ^= w[q].y;
+      }
+      p += RATE;
+      len -= RATE;
+      const bool more = len >= RATE;
+      if (more) {
+#pragma unroll
+        for (int q = 0; q < RATE / 8; q++) w[q] = ld_lane(p + 8 * q);
+      }
+      keccak_f1600(a);
+      if (!more) break;
     }
-    keccak_f1600(a);
-    p += RATE;
-    len -= RATE;
   }
   while (len > 0) {
     pos = absorb_word<RATE>(a, pos, ld_lane(p));
