@@ -87,10 +87,39 @@ __device__ __forceinline__ void move4(uint2 (&dst)[S::NS], const uint2 (&src)[S:
 
 // Absorb whole 8-byte words (len % 8 == 0, p 8-byte aligned) at fill `pos` (a multiple of
 // 8); returns the new fill.
+// Whole blocks at fill 0 load the next block's words before permuting the current one, so the
+// global-load latency passes during the permutation.
 template <class S, int RATE>
 __device__ __forceinline__ int absorb_aligned(uint2 (&a)[S::NS], const S &s, int pos, const uint8_t *p, int len,
                                               bool live) {
   constexpr int W = RATE / 8;
+  if (pos == 0 && len >= RATE) {
+    uint2 w[S::NS];
+#pragma unroll
+    for (int y = 0; y < S::NS; y++) {
+      const int q = s.lane(y);
+      w[y] = (q < W && live) ? ld_lane(p + 8 * q) : make_uint2(0u, 0u);
+    }
+    while (true) {
+#pragma unroll
+      for (int y = 0; y < S::NS; y++) {
+        a[y].x ^= w[y].x;
+        a[y].y ^= w[y].y;
+      }
+      p += RATE;
+      len -= RATE;
+      const bool more = len >= RATE;
+      if (more) {
+#pragma unroll
+        for (int y = 0; y < S::NS; y++) {
+          const int q = s.lane(y);
+          if (q < W && live) w[y] = ld_lane(p + 8 * q);
+        }
+      }
+      s.perm(a);
+      if (!more) break;
+    }
+  }
   while (len > 0) {
     const int take = min(len, RATE - pos);
     const int q0 = pos / 8, nq = take / 8;
