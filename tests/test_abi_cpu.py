@@ -146,3 +146,17 @@ def test_service_host_checks():
     assert lib.dpkem_service_poll(None, None, 0, None) == kem.EINVAL
     assert lib.dpkem_service_drain(None, 10) == kem.EINVAL
     assert lib.dpkem_service_close(None) == kem.EINVAL
+
+
+def test_build_defines_from_tuning(tmp_path, monkeypatch):
+    """Both Keccak round-unroll knobs in tuning.json become compile-time defines."""
+    import json
+
+    from dpcrypto_b200 import build
+
+    t = tmp_path / "tuning.json"
+    t.write_text(json.dumps({"chosen": {"keccak_unroll": 2, "keccak_unroll_rows": 6, "thread_block": 32}}))
+    monkeypatch.setattr(build, "TUNING", str(t))
+    assert build.tuning_defines() == ["-DDPKEM_KECCAK_UNROLL=2", "-DDPKEM_KECCAK_UNROLL_ROWS=6"]
+    t.write_text(json.dumps({"chosen": {"keccak_unroll": 1}}))
+    assert build.tuning_defines() == ["-DDPKEM_KECCAK_UNROLL=1"]
