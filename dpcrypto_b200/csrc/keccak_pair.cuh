@@ -152,12 +152,25 @@ __device__ __forceinline__ int absorb_aligned(uint32_t (&a)[25], int pos, const 
       pos = 0;
     }
   }
-  while (len >= RATE) {
+  // Whole blocks: the next block's words are loaded before this block's permutation, so the
+  // global-load latency passes during it.
+  if (len >= RATE) {
+    uint2 w[RATE / 8];
 #pragma unroll
-    for (int q = 0; q < RATE / 8; q++) a[q] ^= to_slice(ld_lane(m + 8 * q), p);
-    f1600(a, p);
-    m += RATE;
-    len -= RATE;
+    for (int q = 0; q < RATE / 8; q++) w[q] = ld_lane(m + 8 * q);
+    while (true) {
+#pragma unroll
+      for (int q = 0; q < RATE / 8; q++) a[q] ^= to_slice(w[q], p);
+      m += RATE;
+      len -= RATE;
+      const bool more = len >= RATE;
+      if (more) {
+#pragma unroll
+        for (int q = 0; q < RATE / 8; q++) w[q] = ld_lane(m + 8 * q);
+      }
+      f1600(a, p);
+      if (!more) break;
+    }
   }
   while (len > 0) {
 #pragma unroll
